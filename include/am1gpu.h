@@ -1,0 +1,158 @@
+/*
+ * am1gpu.h -- C ABI of the B200 NDDO (AM1/RM1) SCF library, libam1gpu.so.
+ *
+ * This is the drop-in boundary for am1-rs's molecular single point.  Every entry point takes
+ * plain pointers and sizes; all buffers are caller-owned host memory.  Units follow am1-rs:
+ * positions in Bohr in, energies in eV and kcal/mol out, with MOPAC7's constants
+ * (27.21 eV/Hartree, 0.529167 Angstrom/Bohr, 23.061 kcal/mol per eV; src/constants.rs:13-25).
+ *
+ * Thread safety: every entry point may be called from several host threads at once (the
+ * reference's Python binding releases the GIL around run_am1, src/python.rs:162-164).  Each
+ * host thread gets its own CUDA stream and device workspace; the only shared state is the
+ * once-initialised device context and the per-method parameter upload.
+ *
+ * There is no CPU fallback behind these functions: without a usable CUDA device every compute
+ * entry point returns AM1GPU_DEVICE_ERROR.
+ */
+#ifndef AM1GPU_H
+#define AM1GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes.  They mirror am1-rs's Am1Error variants (src/error.rs:13-93). */
+enum am1gpu_status {
+    AM1GPU_OK = 0,
+    AM1GPU_INVALID_INPUT = 1,              /* Am1Error::InvalidInput            (error.rs:18) */
+    AM1GPU_ELEMENT_NOT_PARAMETERIZED = 2,  /* Am1Error::ElementNotParameterized (error.rs:28-32) */
+    AM1GPU_SCF_NOT_CONVERGED = 3,          /* Am1Error::ScfNotConverged          (error.rs:35-38) */
+    AM1GPU_SCF_DIVERGED = 4,               /* Am1Error::ScfDiverged              (error.rs:45-47) */
+    AM1GPU_LINALG = 5,                     /* Am1Error::LinearAlgebra            (error.rs:33) */
+    AM1GPU_UNSUPPORTED = 6,                /* element with a valence shell n >= 4: its Slater
+                                              overlap needs the numerical quadrature of
+                                              src/overlap_numeric.rs, not on this path */
+    AM1GPU_DEVICE_ERROR = 7                /* CUDA failure or no device */
+};
+
+/* ScfReference (src/scf.rs:28-38). */
+enum { AM1GPU_REF_AUTO = 0, AM1GPU_REF_RHF = 1, AM1GPU_REF_UHF = 2 };
+/* ScfAccelerator (src/scf.rs:42-52). */
+enum { AM1GPU_ACCEL_NONE = 0, AM1GPU_ACCEL_CDIIS = 1, AM1GPU_ACCEL_ADIIS_CDIIS = 2 };
+/* NddoMethod (src/method.rs). */
+enum { AM1GPU_METHOD_AM1 = 0, AM1GPU_METHOD_RM1 = 1 };
+/* Arithmetic of the batched path (the plain path is always FP64). */
+enum { AM1GPU_PRECISION_FP64 = 0, AM1GPU_PRECISION_MIXED = 1 };
+
+/*
+ * The molecular subset of Am1Options (src/scf.rs:54-154, defaults :174-197).  Fields that do
+ * nothing for a molecule with default options (realspace_cutoff, ewald, klopman_ohno_tail,
+ * exchange_cutoff, multipole_cutoff, electric_field, cphf_*) are not carried.
+ */
+typedef struct {
+    int32_t reference;     /* AM1GPU_REF_*, default AUTO */
+    int32_t method;        /* AM1GPU_METHOD_*, default AM1 (selects the parameter table) */
+    int32_t max_scf;       /* default 200 */
+    int32_t use_diis;      /* default 1; 0 forces plain iteration */
+    int32_t accelerator;   /* AM1GPU_ACCEL_*, default ADIIS_CDIIS */
+    int32_t precision;     /* AM1GPU_PRECISION_*, default FP64; only am1gpu_scf_batch reads it */
+    double e_tol;          /* eV, default 1e-8 */
+    double p_tol;          /* default 1e-7 */
+    double adiis_switch;   /* default 0.1 */
+} am1gpu_options;
+
+/* One molecule: Molecule (src/system.rs:27-39) plus Am1Options::charge / multiplicity. */
+typedef struct {
+    int32_t natoms;
+    int32_t multiplicity;      /* 2S+1, >= 1 */
+    double charge;             /* total charge, e */
+    const int32_t* z;          /* natoms atomic numbers */
+    const double* xyz_bohr;    /* natoms*3 positions, Bohr */
+} am1gpu_molecule;
+
+/*
+ * Am1Result (src/scf.rs:200-240).  Scalars are always written when the SCF ran (also when it
+ * returns AM1GPU_SCF_NOT_CONVERGED, so the caller can see the residual it reached); the
+ * array pointers are caller-owned outputs and any of them may be NULL to skip it.
+ */
+typedef struct {
+    double electronic_ev;
+    double core_ev;
+    double total_ev;
+    double heat_of_formation_kcal;
+    double dipole_debye[3];
+    double dipole_magnitude;
+    double homo_ev, lumo_ev;             /* NaN when absent */
+    double homo_beta_ev, lumo_beta_ev;   /* UHF only, NaN otherwise */
+    double residual;                     /* ||[F,P]|| of the last iteration */
+    int32_t nao;
+    int32_t n_occ;                       /* doubly occupied (RHF) or alpha occupied (UHF) */
+    int32_t n_occ_beta;
+    int32_t iterations;
+    int32_t converged;
+    int32_t unrestricted;
+    double* charges;        /* [natoms]   Mulliken net charges */
+    double* density;        /* [nao*nao]  total density, row-major */
+    double* spin_density;   /* [nao*nao]  P_alpha - P_beta (UHF only) */
+    double* mo_energies;    /* [nao]      ascending, eV (alpha for UHF) */
+    double* mo_coeff;       /* [nao*nao]  row-major, columns are MOs (alpha for UHF) */
+    double* beta_energies;  /* [nao]      UHF only */
+    double* beta_coeff;     /* [nao*nao]  UHF only */
+} am1gpu_result;
+
+/* Fill *opts with Am1Options::default() (src/scf.rs:174-197). */
+void am1gpu_default_options(am1gpu_options* opts);
+
+/* Number of valence AOs of a molecule: Basis::build (src/basis.rs:37-60).  Returns
+ * AM1GPU_ELEMENT_NOT_PARAMETERIZED for an element the method does not cover. */
+int am1gpu_basis_size(int32_t natoms, const int32_t* z, int32_t method, int32_t* nao);
+
+/*
+ * Plain FP64 single point of one molecule: replaces run_am1 (src/scf.rs:294-468) for a
+ * molecule.  Returns AM1GPU_OK, or the error run_am1 would raise; AM1GPU_SCF_NOT_CONVERGED
+ * still fills *res.
+ */
+int am1gpu_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res);
+
+/*
+ * Batched single points: nmol independent molecules solved together on the device, each with
+ * its own SCF trajectory and convergence test (same per-molecule semantics as am1gpu_scf).
+ * status[i] receives molecule i's return code.  The return value is AM1GPU_OK when every
+ * molecule succeeded, otherwise the first failing code.  opts->precision selects FP64 or
+ * the mixed path (FP32 eigensolve and density with FP64 refinement).
+ */
+int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
+                     am1gpu_result* results, int32_t* status);
+
+/*
+ * Core Hamiltonian and core-core energy of one molecule: replaces build_core_with_neighbors
+ * (src/hamiltonian.rs:211-366) and core_core_energy_with_neighbors (src/repulsion.rs:38-56)
+ * for a molecule.  h_core is nao*nao row-major (eV); *core_ev in eV.
+ */
+int am1gpu_build_core(const am1gpu_molecule* mol, int32_t method, double* h_core, double* core_ev);
+
+/*
+ * Spin Fock matrix F = H_core + J(p_tot) - K(spin_scale * p_spin): replaces
+ * build_fock_spin_with (src/fock.rs:249-511) with FockBase::CoreHamiltonian.  RHF is
+ * p_spin = p_tot with spin_scale 0.5 (build_fock, src/fock.rs:526-546).
+ */
+int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* p_tot,
+                      const double* p_spin, double spin_scale, double* fock);
+
+/*
+ * Symmetric eigendecomposition: replaces symmetric_eigen (src/linalg.rs:276-331).
+ * a is n*n row-major; w receives ascending eigenvalues; v (row-major) the eigenvectors as
+ * columns.  Non-finite input returns AM1GPU_LINALG, as the reference refuses it.
+ */
+int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* am1gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AM1GPU_H */
