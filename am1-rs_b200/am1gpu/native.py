@@ -1,0 +1,252 @@
+"""Python surface of the B200 library, mirroring am1-rs's ``am1_rs.native`` (python/am1_rs/native.py).
+
+``single_point`` and ``orbitals`` take the reference's arguments (atomic numbers, positions in
+Angstrom, charge, multiplicity, reference, method) and return the same dictionary keys
+(src/python.rs:147-199, 1911-1975); errors raise ``ValueError`` as the reference's binding does
+(src/python.rs:27-29).  Every call goes through ``libam1gpu.so``'s C ABI; there is no CPU path.
+``scf`` / ``scf_batch`` expose the full result (density, orbitals) for one molecule or a batch,
+positions in Bohr.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+
+from . import _abi
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Am1GpuError(ValueError):
+    """An am1-rs error (``Am1Error``) reported by the library; ``code`` is the ``am1gpu_status``."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def ensure_loaded() -> ctypes.CDLL:
+    """Load the library (raises if it is missing)."""
+    return _abi.lib()
+
+
+def _check(rc: int, allow_not_converged: bool = False):
+    if rc == _abi.OK or (allow_not_converged and rc == _abi.SCF_NOT_CONVERGED):
+        return
+    raise Am1GpuError(rc, _abi.lib().am1gpu_last_error().decode() or _abi.STATUS_NAMES.get(rc, str(rc)))
+
+
+def _nao(numbers, method) -> int:
+    z = np.ascontiguousarray(np.asarray(numbers, dtype=np.int32).reshape(-1))
+    out = ctypes.c_int32()
+    rc = _abi.lib().am1gpu_basis_size(z.shape[0], z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                      _abi.METHOD[method.lower()], ctypes.byref(out))
+    _check(rc)
+    return out.value
+
+
+def _result_dict(rb: _abi.ResultBuffers, rc: int, want_matrices: bool) -> dict:
+    r = rb.res
+    d = {
+        "status": rc,
+        "energy_ev": r.total_ev,
+        "energy_hartree": r.total_ev * _abi.EV_TO_HARTREE,
+        "electronic_ev": r.electronic_ev,
+        "core_ev": r.core_ev,
+        "heat_of_formation_kcal": r.heat_of_formation_kcal,
+        "charges": rb.charges.copy(),
+        "dipole_debye": list(r.dipole_debye),
+        "dipole_magnitude": r.dipole_magnitude,
+        "homo_ev": r.homo_ev,
+        "lumo_ev": r.lumo_ev,
+        "homo_beta_ev": r.homo_beta_ev,
+        "lumo_beta_ev": r.lumo_beta_ev,
+        "residual": r.residual,
+        "nao": r.nao,
+        "n_occ": r.n_occ,
+        "n_occ_beta": r.n_occ_beta,
+        "iterations": r.iterations,
+        "converged": bool(r.converged),
+        "unrestricted": bool(r.unrestricted),
+        "mo_energies": rb.mo_energies.copy(),
+    }
+    if want_matrices:
+        d["density"] = rb.density.copy()
+        d["mo_coeff"] = rb.mo_coeff.copy()
+        if r.unrestricted:
+            d["spin_density"] = rb.spin_density.copy()
+            d["beta_energies"] = rb.beta_energies.copy()
+            d["beta_coeff"] = rb.beta_coeff.copy()
+    elif r.unrestricted and rb.beta_energies is not None:
+        d["beta_energies"] = rb.beta_energies.copy()
+    return d
+
+
+def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, raise_on_error=False, **opts) -> dict:
+    """One molecule through ``am1gpu_scf`` (the plain FP64 drop-in).  Positions in Bohr."""
+    mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
+    o = _abi.default_options(**opts)
+    method = opts.get("method", "am1")
+    nao = _nao(mb.z, method) if mb.z.size else 0
+    rb = _abi.ResultBuffers(mb.z.shape[0], nao, want_matrices)
+    rc = _abi.lib().am1gpu_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
+    if raise_on_error:
+        _check(rc, allow_not_converged=False)
+    d = _result_dict(rb, rc, want_matrices)
+    if rc:
+        d["error"] = _abi.lib().am1gpu_last_error().decode()
+    return d
+
+
+class Batch:
+    """Host buffers of one batched call; reusable across calls with the same molecules."""
+
+    def __init__(self, mols, method="am1", want_matrices=False):
+        self.mbs = [_abi.MolBuffers(*m) for m in mols]
+        self.arr = (_abi.Molecule * len(self.mbs))(*[m.mol for m in self.mbs])
+        self.rbs = [_abi.ResultBuffers(m.z.shape[0], _nao(m.z, method) if m.z.size else 0, want_matrices,
+                                       unrestricted=(m.mol.multiplicity > 1)) for m in self.mbs]
+        self.res = (_abi.Result * len(self.rbs))(*[r.res for r in self.rbs])
+        self.status = (ctypes.c_int32 * len(self.mbs))()
+        self.want_matrices = want_matrices
+
+    def run(self, **opts) -> int:
+        o = _abi.default_options(**opts)
+        return _abi.lib().am1gpu_scf_batch(len(self.mbs), self.arr, ctypes.byref(o), self.res, self.status)
+
+    def results(self) -> list[dict]:
+        out = []
+        for i, rb in enumerate(self.rbs):
+            rb.res = self.res[i]
+            out.append(_result_dict(rb, int(self.status[i]), self.want_matrices))
+        return out
+
+
+def scf_batch(mols, want_matrices=False, **opts):
+    """Batched solve.  ``mols``: sequence of (numbers, xyz_bohr, charge, multiplicity).
+    Returns (status list, result dicts)."""
+    b = Batch(mols, opts.get("method", "am1"), want_matrices)
+    b.run(**opts)
+    return list(b.status), b.results()
+
+
+def build_core(numbers, xyz_bohr, method="am1"):
+    mb = _abi.MolBuffers(numbers, xyz_bohr)
+    nao = _nao(mb.z, method)
+    h = np.zeros((nao, nao))
+    e = ctypes.c_double()
+    _check(_abi.lib().am1gpu_build_core(ctypes.byref(mb.mol), _abi.METHOD[method], h.ctypes.data_as(_dp), ctypes.byref(e)))
+    return h, e.value
+
+
+def build_fock(numbers, xyz_bohr, p_tot, p_spin, spin_scale, method="am1"):
+    mb = _abi.MolBuffers(numbers, xyz_bohr)
+    pt = np.ascontiguousarray(p_tot, dtype=np.float64)
+    ps = np.ascontiguousarray(p_spin, dtype=np.float64)
+    f = np.zeros_like(pt)
+    _check(_abi.lib().am1gpu_build_fock(ctypes.byref(mb.mol), _abi.METHOD[method], pt.ctypes.data_as(_dp),
+                                        ps.ctypes.data_as(_dp), float(spin_scale), f.ctypes.data_as(_dp)))
+    return f
+
+
+def eigh(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n))
+    _check(_abi.lib().am1gpu_symmetric_eigen(n, a.ctypes.data_as(_dp), w.ctypes.data_as(_dp), v.ctypes.data_as(_dp)))
+    return w, v
+
+
+# ---------------------------------------------------------------------------------------
+# The reference's Python entry points (positions in Angstrom)
+# ---------------------------------------------------------------------------------------
+def _prep(numbers, positions):
+    z = np.asarray(numbers, dtype=np.int32).reshape(-1)
+    xyz = _abi.angstrom_to_bohr(np.asarray(positions, dtype=float).reshape(len(z), 3))
+    return z, xyz
+
+
+def _reference_name(reference: str) -> str:
+    r = reference.strip().lower()
+    if r in ("auto", ""):
+        return "auto"
+    if r in ("rhf", "r", "restricted"):
+        return "rhf"
+    if r in ("uhf", "u", "unrestricted"):
+        return "uhf"
+    raise ValueError(f"invalid reference '{reference}': expected 'auto', 'rhf', or 'uhf'")
+
+
+def _method_name(method: str) -> str:
+    m = method.strip().lower()
+    if m not in _abi.METHOD:
+        raise ValueError(f"unknown method `{m}`; expected one of: am1, rm1")
+    return m
+
+
+def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+                 reference: str = "auto", method: str = "am1", electric_field=None) -> dict:
+    """Single-point energy and properties; the dictionary of am1_rs.native.single_point."""
+    if electric_field is not None:
+        raise ValueError("electric_field is not supported on the GPU path")
+    z, xyz = _prep(numbers, positions)
+    m = _method_name(method)
+    r = scf(z, xyz, charge, multiplicity, want_matrices=False, reference=_reference_name(reference), method=m)
+    _check(r["status"])
+    return {
+        "method": m,
+        "energy_hartree": r["energy_hartree"],
+        "energy_ev": r["energy_ev"],
+        "heat_of_formation_kcal": r["heat_of_formation_kcal"],
+        "electronic_ev": r["electronic_ev"],
+        "core_ev": r["core_ev"],
+        "charges": [float(x) for x in r["charges"]],
+        "dipole_debye": r["dipole_debye"],
+        "dipole_magnitude": r["dipole_magnitude"],
+        "homo_ev": None if np.isnan(r["homo_ev"]) else r["homo_ev"],
+        "lumo_ev": None if np.isnan(r["lumo_ev"]) else r["lumo_ev"],
+        "homo_beta_ev": None if np.isnan(r["homo_beta_ev"]) else r["homo_beta_ev"],
+        "lumo_beta_ev": None if np.isnan(r["lumo_beta_ev"]) else r["lumo_beta_ev"],
+        "field_nuclear_ev": 0.0,
+        "converged": r["converged"],
+        "iterations": r["iterations"],
+        "unrestricted": r["unrestricted"],
+    }
+
+
+def orbitals(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+             reference: str = "auto", method: str = "am1", electric_field=None) -> dict:
+    """Orbital energies and coefficients; the dictionary of am1_rs.native.orbitals."""
+    if electric_field is not None:
+        raise ValueError("electric_field is not supported on the GPU path")
+    z, xyz = _prep(numbers, positions)
+    m = _method_name(method)
+    r = scf(z, xyz, charge, multiplicity, want_matrices=True, reference=_reference_name(reference), method=m)
+    _check(r["status"])
+    labels = []
+    for ia, zz in enumerate(z):
+        labels += [(ia, "s")] if zz == 1 else [(ia, "s"), (ia, "px"), (ia, "py"), (ia, "pz")]
+    d = {
+        "energies_hartree": [e * _abi.EV_TO_HARTREE for e in r["mo_energies"]],
+        "energies_ev": list(r["mo_energies"]),
+        "coefficients": r["mo_coeff"].tolist(),
+        "n_occupied": r["n_occ"],
+        "homo_ev": None if np.isnan(r["homo_ev"]) else r["homo_ev"],
+        "lumo_ev": None if np.isnan(r["lumo_ev"]) else r["lumo_ev"],
+        "unrestricted": r["unrestricted"],
+        "ao_labels": labels,
+    }
+    if r["unrestricted"]:
+        d.update({
+            "beta_energies_hartree": [e * _abi.EV_TO_HARTREE for e in r["beta_energies"]],
+            "beta_energies_ev": list(r["beta_energies"]),
+            "beta_coefficients": r["beta_coeff"].tolist(),
+            "beta_n_occupied": r["n_occ_beta"],
+            "homo_beta_ev": None if np.isnan(r["homo_beta_ev"]) else r["homo_beta_ev"],
+            "lumo_beta_ev": None if np.isnan(r["lumo_beta_ev"]) else r["lumo_beta_ev"],
+        })
+    return d

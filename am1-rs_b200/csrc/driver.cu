@@ -1,0 +1,1000 @@
+// Host driver of libam1gpu: input validation (src/scf.rs:294-366), batch planning, the device
+// memory pool, the SCF iteration loop and the C ABI of include/am1gpu.h.
+//
+// A call solves any number of molecules at once.  All per-molecule work runs in batched kernels
+// (one launch per SCF phase for the whole batch); each molecule keeps its own trajectory and
+// convergence test and retires in place (MolState::active), so a molecule's result does not
+// depend on what else is in the batch.  The host only reads one integer (molecules still
+// active) every few iterations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/am1gpu.h"
+#include "am1gpu_internal.h"
+#include "kernels.h"
+
+namespace am1 {
+
+const DevElem* host_param_table();
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(AM1GPU_DEVICE_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+const char* kSymbols[] = {"X",  "H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al", "Si",
+                          "P",  "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe", "Co", "Ni", "Cu",
+                          "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",  "Zr", "Nb", "Mo", "Tc", "Ru",
+                          "Rh", "Pd", "Ag", "Cd", "In", "Sn", "Sb", "Te", "I",  "Xe", "Cs", "Ba", "La", "Ce", "Pr",
+                          "Nd", "Pm", "Sm", "Eu", "Gd", "Tb", "Dy", "Ho", "Er", "Tm", "Yb", "Lu", "Hf", "Ta", "W",
+                          "Re", "Os", "Ir", "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn"};
+
+inline const DevElem& helem(int method, int z) { return host_param_table()[method * (MAX_Z + 1) + z]; }
+
+// ---------------------------------------------------------------------------------------
+// Device context: parameter table uploaded once per device
+// ---------------------------------------------------------------------------------------
+struct DeviceCtx {
+    std::once_flag once;
+    int rc = AM1GPU_OK;
+    std::string err;
+    DevElem* d_params = nullptr;
+    int sms = 0;
+};
+
+DeviceCtx g_dev[64];
+
+int device_ctx(DeviceCtx** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(AM1GPU_DEVICE_ERROR, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return fail(AM1GPU_DEVICE_ERROR, "device index out of range");
+    DeviceCtx& c = g_dev[dev];
+    std::call_once(c.once, [&c, dev] {
+        auto bad = [&c](const char* what, cudaError_t err) {
+            c.rc = AM1GPU_DEVICE_ERROR;
+            c.err = std::string(what) + ": " + cudaGetErrorString(err);
+        };
+        cudaError_t err;
+        if ((err = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return bad("attr", err);
+        const size_t bytes = sizeof(DevElem) * 2 * (MAX_Z + 1);
+        if ((err = cudaMalloc(&c.d_params, bytes)) != cudaSuccess) return bad("cudaMalloc params", err);
+        if ((err = cudaMemcpy(c.d_params, host_param_table(), bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bad("upload params", err);
+        if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess)
+            return bad("jacobi smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+            return bad("jacobi cluster attribute", err);
+    });
+    if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
+    *out = &c;
+    return AM1GPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-host-thread workspace: stream, grow-only device pool and pinned staging
+// ---------------------------------------------------------------------------------------
+struct Workspace {
+    int dev = -1;
+    cudaStream_t stream = nullptr;
+    char* dpool = nullptr;
+    size_t dcap = 0;
+    char* hpin = nullptr;
+    size_t hcap = 0;
+    ~Workspace() {
+        // process exit: the driver frees everything with the context
+    }
+};
+
+thread_local Workspace tl_ws;
+
+int workspace(Workspace** out, size_t dbytes, size_t hbytes) {
+    Workspace& w = tl_ws;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (w.dev != dev) {  // first use on this device from this thread
+        w = Workspace();
+        w.dev = dev;
+        CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+    }
+    if (dbytes > w.dcap) {
+        if (w.dpool) CK(cudaFree(w.dpool));
+        w.dpool = nullptr;
+        w.dcap = 0;
+        CK(cudaMalloc(&w.dpool, dbytes));
+        w.dcap = dbytes;
+    }
+    if (hbytes > w.hcap) {
+        if (w.hpin) CK(cudaFreeHost(w.hpin));
+        w.hpin = nullptr;
+        w.hcap = 0;
+        CK(cudaMallocHost(&w.hpin, hbytes));
+        w.hcap = hbytes;
+    }
+    *out = &w;
+    return AM1GPU_OK;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// ---------------------------------------------------------------------------------------
+// Batch planning
+// ---------------------------------------------------------------------------------------
+struct MolPlan {
+    int user;          // index in the caller's array
+    int natoms, nheavy, nao, nch, n_occ[2], npad, cluster;
+    std::vector<int> order;  // internal atom -> caller atom
+    std::vector<int> ao_map; // internal AO -> caller AO
+};
+
+int choose_cluster(int n, int* npad_out, int* c_out) {
+    static const int cs[5] = {1, 2, 4, 8, 16};
+    for (int k = 0; k < 5; ++k) {
+        const int C = cs[k];
+        const int npad = ((std::max(n, 2) + 2 * C - 1) / (2 * C)) * (2 * C);
+        const int q = npad / 2 / C;
+        if (C > 1 && q < 2) continue;
+        if (jacobi_smem_bytes(n, npad, C) <= 232448 - 1024) {  // leave room for static shared memory
+            *npad_out = npad;
+            *c_out = C;
+            return 1;
+        }
+    }
+    return 0;
+}
+
+// Validates one molecule exactly as run_am1's head does (src/scf.rs:294-366) and plans it.
+int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, MolPlan& p) {
+    if (m.natoms < 0 || (m.natoms > 0 && (!m.z || !m.xyz_bohr))) return fail(AM1GPU_INVALID_INPUT, "null molecule arrays");
+    if (m.multiplicity < 1) return fail(AM1GPU_INVALID_INPUT, "multiplicity must be >= 1");
+    const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
+    for (int i = 0; i < m.natoms; ++i) {
+        const int z = m.z[i];
+        if (z < 0 || z > MAX_Z || !helem(method, z).present) {
+            std::string sup;
+            for (int k = 1; k <= MAX_Z; ++k)
+                if (helem(method, k).present) sup += (sup.empty() ? "" : ", ") + std::string(kSymbols[k]);
+            const char* name = method ? "RM1" : "AM1";
+            return fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, std::string(name) + " has no parameters for element Z=" +
+                                                              std::to_string(z) + "; " + name + " covers " + sup);
+        }
+        if (helem(method, z).n > 3)
+            return fail(AM1GPU_UNSUPPORTED, std::string("element ") + kSymbols[z] +
+                                                " has a valence shell n >= 4; its Slater overlap needs the numerical quadrature, "
+                                                "which this GPU path does not implement");
+        if (!std::isfinite(m.xyz_bohr[3 * i]) || !std::isfinite(m.xyz_bohr[3 * i + 1]) || !std::isfinite(m.xyz_bohr[3 * i + 2]))
+            return fail(AM1GPU_INVALID_INPUT, "non-finite coordinate for atom " + std::to_string(i));
+    }
+    double n_elec = 0.0;
+    for (int i = 0; i < m.natoms; ++i) n_elec += helem(method, m.z[i]).core_charge;
+    n_elec -= m.charge;
+    const long long ne = (long long)std::llround(n_elec);
+    if (std::fabs(n_elec - (double)ne) > 1.0e-6 || ne < 0)
+        return fail(AM1GPU_INVALID_INPUT, "invalid electron count " + std::to_string(n_elec));
+    const long long unp = m.multiplicity - 1;
+    if ((ne - unp) < 0 || (ne - unp) % 2 != 0)
+        return fail(AM1GPU_INVALID_INPUT, "electron count " + std::to_string(ne) + " is incompatible with multiplicity " +
+                                              std::to_string(m.multiplicity) + " (need same parity)");
+    const int n_alpha = (int)((ne + unp) / 2), n_beta = (int)((ne - unp) / 2);
+    const bool closed = n_alpha == n_beta;
+    bool uhf;
+    if (o.reference == AM1GPU_REF_AUTO) uhf = !closed;
+    else if (o.reference == AM1GPU_REF_UHF) uhf = true;
+    else {
+        if (!closed)
+            return fail(AM1GPU_INVALID_INPUT, "restricted (RHF) reference requires a closed shell, but multiplicity " +
+                                                  std::to_string(m.multiplicity) + " gives " + std::to_string(n_alpha) +
+                                                  " alpha and " + std::to_string(n_beta) +
+                                                  " beta electrons; use the unrestricted (UHF) reference for open-shell systems");
+        uhf = false;
+    }
+    p.user = user;
+    p.natoms = m.natoms;
+    p.nch = uhf ? 2 : 1;
+    p.n_occ[0] = n_alpha;
+    p.n_occ[1] = uhf ? n_beta : n_alpha;
+    p.order.clear();
+    for (int i = 0; i < m.natoms; ++i)
+        if (helem(method, m.z[i]).norb == 4) p.order.push_back(i);
+    p.nheavy = (int)p.order.size();
+    for (int i = 0; i < m.natoms; ++i)
+        if (helem(method, m.z[i]).norb != 4) p.order.push_back(i);
+    p.nao = 4 * p.nheavy + (m.natoms - p.nheavy);
+    // caller AO offsets
+    std::vector<int> uoff(m.natoms);
+    int acc = 0;
+    for (int i = 0; i < m.natoms; ++i) {
+        uoff[i] = acc;
+        acc += helem(method, m.z[i]).norb;
+    }
+    p.ao_map.assign(p.nao, 0);
+    int k = 0;
+    for (int ia = 0; ia < m.natoms; ++ia) {
+        const int u = p.order[ia];
+        const int no = helem(method, m.z[u]).norb;
+        for (int t = 0; t < no; ++t) p.ao_map[k++] = uoff[u] + t;
+    }
+    if (!choose_cluster(p.nao, &p.npad, &p.cluster))
+        return fail(AM1GPU_UNSUPPORTED, "molecule with " + std::to_string(p.nao) +
+                                            " orbitals exceeds the cluster eigensolver's shared-memory capacity (448)");
+    return AM1GPU_OK;
+}
+
+struct Batch {
+    int nmol = 0, natoms = 0, nblk = 1, maxn = 0;
+    long long npairs = 0;
+    std::vector<MolPlan> plans;
+    // device pointers (into the pool)
+    MolDesc* d_mols;
+    int *d_atom_z, *d_atom_mol;
+    double* d_atom_xyz;
+    long long* d_pair_prefix;
+    ChanJob* d_jobs;
+    int* d_job0;
+    GemmJob *d_gj_fp, *d_gj_gt, *d_gj_dn;
+    GemmTile *d_gt_fp, *d_gt_gt, *d_gt_dn;
+    int nt_fp = 0, nt_gt = 0, nt_dn = 0;
+    EigJob* d_eig;
+    int neig = 0;
+    struct Bucket { int off, count, C; size_t smem; };
+    std::vector<Bucket> buckets;
+    MolState* d_st;
+    int* d_status;
+    double *d_wstore, *d_ecc, *d_arena, *d_res, *d_charges;
+    int* d_active;
+    // host mirrors needed for output
+    std::vector<MolDesc> mols;
+    std::vector<ChanJob> jobs;
+    std::vector<int> job0;
+    int* h_active;
+    double* h_res;
+    double* h_charges;
+};
+
+// Lays out the batch in one device pool and one pinned staging area, copies inputs.
+int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<MolPlan>&& plans, Batch& b, Workspace** wsp,
+                double spin_scale_override = -1.0) {
+    b.plans = std::move(plans);
+    b.nmol = (int)b.plans.size();
+    const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
+    const bool adiis = o.use_diis && o.accelerator == AM1GPU_ACCEL_ADIIS_CDIIS;
+    // sizes
+    long long natoms = 0, npairs = 0, wsize = 0, arena = 0, hist = 0, nch_total = 0;
+    int maxn = 0;
+    for (auto& p : b.plans) {
+        natoms += p.natoms;
+        npairs += (long long)p.natoms * (p.natoms - 1) / 2;
+        const long long h = p.nheavy, H = p.natoms - p.nheavy;
+        wsize += 100 * h * (h - 1) / 2 + 10 * h * H + H * (H - 1) / 2;
+        const long long nn = (long long)p.nao * p.nao;
+        arena += nn + p.nch * (5 * nn + (long long)p.npad * p.nao) + 64;
+        const long long ls = packed_sym_len(p.nao), la = packed_anti_len(p.nao);
+        hist += p.nch * MAX_DIIS * (ls + la + ((adiis && p.nch == 1) ? ls : 0)) + 64;
+        nch_total += p.nch;
+        maxn = std::max(maxn, p.nao);
+    }
+    b.natoms = (int)natoms;
+    b.npairs = npairs;
+    b.maxn = maxn;
+    b.nblk = std::max(1, std::min(32, (maxn + 15) / 16));
+    const int nblk = b.nblk;
+    // GEMM tile counts
+    int tiles_nn = 0;
+    for (auto& p : b.plans) tiles_nn += p.nch * ((p.nao + 63) / 64) * ((p.nao + 63) / 64);
+    // ---- staged (host -> device) region layout
+    size_t st = 0;
+    auto take = [](size_t& cur, size_t bytes) {
+        cur = align256(cur);
+        const size_t o2 = cur;
+        cur += bytes;
+        return o2;
+    };
+    const size_t o_mols = take(st, sizeof(MolDesc) * b.nmol);
+    const size_t o_z = take(st, sizeof(int) * natoms);
+    const size_t o_am = take(st, sizeof(int) * natoms);
+    const size_t o_xyz = take(st, sizeof(double) * 3 * natoms);
+    const size_t o_pp = take(st, sizeof(long long) * (b.nmol + 1));
+    const size_t o_jobs = take(st, sizeof(ChanJob) * nch_total);
+    const size_t o_job0 = take(st, sizeof(int) * b.nmol);
+    const size_t o_gfp = take(st, sizeof(GemmJob) * nch_total);
+    const size_t o_ggt = take(st, sizeof(GemmJob) * nch_total);
+    const size_t o_gdn = take(st, sizeof(GemmJob) * nch_total);
+    const size_t o_tfp = take(st, sizeof(GemmTile) * tiles_nn);
+    const size_t o_tgt = take(st, sizeof(GemmTile) * tiles_nn);
+    const size_t o_tdn = take(st, sizeof(GemmTile) * tiles_nn);
+    const size_t o_eig = take(st, sizeof(EigJob) * nch_total);
+    const size_t o_st = take(st, sizeof(MolState) * b.nmol);
+    const size_t staged = align256(st);
+    // ---- device-only region
+    size_t dv = staged;
+    const size_t o_status = take(dv, sizeof(int) * b.nmol);
+    const size_t o_active = take(dv, sizeof(int) * 4);
+    const size_t o_w = take(dv, sizeof(double) * std::max<long long>(wsize, 1));
+    const size_t o_ecc = take(dv, sizeof(double) * std::max<long long>(npairs, 1));
+    const size_t o_arena = take(dv, sizeof(double) * arena);
+    const size_t o_hist = take(dv, sizeof(double) * hist);
+    long long misc = 0;
+    for (auto& p : b.plans) misc += p.nch * (2LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + 64);
+    const size_t o_misc = take(dv, sizeof(double) * misc);
+    const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
+    const size_t o_res = take(dv, sizeof(double) * RES_N * b.nmol);
+    const size_t o_chg = take(dv, sizeof(double) * std::max<long long>(natoms, 1));
+    const size_t dtotal = align256(dv);
+    // pinned staging also receives the outputs
+    size_t hs = staged;
+    const size_t h_o_active = take(hs, sizeof(int) * 4);
+    const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
+    const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
+    Workspace* ws;
+    int rc = workspace(&ws, dtotal, align256(hs));
+    if (rc) return rc;
+    *wsp = ws;
+    char* D = ws->dpool;
+    char* Hs = ws->hpin;
+    auto dptr = [D](size_t off) { return (void*)(D + off); };
+    b.d_mols = (MolDesc*)dptr(o_mols);
+    b.d_atom_z = (int*)dptr(o_z);
+    b.d_atom_mol = (int*)dptr(o_am);
+    b.d_atom_xyz = (double*)dptr(o_xyz);
+    b.d_pair_prefix = (long long*)dptr(o_pp);
+    b.d_jobs = (ChanJob*)dptr(o_jobs);
+    b.d_job0 = (int*)dptr(o_job0);
+    b.d_gj_fp = (GemmJob*)dptr(o_gfp);
+    b.d_gj_gt = (GemmJob*)dptr(o_ggt);
+    b.d_gj_dn = (GemmJob*)dptr(o_gdn);
+    b.d_gt_fp = (GemmTile*)dptr(o_tfp);
+    b.d_gt_gt = (GemmTile*)dptr(o_tgt);
+    b.d_gt_dn = (GemmTile*)dptr(o_tdn);
+    b.d_eig = (EigJob*)dptr(o_eig);
+    b.d_st = (MolState*)dptr(o_st);
+    b.d_status = (int*)dptr(o_status);
+    b.d_active = (int*)dptr(o_active);
+    b.d_wstore = (double*)dptr(o_w);
+    b.d_ecc = (double*)dptr(o_ecc);
+    b.d_arena = (double*)dptr(o_arena);
+    double* d_hist = (double*)dptr(o_hist);
+    double* d_misc = (double*)dptr(o_misc);
+    int* d_colid = (int*)dptr(o_colid);
+    b.d_res = (double*)dptr(o_res);
+    b.d_charges = (double*)dptr(o_chg);
+    b.h_active = (int*)(Hs + h_o_active);
+    b.h_res = (double*)(Hs + h_o_res);
+    b.h_charges = (double*)(Hs + h_o_chg);
+    // ---- fill the staged region
+    MolDesc* hm = (MolDesc*)(Hs + o_mols);
+    int* hz = (int*)(Hs + o_z);
+    int* ham = (int*)(Hs + o_am);
+    double* hxyz = (double*)(Hs + o_xyz);
+    long long* hpp = (long long*)(Hs + o_pp);
+    ChanJob* hj = (ChanJob*)(Hs + o_jobs);
+    int* hj0 = (int*)(Hs + o_job0);
+    GemmJob* hgfp = (GemmJob*)(Hs + o_gfp);
+    GemmJob* hggt = (GemmJob*)(Hs + o_ggt);
+    GemmJob* hgdn = (GemmJob*)(Hs + o_gdn);
+    GemmTile* htfp = (GemmTile*)(Hs + o_tfp);
+    GemmTile* htgt = (GemmTile*)(Hs + o_tgt);
+    GemmTile* htdn = (GemmTile*)(Hs + o_tdn);
+    EigJob* heig = (EigJob*)(Hs + o_eig);
+    MolState* hst = (MolState*)(Hs + o_st);
+    long long a_off = 0, w_off = 0, ar_off = 0, hi_off = 0, mi_off = 0;
+    int atom_base = 0, job = 0, ntile = 0, cid_off = 0;
+    std::vector<EigJob> eig_all;
+    std::vector<int> eig_cluster;
+    for (int mi = 0; mi < b.nmol; ++mi) {
+        MolPlan& p = b.plans[mi];
+        const am1gpu_molecule& m = in[p.user];
+        MolDesc md{};
+        md.natoms = p.natoms;
+        md.nheavy = p.nheavy;
+        md.nao = p.nao;
+        md.nch = p.nch;
+        md.n_occ[0] = p.n_occ[0];
+        md.n_occ[1] = p.n_occ[1];
+        md.method = method;
+        md.atom_base = atom_base;
+        md.pair_base = a_off;
+        md.w_base = w_off;
+        md.spin_scale = p.nch == 2 ? 1.0 : 0.5;
+        md.occ_weight = p.nch == 2 ? 1.0 : 2.0;
+        if (spin_scale_override >= 0.0) md.spin_scale = spin_scale_override;
+        const long long n = p.nao, nn = n * n;
+        md.h_base = ar_off;
+        long long cur = ar_off + nn;
+        for (int c = 0; c < p.nch; ++c) {
+            md.ch_base[c] = cur;
+            cur += 5 * nn + (long long)p.npad * n;
+        }
+        ar_off = (cur + 31) & ~31LL;
+        for (int ia = 0; ia < p.natoms; ++ia) {
+            const int u = p.order[ia];
+            hz[atom_base + ia] = m.z[u];
+            ham[atom_base + ia] = mi;
+            for (int k = 0; k < 3; ++k) hxyz[3 * (atom_base + ia) + k] = m.xyz_bohr[3 * u + k];
+        }
+        hpp[mi] = a_off;
+        const long long h = p.nheavy, H = p.natoms - p.nheavy;
+        a_off += (long long)p.natoms * (p.natoms - 1) / 2;
+        w_off += 100 * h * (h - 1) / 2 + 10 * h * H + H * (H - 1) / 2;
+        atom_base += p.natoms;
+        hj0[mi] = job;
+        const long long ls = packed_sym_len((int)n), la = packed_anti_len((int)n);
+        for (int c = 0; c < p.nch; ++c) {
+            double* base = b.d_arena + md.ch_base[c];
+            ChanJob cj{};
+            cj.mol = mi;
+            cj.ch = c;
+            cj.n = (int)n;
+            cj.F = base + SLOT_F * nn;
+            cj.FP = base + SLOT_FP * nn;
+            cj.P = base + SLOT_P * nn;
+            cj.Ct = base + SLOT_CT * nn;
+            cj.Pnew = base + SLOT_GT * nn;
+            cj.H = b.d_arena + md.h_base;
+            md.pk_base[c] = hi_off;
+            cj.hF = d_hist + hi_off;
+            hi_off += MAX_DIIS * ls;
+            cj.hE = d_hist + hi_off;
+            hi_off += MAX_DIIS * la;
+            cj.hD = nullptr;
+            if (adiis && p.nch == 1) {
+                cj.hD = d_hist + hi_off;
+                hi_off += MAX_DIIS * ls;
+            }
+            hi_off = (hi_off + 31) & ~31LL;
+            cj.rowmin = d_misc + mi_off;
+            mi_off += n;
+            cj.eps = d_misc + mi_off;
+            mi_off += n;
+            double* lam = d_misc + mi_off;
+            mi_off += p.npad;
+            cj.red = d_misc + mi_off;
+            mi_off += (long long)nblk * RED_N;
+            cj.red2 = d_misc + mi_off;
+            mi_off += nblk;
+            mi_off = (mi_off + 31) & ~31LL;
+            hj[job] = cj;
+            // GEMMs: F.P, C^T F*, w C_occ^T C_occ
+            hgfp[job] = GemmJob{cj.F, cj.P, cj.FP, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
+            hggt[job] = GemmJob{cj.Ct, cj.FP, base + SLOT_GT * nn, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
+            hgdn[job] = GemmJob{cj.Ct, cj.Ct, cj.Pnew, (int)n, (int)n, p.n_occ[c], (int)n, (int)n, (int)n, md.occ_weight, mi};
+            const int tn = (int)((n + 63) / 64);
+            for (int x = 0; x < tn; ++x)
+                for (int y = 0; y < tn; ++y) {
+                    htfp[ntile] = GemmTile{job, x, y};
+                    htgt[ntile] = GemmTile{job, x, y};
+                    htdn[ntile] = GemmTile{job, x, y};
+                    ++ntile;
+                }
+            EigJob ej{};
+            ej.Gt = base + SLOT_GT * nn;
+            ej.Ct = cj.Ct;
+            ej.Vs = base + SLOT_VS * nn;
+            ej.lam = lam;
+            ej.colid_out = d_colid + cid_off;
+            cid_off += p.npad + 32;
+            ej.eps = cj.eps;
+            ej.Ct_out = cj.Ct;
+            ej.rowmin = cj.rowmin;
+            ej.sweeps_out = nullptr;
+            ej.n = (int)n;
+            ej.npad = p.npad;
+            ej.mol = mi;
+            eig_all.push_back(ej);
+            eig_cluster.push_back(p.cluster);
+            ++job;
+        }
+        hm[mi] = md;
+        MolState s{};
+        s.active = 1;
+        s.e_old = 0.0;
+        s.residual = INFINITY;
+        hst[mi] = s;
+    }
+    hpp[b.nmol] = a_off;
+    b.nt_fp = b.nt_gt = b.nt_dn = ntile;
+    // eigen jobs grouped by cluster size, largest first inside a group
+    std::vector<int> idx(eig_all.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+        if (eig_cluster[x] != eig_cluster[y]) return eig_cluster[x] > eig_cluster[y];
+        return eig_all[x].n > eig_all[y].n;
+    });
+    b.buckets.clear();
+    for (size_t i = 0; i < idx.size(); ++i) {
+        heig[i] = eig_all[idx[i]];
+        const int C = eig_cluster[idx[i]];
+        const size_t sm = jacobi_smem_bytes(eig_all[idx[i]].n, eig_all[idx[i]].npad, C);
+        if (b.buckets.empty() || b.buckets.back().C != C) b.buckets.push_back({(int)i, 0, C, 0});
+        b.buckets.back().count++;
+        b.buckets.back().smem = std::max(b.buckets.back().smem, sm);
+    }
+    b.neig = (int)idx.size();
+    b.mols.assign(hm, hm + b.nmol);
+    b.jobs.assign(hj, hj + job);
+    b.job0.assign(hj0, hj0 + b.nmol);
+    CK(cudaMemcpyAsync(D, Hs, staged, cudaMemcpyHostToDevice, ws->stream));
+    CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, ws->stream));
+    CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * arena, ws->stream));
+    return AM1GPU_OK;
+}
+
+inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+int launch_core(Batch& b, Workspace* ws, const DevElem* dp) {
+    cudaStream_t s = ws->stream;
+    if (b.npairs > 0)
+        k_pair_integrals<<<cdiv(b.npairs, 128), 128, 0, s>>>(b.d_mols, b.nmol, b.d_pair_prefix, b.npairs, dp, b.d_atom_z,
+                                                            b.d_atom_xyz, b.d_wstore, b.d_arena, b.d_ecc, b.d_status);
+    if (b.natoms > 0)
+        k_core_diag<<<cdiv(b.natoms, 128), 128, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena);
+    k_core_energy<<<b.nmol, 256, 0, s>>>(b.d_mols, b.d_ecc, b.d_st);
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+int launch_jacobi(Batch& b, Workspace* ws, int force) {
+    for (auto& bk : b.buckets) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(bk.count * bk.C, 1, 1);
+        cfg.blockDim = dim3(256, 1, 1);
+        cfg.dynamicSmemBytes = bk.smem;
+        cfg.stream = ws->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = bk.C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_jacobi, (const EigJob*)(b.d_eig + bk.off), (const MolState*)b.d_st, b.d_status, force));
+    }
+    return AM1GPU_OK;
+}
+
+int run_scf(Batch& b, Workspace* ws, const DevElem* dp, const am1gpu_options& o) {
+    cudaStream_t s = ws->stream;
+    int rc = launch_core(b, ws, dp);
+    if (rc) return rc;
+    const int njobs = (int)b.jobs.size();
+    if (b.natoms > 0) k_sad_init<<<cdiv(b.natoms, 128), 128, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_arena);
+    k_identity<<<dim3(cdiv(b.maxn, 256), njobs), 256, 0, s>>>(b.d_jobs);
+    CK(cudaGetLastError());
+    ScfParams prm{o.max_scf, o.use_diis, o.accelerator, o.e_tol, o.p_tol, o.adiis_switch};
+    const int nblk = b.nblk;
+    const int rowblk = std::max(1, std::min(64, (b.maxn + 7) / 8));
+    int done = 0;
+    const int check = b.nmol > 64 ? 4 : 1;
+    while (done < o.max_scf) {
+        for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
+            CK(cudaMemsetAsync(b.d_active, 0, sizeof(int), s));
+            k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena,
+                                                      b.d_st, 0);
+            k_gemm_nn<<<b.nt_fp, 256, 0, s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0);
+            k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
+            k_diis_solve<<<cdiv(b.nmol, 64), 64, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm);
+            k_combine<<<dim3(rowblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, 0);
+            k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0);
+            CK(cudaGetLastError());
+            rc = launch_jacobi(b, ws, 0);
+            if (rc) return rc;
+            k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0);
+            k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0);
+            k_density_post<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, nblk);
+            k_converge<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm,
+                                                         b.d_active);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpyAsync(b.h_active, b.d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (*b.h_active == 0) break;
+    }
+    // final energy at the final density (src/scf.rs:698-701, 835-839)
+    k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena, b.d_st, 1);
+    k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 1, 1);
+    k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
+    k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
+                                                 b.d_atom_xyz, b.d_res, b.d_charges);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(b.h_res, b.d_res, sizeof(double) * RES_N * b.nmol, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(b.h_charges, b.d_charges, sizeof(double) * std::max(b.natoms, 1), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return AM1GPU_OK;
+}
+
+// Copies one device matrix (internal AO order) out to the caller's order.
+int fetch_matrix(Workspace* ws, const double* dsrc, int n, std::vector<double>& tmp) {
+    tmp.resize((size_t)n * n);
+    CK(cudaMemcpyAsync(tmp.data(), dsrc, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaStreamSynchronize(ws->stream));
+    return AM1GPU_OK;
+}
+
+int write_result(Batch& b, Workspace* ws, int mi, am1gpu_result* r) {
+    const MolPlan& p = b.plans[mi];
+    const double* rec = b.h_res + (size_t)mi * RES_N;
+    r->electronic_ev = rec[RES_ELEC];
+    r->core_ev = rec[RES_CORE];
+    r->total_ev = rec[RES_TOTAL];
+    r->heat_of_formation_kcal = rec[RES_HOF];
+    for (int k = 0; k < 3; ++k) r->dipole_debye[k] = rec[RES_DIP + k];
+    r->dipole_magnitude = rec[RES_DIPMAG];
+    r->homo_ev = rec[RES_HOMO];
+    r->lumo_ev = rec[RES_LUMO];
+    r->homo_beta_ev = rec[RES_HOMO_B];
+    r->lumo_beta_ev = rec[RES_LUMO_B];
+    r->residual = rec[RES_RESID];
+    r->nao = p.nao;
+    r->n_occ = p.n_occ[0];
+    r->n_occ_beta = p.n_occ[1];
+    r->iterations = (int)rec[RES_ITER];
+    r->converged = (int)rec[RES_CONV];
+    r->unrestricted = p.nch == 2 ? 1 : 0;
+    const MolDesc& md = b.mols[mi];
+    if (r->charges)
+        for (int ia = 0; ia < p.natoms; ++ia) r->charges[p.order[ia]] = b.h_charges[md.atom_base + ia];
+    const int n = p.nao;
+    const auto& map = p.ao_map;
+    std::vector<double> t0, t1;
+    const ChanJob& j0 = b.jobs[b.job0[mi]];
+    if (r->density || r->spin_density) {
+        int rc = fetch_matrix(ws, j0.P, n, t0);
+        if (rc) return rc;
+        if (p.nch == 2) {
+            rc = fetch_matrix(ws, b.jobs[b.job0[mi] + 1].P, n, t1);
+            if (rc) return rc;
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const size_t s = (size_t)i * n + j, d = (size_t)map[i] * n + map[j];
+                if (r->density) r->density[d] = p.nch == 2 ? t0[s] + t1[s] : t0[s];
+                if (r->spin_density && p.nch == 2) r->spin_density[d] = t0[s] - t1[s];
+            }
+    }
+    for (int c = 0; c < p.nch; ++c) {
+        double* e_out = c == 0 ? r->mo_energies : r->beta_energies;
+        double* c_out = c == 0 ? r->mo_coeff : r->beta_coeff;
+        const ChanJob& jc = b.jobs[b.job0[mi] + c];
+        if (e_out) {
+            CK(cudaMemcpyAsync(e_out, jc.eps, sizeof(double) * n, cudaMemcpyDeviceToHost, ws->stream));
+            CK(cudaStreamSynchronize(ws->stream));
+        }
+        if (c_out) {
+            int rc = fetch_matrix(ws, jc.Ct, n, t0);
+            if (rc) return rc;
+            for (int k = 0; k < n; ++k)
+                for (int mu = 0; mu < n; ++mu) c_out[(size_t)map[mu] * n + k] = t0[(size_t)k * n + mu];
+        }
+    }
+    const int status = (int)rec[RES_STATUS];
+    if (status == AM1GPU_SCF_DIVERGED)
+        return fail(AM1GPU_SCF_DIVERGED, "the AM1 SCF diverged at iteration " + std::to_string(r->iterations) +
+                                             ": a non-finite energy or density appeared");
+    if (status == AM1GPU_LINALG) return fail(AM1GPU_LINALG, "the eigensolver refused a non-finite or unconverged matrix");
+    if (status == AM1GPU_UNSUPPORTED) return fail(AM1GPU_UNSUPPORTED, "overlap not covered for an element of this molecule");
+    if (!r->converged) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "AM1 SCF did not converge after %d iterations (error=%.3e)", r->iterations, r->residual);
+        return fail(AM1GPU_SCF_NOT_CONVERGED, buf);
+    }
+    return AM1GPU_OK;
+}
+
+void fill_empty(am1gpu_result* r) {
+    // a molecule with no atoms: nothing to solve (run_am1 converges at its second iteration)
+    r->electronic_ev = r->core_ev = r->total_ev = r->heat_of_formation_kcal = 0.0;
+    r->dipole_debye[0] = r->dipole_debye[1] = r->dipole_debye[2] = r->dipole_magnitude = 0.0;
+    r->homo_ev = r->lumo_ev = r->homo_beta_ev = r->lumo_beta_ev = NAN;
+    r->residual = 0.0;
+    r->nao = r->n_occ = r->n_occ_beta = 0;
+    r->iterations = 2;
+    r->converged = 1;
+    r->unrestricted = 0;
+}
+
+}  // namespace
+
+int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* res, int* status) {
+    g_err.clear();
+    if (nmol < 0 || (nmol > 0 && (!mols || !res)) || !opts) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) {
+        for (int i = 0; i < nmol; ++i)
+            if (status) status[i] = rc;
+        return rc;
+    }
+    std::vector<MolPlan> plans;
+    int first = AM1GPU_OK;
+    std::string first_msg;
+    for (int i = 0; i < nmol; ++i) {
+        MolPlan p;
+        int r = AM1GPU_OK;
+        if (mols[i].natoms == 0 && mols[i].multiplicity >= 1 && std::fabs(mols[i].charge) < 1e-6) {
+            fill_empty(&res[i]);
+        } else {
+            r = plan_molecule(mols[i], *opts, i, p);
+            if (r == AM1GPU_OK) plans.push_back(std::move(p));
+        }
+        if (status) status[i] = r;
+        if (r && !first) {
+            first = r;
+            first_msg = g_err;
+        }
+    }
+    if (!plans.empty()) {
+        Batch b;
+        Workspace* ws;
+        rc = build_batch(mols, *opts, std::move(plans), b, &ws);
+        if (!rc) rc = run_scf(b, ws, ctx->d_params, *opts);
+        if (rc) {
+            for (auto& p : b.plans)
+                if (status) status[p.user] = rc;
+            return rc;
+        }
+        for (int mi = 0; mi < b.nmol; ++mi) {
+            const int u = b.plans[mi].user;
+            int r = write_result(b, ws, mi, &res[u]);
+            if (status) status[u] = r;
+            if (r && !first) {
+                first = r;
+                first_msg = g_err;
+            }
+        }
+    }
+    if (first) g_err = first_msg;
+    return first;
+}
+
+int build_core_one(const am1gpu_molecule* mol, int method, double* h_core, double* core_ev) {
+    g_err.clear();
+    if (!mol) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    am1gpu_options o;
+    am1gpu_default_options(&o);
+    o.method = method;
+    o.reference = AM1GPU_REF_UHF;  // geometry only; the spin choice does not matter here
+    am1gpu_molecule m = *mol;
+    MolPlan p;
+    // the electron count is irrelevant for H_core: validate elements with a neutral closed shell
+    m.multiplicity = 1;
+    m.charge = 0.0;
+    double ne = 0.0;
+    for (int i = 0; i < m.natoms; ++i)
+        if (m.z[i] >= 0 && m.z[i] <= MAX_Z) ne += helem(method == 1, m.z[i]).core_charge;
+    if (((long long)std::llround(ne)) % 2) m.multiplicity = 2;
+    rc = plan_molecule(m, o, 0, p);
+    if (rc) return rc;
+    std::vector<MolPlan> plans{std::move(p)};
+    Batch b;
+    Workspace* ws;
+    rc = build_batch(&m, o, std::move(plans), b, &ws);
+    if (rc) return rc;
+    rc = launch_core(b, ws, ctx->d_params);
+    if (rc) return rc;
+    MolState st;
+    CK(cudaMemcpyAsync(&st, b.d_st, sizeof(MolState), cudaMemcpyDeviceToHost, ws->stream));
+    std::vector<double> t;
+    rc = fetch_matrix(ws, b.d_arena + b.mols[0].h_base, b.plans[0].nao, t);
+    if (rc) return rc;
+    const int n = b.plans[0].nao;
+    const auto& map = b.plans[0].ao_map;
+    if (h_core)
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) h_core[(size_t)map[i] * n + map[j]] = t[(size_t)i * n + j];
+    if (core_ev) *core_ev = st.core_ev;
+    return AM1GPU_OK;
+}
+
+int build_fock_one(const am1gpu_molecule* mol, int method, const double* p_tot, const double* p_spin, double spin_scale,
+                   double* fock) {
+    g_err.clear();
+    if (!mol || !p_tot || !p_spin || !fock) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    am1gpu_options o;
+    am1gpu_default_options(&o);
+    o.method = method;
+    o.reference = AM1GPU_REF_UHF;  // two density slots: P0 = p_spin, P1 = p_tot - p_spin
+    am1gpu_molecule m = *mol;
+    m.charge = 0.0;
+    double ne = 0.0;
+    for (int i = 0; i < m.natoms; ++i)
+        if (m.z[i] >= 0 && m.z[i] <= MAX_Z) ne += helem(method == 1, m.z[i]).core_charge;
+    m.multiplicity = ((long long)std::llround(ne)) % 2 ? 2 : 1;
+    MolPlan p;
+    rc = plan_molecule(m, o, 0, p);
+    if (rc) return rc;
+    std::vector<MolPlan> plans{std::move(p)};
+    Batch b;
+    Workspace* ws;
+    rc = build_batch(&m, o, std::move(plans), b, &ws, spin_scale);
+    if (rc) return rc;
+    rc = launch_core(b, ws, ctx->d_params);
+    if (rc) return rc;
+    const int n = b.plans[0].nao;
+    const auto& map = b.plans[0].ao_map;
+    std::vector<double> p0((size_t)n * n), p1((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const size_t u = (size_t)map[i] * n + map[j];
+            p0[(size_t)i * n + j] = p_spin[u];
+            p1[(size_t)i * n + j] = p_tot[u] - p_spin[u];
+        }
+    CK(cudaMemcpyAsync(b.jobs[0].P, p0.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, ws->stream));
+    CK(cudaMemcpyAsync(b.jobs[1].P, p1.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, ws->stream));
+    k_fock<<<cdiv(b.natoms, 8), 256, 0, ws->stream>>>(b.d_mols, b.d_atom_mol, b.natoms, ctx->d_params, b.d_atom_z, b.d_wstore,
+                                                      b.d_arena, b.d_st, 1);
+    CK(cudaGetLastError());
+    std::vector<double> t;
+    rc = fetch_matrix(ws, b.jobs[0].F, n, t);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) fock[(size_t)map[i] * n + map[j]] = t[(size_t)i * n + j];
+    return AM1GPU_OK;
+}
+
+int symmetric_eigen_one(int n, const double* a, double* w, double* v) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && (!a || !w || !v))) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (n == 0) return AM1GPU_OK;
+    for (long long i = 0; i < (long long)n * n; ++i)
+        if (!std::isfinite(a[i])) {
+            return fail(AM1GPU_LINALG, "the " + std::to_string(n) + "x" + std::to_string(n) +
+                                           " matrix handed to the eigensolver is not finite: element (" + std::to_string(i / n) +
+                                           ", " + std::to_string(i % n) + ")");
+        }
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    int npad, C;
+    if (!choose_cluster(n, &npad, &C))
+        return fail(AM1GPU_UNSUPPORTED, "matrix larger than the cluster eigensolver's shared-memory capacity");
+    // layout: Gt (n*n, the lower triangle mirrored), Ct (n*n identity), Vs (npad*n), lam, colid, eps, rowmin, state
+    const size_t nn = (size_t)n * n;
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        off = align256(off);
+        const size_t o2 = off;
+        off += bytes;
+        return o2;
+    };
+    const size_t o_g = take(nn * 8), o_c = take(nn * 8), o_v = take((size_t)npad * n * 8), o_l = take(npad * 8),
+                 o_id = take(npad * 4), o_e = take(n * 8), o_r = take(n * 8), o_st = take(sizeof(MolState)),
+                 o_status = take(16), o_job = take(sizeof(EigJob));
+    Workspace* ws;
+    rc = workspace(&ws, align256(off), align256(off));
+    if (rc) return rc;
+    char* D = ws->dpool;
+    char* Hh = ws->hpin;
+    double* g = (double*)(Hh + o_g);
+    double* c = (double*)(Hh + o_c);
+    double* rmin = (double*)(Hh + o_r);
+    for (int i = 0; i < n; ++i) {
+        double bound = 0.0;
+        for (int j = 0; j < n; ++j) {
+            const double x = i >= j ? a[(size_t)i * n + j] : a[(size_t)j * n + i];  // lower triangle
+            g[(size_t)i * n + j] = x;
+            c[(size_t)i * n + j] = i == j ? 1.0 : 0.0;
+            if (i != j) bound += std::fabs(x);
+        }
+        rmin[i] = g[(size_t)i * n + i] - bound;
+    }
+    MolState* hs = (MolState*)(Hh + o_st);
+    *hs = MolState{};
+    hs->active = 1;
+    EigJob* ej = (EigJob*)(Hh + o_job);
+    *ej = EigJob{};
+    ej->Gt = (double*)(D + o_g);
+    ej->Ct = (double*)(D + o_c);
+    ej->Vs = (double*)(D + o_v);
+    ej->lam = (double*)(D + o_l);
+    ej->colid_out = (int*)(D + o_id);
+    ej->eps = (double*)(D + o_e);
+    ej->Ct_out = (double*)(D + o_c);
+    ej->rowmin = (double*)(D + o_r);
+    ej->n = n;
+    ej->npad = npad;
+    ej->mol = 0;
+    std::memset(Hh + o_status, 0, 16);
+    CK(cudaMemcpyAsync(D, Hh, align256(off), cudaMemcpyHostToDevice, ws->stream));
+    Batch b;
+    b.d_eig = (EigJob*)(D + o_job);
+    b.d_st = (MolState*)(D + o_st);
+    b.d_status = (int*)(D + o_status);
+    b.buckets = {{0, 1, C, jacobi_smem_bytes(n, npad, C)}};
+    b.neig = 1;
+    rc = launch_jacobi(b, ws, 1);
+    if (rc) return rc;
+    k_eig_sort<<<1, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1);
+    CK(cudaGetLastError());
+    std::vector<double> ct(nn);
+    int st = 0;
+    CK(cudaMemcpyAsync(w, D + o_e, n * 8, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaMemcpyAsync(ct.data(), D + o_c, nn * 8, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaMemcpyAsync(&st, D + o_status, 4, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaStreamSynchronize(ws->stream));
+    if (st) return fail(AM1GPU_LINALG, "Jacobi eigensolver did not converge");
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) v[(size_t)i * n + k] = ct[(size_t)k * n + i];
+    return AM1GPU_OK;
+}
+
+}  // namespace am1
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+extern "C" {
+
+void am1gpu_default_options(am1gpu_options* o) {
+    if (!o) return;
+    o->reference = AM1GPU_REF_AUTO;
+    o->method = AM1GPU_METHOD_AM1;
+    o->max_scf = 200;
+    o->use_diis = 1;
+    o->accelerator = AM1GPU_ACCEL_ADIIS_CDIIS;
+    o->precision = AM1GPU_PRECISION_FP64;
+    o->e_tol = 1.0e-8;
+    o->p_tol = 1.0e-7;
+    o->adiis_switch = 0.1;
+}
+
+int am1gpu_basis_size(int32_t natoms, const int32_t* z, int32_t method, int32_t* nao) {
+    if (natoms < 0 || (natoms > 0 && !z) || !nao) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    int tot = 0;
+    for (int i = 0; i < natoms; ++i) {
+        if (z[i] < 0 || z[i] > am1::MAX_Z || !am1::helem(method == 1, z[i]).present)
+            return am1::fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, "element Z=" + std::to_string(z[i]) + " is not parameterized");
+        tot += am1::helem(method == 1, z[i]).norb;
+    }
+    *nao = tot;
+    return AM1GPU_OK;
+}
+
+int am1gpu_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res) {
+    if (!mol || !opts || !res) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    int32_t st = 0;
+    return am1::scf_batch(1, mol, opts, res, &st);
+}
+
+int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* results,
+                     int32_t* status) {
+    return am1::scf_batch(nmol, mols, opts, results, status);
+}
+
+int am1gpu_build_core(const am1gpu_molecule* mol, int32_t method, double* h_core, double* core_ev) {
+    return am1::build_core_one(mol, method, h_core, core_ev);
+}
+
+int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* p_tot, const double* p_spin,
+                      double spin_scale, double* fock) {
+    return am1::build_fock_one(mol, method, p_tot, p_spin, spin_scale, fock);
+}
+
+int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {
+    return am1::symmetric_eigen_one(n, a, w, v);
+}
+
+const char* am1gpu_last_error(void) { return am1::g_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,503 @@
+// The per-iteration SCF bookkeeping kernels (am1-rs src/scf.rs:475-1204), batched over
+// molecules and spin channels:
+//   k_sad_init     superposition-of-atomic-densities guess            scf.rs:475-494, 730-740
+//   k_post_fock    one pass over the upper triangle of F, F.P, P, H:
+//                  energy traces (scf.rs:595, 767), the commutator e = FP - (FP)^T and its norm
+//                  (scf.rs:531-544, 600), the packed history push (scf.rs:603-614, 877-952) and
+//                  the new row/column of the CDIIS and A-DIIS Gram matrices (only those change)
+//   k_diis_solve   one thread per molecule: history bookkeeping, divergence guard
+//                  (scf.rs:621-625), CDIIS bordered solve with the 1e-12 pivot guard
+//                  (scf.rs:966-988, 1095-1141), A-DIIS simplex (scf.rs:1061-1091, 1144-1204)
+//   k_combine      F* = sum c_i F_i from the packed history (scf.rs:955-963), Gershgorin bounds
+//   k_density_post rms(P_new - P) and P <- P_new                      scf.rs:546-555
+//   k_converge     de / dp test and iteration count                   scf.rs:663-696, 810-823
+#include <cuda_runtime.h>
+
+#include "am1gpu_internal.h"
+#include "kernels.h"
+
+namespace am1 {
+
+__device__ __forceinline__ long long sym_row(int r, int n) { return (long long)r * n - (long long)r * (r - 1) / 2; }
+__device__ __forceinline__ long long anti_row(int r, int n) { return (long long)r * n - (long long)r * (r + 1) / 2; }
+
+__global__ void k_sad_init(const MolDesc* __restrict__ mols, const int* __restrict__ atom_mol, int natoms_total,
+                           const DevElem* __restrict__ params, const int* __restrict__ atom_z, double* __restrict__ arena) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= natoms_total) return;
+    const MolDesc md = mols[atom_mol[a]];
+    const int A = a - md.atom_base, h = md.nheavy, n = md.nao;
+    const DevElem& e = params[md.method * (MAX_Z + 1) + atom_z[a]];
+    const double zv = e.core_charge;
+    const double ns = fmin(zv, 2.0), np = fmax(zv - ns, 0.0);
+    double scale[2] = {1.0, 1.0};
+    if (md.nch == 2) {
+        const double tot = (double)max(md.n_occ[0] + md.n_occ[1], 1);
+        scale[0] = (double)md.n_occ[0] / tot;
+        scale[1] = (double)md.n_occ[1] / tot;
+    }
+    for (int c = 0; c < md.nch; ++c) {
+        double* P = arena + md.ch_base[c] + SLOT_P * (long long)n * n;
+        if (A < h) {
+            const int o = 4 * A;
+            P[(long long)o * n + o] = ns * scale[c];
+            for (int k = 1; k < 4; ++k) P[(long long)(o + k) * n + o + k] = np / 3.0 * scale[c];
+        } else {
+            const int o = 4 * h + (A - h);
+            P[(long long)o * n + o] = ns * scale[c];
+        }
+    }
+}
+
+// Identity warm start for the eigensolver (C^T = I; the slot is zero-filled beforehand).
+__global__ void k_identity(const ChanJob* __restrict__ jobs) {
+    const ChanJob jb = jobs[blockIdx.y];
+    double* Ct = jb.Ct;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.n; i += gridDim.x * blockDim.x) Ct[(long long)i * jb.n + i] = 1.0;
+}
+
+__device__ __forceinline__ void live_slots(const MolState& s, int& newslot, unsigned& live_mask) {
+    const int c = s.hist_count, head = s.hist_head;
+    live_mask = 0;
+    if (c < MAX_DIIS) {
+        newslot = (head + c) % MAX_DIIS;
+        for (int i = 0; i < c; ++i) live_mask |= 1u << ((head + i) % MAX_DIIS);
+    } else {
+        newslot = head;
+        for (int i = 1; i < MAX_DIIS; ++i) live_mask |= 1u << ((head + i) % MAX_DIIS);
+    }
+}
+
+constexpr int POST_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __restrict__ jobs, const MolDesc* __restrict__ mols,
+                                                               const MolState* __restrict__ st, int nblk, int energy_only, int force) {
+    const ChanJob jb = jobs[blockIdx.y];
+    const MolState& s = st[jb.mol];
+    if (!force && !s.active) return;
+    const int n = jb.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int newslot = 0;
+    unsigned live = 0;
+    live_slots(s, newslot, live);
+    const long long ls = packed_sym_len(n), la = packed_anti_len(n);
+    double acc[RED_N];
+#pragma unroll
+    for (int k = 0; k < RED_N; ++k) acc[k] = 0.0;
+    const bool adiis = jb.hD != nullptr;
+    for (int r = blockIdx.x * POST_WARPS + warp; r < n; r += nblk * POST_WARPS) {
+        const double* Fr = jb.F + (long long)r * n;
+        const double* Pr = jb.P + (long long)r * n;
+        const double* Hr = jb.H + (long long)r * n;
+        const long long rs = sym_row(r, n), ra = anti_row(r, n);
+        for (int c = r + lane; c < n; c += 32) {
+            const double f = Fr[c], p = Pr[c], hh = Hr[c];
+            const double wgt = c == r ? 1.0 : 2.0;
+            acc[RED_E_H] += wgt * p * hh;
+            acc[RED_E_F] += wgt * p * f;
+            if (energy_only) continue;
+            const long long si = rs + (c - r);
+            jb.hF[newslot * ls + si] = f;
+            if (adiis) {
+                jb.hD[newslot * ls + si] = p;
+                acc[RED_GROW + newslot] += wgt * p * f;
+#pragma unroll
+                for (int j = 0; j < MAX_DIIS; ++j)
+                    if (live >> j & 1u) {
+                        acc[RED_GROW + j] += wgt * p * jb.hF[j * ls + si];
+                        acc[RED_GCOL + j] += wgt * jb.hD[j * ls + si] * f;
+                    }
+            }
+            if (c > r) {
+                const double e = jb.FP[(long long)r * n + c] - jb.FP[(long long)c * n + r];
+                const long long ai = ra + (c - r - 1);
+                jb.hE[newslot * la + ai] = e;
+                acc[RED_ERR2] += 2.0 * e * e;
+                acc[RED_B + newslot] += e * e;
+#pragma unroll
+                for (int j = 0; j < MAX_DIIS; ++j)
+                    if (live >> j & 1u) acc[RED_B + j] += e * jb.hE[j * la + ai];
+            }
+        }
+    }
+    __shared__ double part[POST_WARPS][RED_N];
+#pragma unroll
+    for (int k = 0; k < RED_N; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) part[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < RED_N) {
+        double v = 0.0;
+        for (int w = 0; w < POST_WARPS; ++w) v += part[w][threadIdx.x];
+        jb.red[(long long)blockIdx.x * RED_N + threadIdx.x] = v;
+    }
+}
+
+// Gaussian elimination with partial pivoting; false when a pivot is below 1e-12.
+__device__ bool solve_small(int n, double* m, double* rhs, double* x) {
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        double best = fabs(m[col * n + col]);
+        for (int row = col + 1; row < n; ++row) {
+            const double v = fabs(m[row * n + col]);
+            if (v > best) {
+                best = v;
+                piv = row;
+            }
+        }
+        if (best < 1.0e-12) return false;
+        if (piv != col) {
+            for (int j = 0; j < n; ++j) {
+                const double t = m[col * n + j];
+                m[col * n + j] = m[piv * n + j];
+                m[piv * n + j] = t;
+            }
+            const double t = rhs[col];
+            rhs[col] = rhs[piv];
+            rhs[piv] = t;
+        }
+        for (int row = col + 1; row < n; ++row) {
+            const double factor = m[row * n + col] / m[col * n + col];
+            if (factor == 0.0) continue;
+            for (int j = col; j < n; ++j) m[row * n + j] -= factor * m[col * n + j];
+            rhs[row] -= factor * rhs[col];
+        }
+    }
+    for (int col = n - 1; col >= 0; --col) {
+        double sum = rhs[col];
+        for (int j = col + 1; j < n; ++j) sum -= m[col * n + j] * x[j];
+        x[col] = sum / m[col * n + col];
+    }
+    return true;
+}
+
+// Euclidean projection onto the probability simplex (sort descending, running threshold).
+__device__ void simplex_project(int n, const double* v, double* out) {
+    double u[MAX_DIIS];
+    for (int i = 0; i < n; ++i) u[i] = v[i];
+    for (int i = 1; i < n; ++i) {  // insertion sort, descending
+        const double x = u[i];
+        int j = i - 1;
+        while (j >= 0 && u[j] < x) {
+            u[j + 1] = u[j];
+            --j;
+        }
+        u[j + 1] = x;
+    }
+    double css = 0.0, theta = 0.0;
+    for (int j = 0; j < n; ++j) {
+        css += u[j];
+        const double t = (css - 1.0) / ((double)j + 1.0);
+        if (u[j] - t > 0.0) theta = t;
+    }
+    for (int i = 0; i < n; ++i) out[i] = fmax(v[i] - theta, 0.0);
+}
+
+__device__ void adiis_simplex(int m, const double* d, const double* S, double* c) {
+    double L = 1.0e-12;
+    for (int i = 0; i < m; ++i) {
+        double row = 0.0;
+        for (int j = 0; j < m; ++j) row += fabs(S[i * MAX_DIIS + j] + S[j * MAX_DIIS + i]);
+        L = fmax(L, row);
+    }
+    const double lr = 1.0 / L;
+    for (int i = 0; i < m; ++i) c[i] = 0.0;
+    c[m - 1] = 1.0;
+    for (int it = 0; it < 400; ++it) {
+        double trial[MAX_DIIS], proj[MAX_DIIS];
+        for (int k = 0; k < m; ++k) {
+            double acc = 2.0 * d[k];
+            for (int j = 0; j < m; ++j) acc += (S[k * MAX_DIIS + j] + S[j * MAX_DIIS + k]) * c[j];
+            trial[k] = c[k] - lr * acc;
+        }
+        simplex_project(m, trial, proj);
+        double delta = 0.0;
+        for (int i = 0; i < m; ++i) {
+            delta += fabs(proj[i] - c[i]);
+            c[i] = proj[i];
+        }
+        if (delta < 1.0e-12) break;
+    }
+}
+
+__global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __restrict__ jobs, const int* __restrict__ mol_job0,
+                             int nmol, MolState* __restrict__ st, int* __restrict__ mol_status, int nblk, ScfParams prm) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= nmol) return;
+    MolState& s = st[mi];
+    if (!s.active) return;
+    const MolDesc md = mols[mi];
+    double tot[RED_N];
+    for (int k = 0; k < RED_N; ++k) tot[k] = 0.0;
+    for (int c = 0; c < md.nch; ++c) {
+        const ChanJob& jb = jobs[mol_job0[mi] + c];
+        for (int b = 0; b < nblk; ++b)
+            for (int k = 0; k < RED_N; ++k) tot[k] += jb.red[(long long)b * RED_N + k];
+    }
+    const double e_elec = 0.5 * (tot[RED_E_H] + tot[RED_E_F]);
+    const double err = sqrt(tot[RED_ERR2]);
+    // history bookkeeping: physical slot of logical index i is (head + i) % 8
+    const int cnt = s.hist_count;
+    int newslot;
+    unsigned live;
+    live_slots(s, newslot, live);
+    if (cnt == MAX_DIIS) {  // drop the oldest: shift the Gram matrices up-left
+        for (int i = 0; i < MAX_DIIS - 1; ++i)
+            for (int j = 0; j < MAX_DIIS - 1; ++j) {
+                s.bmat[i * MAX_DIIS + j] = s.bmat[(i + 1) * MAX_DIIS + j + 1];
+                s.gmat[i * MAX_DIIS + j] = s.gmat[(i + 1) * MAX_DIIS + j + 1];
+            }
+        s.hist_head = (s.hist_head + 1) % MAX_DIIS;
+        s.hist_count = MAX_DIIS;
+    } else {
+        s.hist_count = cnt + 1;
+    }
+    const int m = s.hist_count, last = m - 1;
+    for (int i = 0; i < m; ++i) {
+        const int phys = (s.hist_head + i) % MAX_DIIS;
+        const double b = 2.0 * tot[RED_B + phys];
+        s.bmat[last * MAX_DIIS + i] = b;
+        s.bmat[i * MAX_DIIS + last] = b;
+        s.gmat[last * MAX_DIIS + i] = tot[RED_GROW + phys];  // <D_last, F_i>
+        s.gmat[i * MAX_DIIS + last] = tot[RED_GCOL + phys];  // <D_i, F_last>
+    }
+    s.gmat[last * MAX_DIIS + last] = tot[RED_GROW + newslot];
+    s.e_elec = e_elec;
+    s.err_norm = err;
+    s.mode = 0;
+    s.accel_used = 0;
+    if (!isfinite(e_elec) || !isfinite(err)) {
+        s.status = 4;  // AM1GPU_SCF_DIVERGED
+        mol_status[mi] = 4;
+        s.active = 0;
+        s.iter += 1;
+        return;
+    }
+    int accel = prm.use_diis ? prm.accelerator : 0;
+    if (md.nch == 2) accel = prm.use_diis ? 1 : 0;  // UHF: CDIIS only (scf.rs:770-803)
+    bool use_adiis = accel == 2 && err > prm.adiis_switch;
+    if (accel == 1 || (accel == 2 && !use_adiis)) {
+        if (m >= 2) {
+            const int dim = m + 1;
+            double B[(MAX_DIIS + 1) * (MAX_DIIS + 1)], rhs[MAX_DIIS + 1], x[MAX_DIIS + 1];
+            for (int i = 0; i < dim * dim; ++i) B[i] = 0.0;
+            for (int i = 0; i < m; ++i) {
+                for (int j = 0; j < m; ++j) B[i * dim + j] = s.bmat[i * MAX_DIIS + j];
+                B[i * dim + m] = -1.0;
+                B[m * dim + i] = -1.0;
+            }
+            for (int i = 0; i < dim; ++i) rhs[i] = 0.0;
+            rhs[m] = -1.0;
+            if (solve_small(dim, B, rhs, x)) {
+                double wsum = 0.0;
+                bool fin = true;
+                for (int i = 0; i < m; ++i) {
+                    wsum += fabs(x[i]);
+                    fin = fin && isfinite(x[i]);
+                }
+                if (isfinite(wsum) && fin) {
+                    for (int i = 0; i < m; ++i) s.coeff[i] = x[i];
+                    s.mode = 1;
+                    s.accel_used = 1;
+                }
+            }
+        }
+    } else if (use_adiis && m >= 2) {
+        double d[MAX_DIIS], S[MAX_DIIS * MAX_DIIS], c[MAX_DIIS];
+        const double gll = s.gmat[last * MAX_DIIS + last];
+        for (int i = 0; i < m; ++i) d[i] = s.gmat[i * MAX_DIIS + last] - gll;
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                S[i * MAX_DIIS + j] = s.gmat[i * MAX_DIIS + j] - s.gmat[i * MAX_DIIS + last] - s.gmat[last * MAX_DIIS + j] + gll;
+        adiis_simplex(m, d, S, c);
+        bool fin = true;
+        for (int i = 0; i < m; ++i) fin = fin && isfinite(c[i]);
+        if (fin) {
+            for (int i = 0; i < m; ++i) s.coeff[i] = c[i];
+            s.mode = 1;
+            s.accel_used = 2;
+        }
+    }
+}
+
+__global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int force) {
+    const ChanJob jb = jobs[blockIdx.y];
+    const MolState& s = st[jb.mol];
+    if (!force && !s.active) return;
+    const int n = jb.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const long long ls = packed_sym_len(n);
+    const int m = s.hist_count;
+    for (int r = blockIdx.x * nw + warp; r < n; r += gridDim.x * nw) {
+        double* out = jb.FP + (long long)r * n;
+        double bound = 0.0, diag = 0.0;
+        for (int c = lane; c < n; c += 32) {
+            double v;
+            if (s.mode == 0) {
+                v = jb.F[(long long)r * n + c];
+            } else {
+                const int lo = min(r, c), hi = max(r, c);
+                const long long si = sym_row(lo, n) + (hi - lo);
+                v = 0.0;
+                for (int i = 0; i < m; ++i) v += s.coeff[i] * jb.hF[((s.hist_head + i) % MAX_DIIS) * ls + si];
+            }
+            out[c] = v;
+            if (c == r) diag = v;
+            else bound += fabs(v);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            bound += __shfl_xor_sync(0xffffffffu, bound, o);
+            diag += __shfl_xor_sync(0xffffffffu, diag, o);
+        }
+        if (lane == 0) jb.rowmin[r] = diag - bound;
+    }
+}
+
+__global__ void k_density_post(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int nblk) {
+    const ChanJob jb = jobs[blockIdx.y];
+    if (!st[jb.mol].active) return;
+    const long long nn = (long long)jb.n * jb.n;
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)nblk * blockDim.x) {
+        const double pn = jb.Pnew[i];
+        const double d = pn - jb.P[i];
+        acc += d * d;
+        jb.P[i] = pn;
+    }
+    __shared__ double part[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) part[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += part[w];
+        jb.red2[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_converge(const MolDesc* __restrict__ mols, const ChanJob* __restrict__ jobs, const int* __restrict__ mol_job0,
+                           int nmol, MolState* __restrict__ st, int* __restrict__ mol_status, int nblk, ScfParams prm,
+                           int* __restrict__ active_count) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= nmol) return;
+    MolState& s = st[mi];
+    if (!s.active) return;
+    if (mol_status[mi] != 0) {  // the eigensolver refused its input
+        s.active = 0;
+        s.status = mol_status[mi];
+        s.iter += 1;
+        return;
+    }
+    const MolDesc md = mols[mi];
+    double dp = 0.0;
+    for (int c = 0; c < md.nch; ++c) {
+        const ChanJob& jb = jobs[mol_job0[mi] + c];
+        double ss = 0.0;
+        for (int b = 0; b < nblk; ++b) ss += jb.red2[b];
+        dp += sqrt(ss / fmax((double)jb.n * jb.n, 1.0));
+    }
+    const double de = fabs(s.e_elec - s.e_old);
+    s.dp = dp;
+    s.e_old = s.e_elec;
+    s.residual = s.err_norm;
+    const int it = s.iter;
+    s.iter = it + 1;
+    if (it > 0 && de < prm.e_tol && (dp < prm.p_tol || s.err_norm < 1.0e-7)) {
+        s.converged = 1;
+        s.active = 0;
+    } else if (s.iter >= prm.max_scf) {
+        s.active = 0;
+    }
+    if (s.active) atomicAdd(active_count, 1);
+}
+
+__global__ void k_final_energy(const MolDesc* __restrict__ mols, const ChanJob* __restrict__ jobs, const int* __restrict__ mol_job0,
+                               int nmol, MolState* __restrict__ st, int nblk) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= nmol) return;
+    const MolDesc md = mols[mi];
+    double eh = 0.0, ef = 0.0;
+    for (int c = 0; c < md.nch; ++c) {
+        const ChanJob& jb = jobs[mol_job0[mi] + c];
+        for (int b = 0; b < nblk; ++b) {
+            eh += jb.red[(long long)b * RED_N + RED_E_H];
+            ef += jb.red[(long long)b * RED_N + RED_E_F];
+        }
+    }
+    st[mi].e_final = 0.5 * (eh + ef);
+}
+
+// Result record of one molecule (src/scf.rs:370-438): energies, heat of formation, Mulliken
+// charges, dipole (point charges + s-p hybrid term), frontier orbitals.
+__global__ void k_results(const MolDesc* __restrict__ mols, const ChanJob* __restrict__ jobs, const int* __restrict__ mol_job0,
+                          int nmol, const MolState* __restrict__ st, const int* __restrict__ mol_status,
+                          const DevElem* __restrict__ params, const int* __restrict__ atom_z, const double* __restrict__ atom_xyz,
+                          double* __restrict__ res, double* __restrict__ charges) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= nmol) return;
+    const MolDesc md = mols[mi];
+    const MolState& s = st[mi];
+    const int n = md.nao, h = md.nheavy;
+    const long long nn = (long long)n * n;
+    const double* P0 = jobs[mol_job0[mi]].P;
+    const double* P1 = md.nch == 2 ? jobs[mol_job0[mi] + 1].P : nullptr;
+    double e_isol = 0.0, eheat = 0.0, dip[3] = {0.0, 0.0, 0.0};
+    for (int A = 0; A < md.natoms; ++A) {
+        const int a = md.atom_base + A;
+        const DevElem& e = params[md.method * (MAX_Z + 1) + atom_z[a]];
+        e_isol += e.e_isol;
+        eheat += e.eheat_ev;
+        const int o = A < h ? 4 * A : 4 * h + (A - h), no = A < h ? 4 : 1;
+        double pop = 0.0;
+        for (int k = 0; k < no; ++k) {
+            const long long d = (long long)(o + k) * n + o + k;
+            pop += P1 ? P0[d] + P1[d] : P0[d];
+        }
+        const double q = e.core_charge - pop;
+        charges[a] = q;
+        for (int k = 0; k < 3; ++k) dip[k] += atom_xyz[3 * a + k] * q;
+        if (e.norb == 4) {
+            const double hyb = -2.0 * e.dd;
+            for (int k = 0; k < 3; ++k) {
+                const long long idx = (long long)o * n + o + 1 + k;
+                dip[k] += hyb * (P1 ? P0[idx] + P1[idx] : P0[idx]);
+            }
+        }
+    }
+    (void)nn;
+    double* r = res + (long long)mi * RES_N;
+    const double total = s.e_final + s.core_ev;
+    r[RES_ELEC] = s.e_final;
+    r[RES_CORE] = s.core_ev;
+    r[RES_TOTAL] = total;
+    r[RES_HOF] = (total - e_isol + eheat) * EV_TO_KCAL;
+    double mag = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        r[RES_DIP + k] = dip[k] * AU_DIPOLE_TO_DEBYE;
+        mag += r[RES_DIP + k] * r[RES_DIP + k];
+    }
+    r[RES_DIPMAG] = sqrt(mag);
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    const double* ea = jobs[mol_job0[mi]].eps;
+    const int na = md.n_occ[0], nb = md.n_occ[1];
+    r[RES_HOMO] = na >= 1 ? ea[na - 1] : nan;
+    r[RES_LUMO] = na < n ? ea[na] : nan;
+    r[RES_HOMO_B] = nan;
+    r[RES_LUMO_B] = nan;
+    if (md.nch == 2) {
+        const double* eb = jobs[mol_job0[mi] + 1].eps;
+        r[RES_HOMO_B] = nb >= 1 ? eb[nb - 1] : nan;
+        r[RES_LUMO_B] = nb < n ? eb[nb] : nan;
+    }
+    r[RES_RESID] = s.residual;
+    r[RES_ITER] = (double)s.iter;
+    r[RES_CONV] = (double)s.converged;
+    r[RES_STATUS] = (double)(mol_status[mi] ? mol_status[mi] : s.status);
+}
+
+}  // namespace am1

@@ -1,0 +1,97 @@
+// Kernel interfaces of libam1gpu (device side), shared with the host driver.
+#pragma once
+
+#include <cstddef>
+
+#include "am1gpu_internal.h"
+
+namespace am1 {
+
+struct GemmJob {
+    const double* A;
+    const double* B;
+    double* C;
+    int M, N, K, lda, ldb, ldc;
+    double alpha;
+    int mol;
+};
+
+struct GemmTile {
+    int job;
+    int tm, tn;
+};
+
+// One eigenproblem (a channel of a molecule).
+struct EigJob {
+    const double* Gt;      // C0^T F (rows = columns of F C0), n x n
+    const double* Ct;      // warm start C0^T (rows = vectors), n x n
+    double* Vs;            // npad x n: eigenvector rows in slot order (scratch)
+    double* lam;           // npad: eigenvalues in slot order (scratch)
+    int* colid_out;        // npad: column id per slot (scratch)
+    double* eps;           // n: sorted eigenvalues (output)
+    double* Ct_out;        // n x n: sorted eigenvector rows (output)
+    const double* rowmin;  // n: Gershgorin row lower bounds of F
+    int* sweeps_out;       // optional
+    int n, npad, mol;
+};
+
+// One (molecule, channel) job of the element-wise SCF passes.
+struct ChanJob {
+    int mol, ch, n;
+    double* F;
+    double* FP;       // F.P, then reused for the extrapolated Fock
+    double* P;
+    double* Pnew;
+    double* Ct;       // eigenvector rows (C^T), n x n
+    double* eps;      // sorted eigenvalues, n
+    const double* H;
+    double* hF;       // packed history of F  [8][n(n+1)/2]
+    double* hE;       // packed history of [F,P] [8][n(n-1)/2]
+    double* hD;       // packed history of P  [8][n(n+1)/2] (A-DIIS) or nullptr
+    double* rowmin;   // n
+    double* red;      // per-block partial sums [nblk][RED_N]
+    double* red2;     // per-block partial sums of (P_new - P)^2 [nblk]
+};
+
+struct ScfParams {
+    int max_scf, use_diis, accelerator;
+    double e_tol, p_tol, adiis_switch;
+};
+
+__global__ void k_pair_integrals(const MolDesc* mols, int nmol, const long long* pair_prefix, long long npairs,
+                                 const DevElem* params, const int* atom_z, const double* atom_xyz, double* wstore,
+                                 double* hmat, double* ecc, int* mol_status);
+__global__ void k_core_diag(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
+                            const int* atom_z, const double* wstore, double* hmat);
+__global__ void k_core_energy(const MolDesc* mols, const double* ecc, MolState* st);
+__global__ void k_fock(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
+                       const int* atom_z, const double* wstore, double* arena, const MolState* st, int force);
+// C = alpha A B (A row-major M x K) and C = alpha A^T B (A stored K x M)
+__global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force);
+__global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force);
+__global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force);
+__global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force);
+size_t jacobi_smem_bytes(int n, int npad, int C);
+
+__global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
+                           const int* atom_z, double* arena);
+__global__ void k_identity(const ChanJob* jobs);
+__global__ void k_post_fock(const ChanJob* jobs, const MolDesc* mols, const MolState* st, int nblk, int energy_only,
+                            int force);
+__global__ void k_diis_solve(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,
+                             int* mol_status, int nblk, ScfParams prm);
+__global__ void k_combine(const ChanJob* jobs, const MolState* st, int force);
+__global__ void k_density_post(const ChanJob* jobs, const MolState* st, int nblk);
+__global__ void k_converge(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,
+                           int* mol_status, int nblk, ScfParams prm, int* active_count);
+__global__ void k_final_energy(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,
+                               int nblk);
+// Per-molecule result record (doubles), see RES_* below; charges in internal atom order.
+__global__ void k_results(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, const MolState* st,
+                          const int* mol_status, const DevElem* params, const int* atom_z, const double* atom_xyz,
+                          double* res, double* charges);
+constexpr int RES_ELEC = 0, RES_CORE = 1, RES_TOTAL = 2, RES_HOF = 3, RES_DIP = 4, RES_DIPMAG = 7, RES_HOMO = 8,
+              RES_LUMO = 9, RES_HOMO_B = 10, RES_LUMO_B = 11, RES_RESID = 12, RES_ITER = 13, RES_CONV = 14,
+              RES_STATUS = 15, RES_N = 16;
+
+}  // namespace am1

@@ -1,0 +1,56 @@
+"""The C ABI library loads and exports every entry point include/am1gpu.h declares (CPU only:
+no compute call is made here)."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+
+from conftest import ROOT
+
+
+def _declared():
+    text = (ROOT / "include" / "am1gpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(am1gpu_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = _declared()
+    for required in ("am1gpu_scf", "am1gpu_scf_batch", "am1gpu_build_core", "am1gpu_build_fock",
+                     "am1gpu_symmetric_eigen", "am1gpu_basis_size", "am1gpu_default_options",
+                     "am1gpu_last_error"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    from am1gpu import _abi
+
+    assert _abi.LIB_PATH.exists(), "build libam1gpu.so first (__graft_entry__.build())"
+    dll = ctypes.CDLL(str(_abi.LIB_PATH))
+    for name in _declared():
+        assert hasattr(dll, name), name
+    # the ctypes signature table covers the header
+    assert set(_declared()) <= set(_abi.SIGNATURES)
+
+
+def test_default_options_match_the_reference():
+    # Am1Options::default(), src/scf.rs:174-197; am1gpu_default_options needs no device
+    from am1gpu import _abi
+
+    o = _abi.default_options()
+    assert (o.max_scf, o.use_diis, o.accelerator, o.reference, o.method) == (200, 1, 2, 0, 0)
+    assert (o.e_tol, o.p_tol, o.adiis_switch) == (1e-8, 1e-7, 0.1)
+
+
+def test_basis_size_without_a_device():
+    from am1gpu import native
+
+    assert native._nao([8, 1, 1], "am1") == 6
+    assert native._nao([6, 6, 1, 1, 1, 1, 1, 1], "am1") == 14
+    try:
+        native._nao([2], "am1")
+    except native.Am1GpuError as e:
+        assert e.code == 2
+    else:
+        raise AssertionError("helium must be refused")

@@ -1,0 +1,211 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle, on a B200.
+
+Tolerances are the north-star bars for the plain FP64 path: heat of formation within 1e-6
+kcal/mol, Mulliken charges within 1e-7 e, density within 1e-8 max-abs; operators (H_core,
+Fock) within 1e-10 eV, eigenvalues within 1e-10 relative.  Eigenvectors are compared through
+sign- and rotation-invariant quantities (reconstruction, density), as the reference's own tests do.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import atoms_to_arrays
+
+pytestmark = pytest.mark.gpu
+
+HOF_TOL = 1e-6      # kcal/mol
+Q_TOL = 1e-7        # e
+P_TOL = 1e-8        # max |dP|
+OP_TOL = 1e-10      # eV, operator elements
+
+
+def _golden_molecules(ref_values):
+    out = []
+    for c in ref_values["auxiliary_integral_impact"]["cases"]:
+        out.append((c["name"], *atoms_to_arrays(c["atoms"])))
+    out.append(("formaldehyde", *atoms_to_arrays(ref_values["scf_formaldehyde"]["atoms"])))
+    return out
+
+
+def _compare_scf(g, o, tag):
+    assert g["status"] == o["status"] == 0, (tag, g.get("error"), o.get("error"))
+    assert g["converged"] and o["converged"], tag
+    assert abs(g["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < HOF_TOL, (tag, g["heat_of_formation_kcal"], o["heat_of_formation_kcal"])
+    assert np.max(np.abs(g["charges"] - o["charges"])) < Q_TOL, tag
+    if "density" in g and "density" in o:
+        assert np.max(np.abs(g["density"] - o["density"])) < P_TOL, (tag, np.max(np.abs(g["density"] - o["density"])))
+    assert abs(g["iterations"] - o["iterations"]) <= 1, (tag, g["iterations"], o["iterations"])
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 64, 100, 113, 161, 200, 257, 330, 400])
+def test_symmetric_eigen(gpu, oracle, n):
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n))
+    a = a + a.T
+    w, v = gpu.eigh(a)
+    wo, _ = oracle.eigh(a)
+    scale = max(1.0, np.max(np.abs(wo)))
+    assert np.all(np.diff(w) >= 0)
+    assert np.max(np.abs(w - wo)) < 1e-10 * scale
+    assert np.max(np.abs(v.T @ v - np.eye(n))) < 1e-11 * max(1, n)
+    assert np.max(np.abs(v @ np.diag(w) @ v.T - a)) < 1e-11 * scale * max(1, n)
+
+
+def test_symmetric_eigen_known_answers(gpu):
+    # src/linalg.rs:479-519
+    w, v = gpu.eigh(np.array([[2.0, 1.0], [1.0, 2.0]]))
+    assert abs(w[0] - 1) < 1e-10 and abs(w[1] - 3) < 1e-10
+    a = np.array([[4.0, 1.0, 2.0], [1.0, 3.0, 0.0], [2.0, 0.0, 1.0]])
+    w, v = gpu.eigh(a)
+    assert np.max(np.abs(v @ np.diag(w) @ v.T - a)) < 1e-9
+
+
+def test_symmetric_eigen_refuses_non_finite(gpu):
+    # src/linalg.rs:292-304
+    a = np.eye(4)
+    a[2, 1] = np.nan
+    with pytest.raises(gpu.Am1GpuError) as e:
+        gpu.eigh(a)
+    assert e.value.code == 5
+
+
+def test_core_hamiltonian(gpu, oracle, ref_values):
+    from am1gpu import workloads as W, _abi
+
+    mols = _golden_molecules(ref_values)
+    w = W.water_cluster(5, np.random.default_rng(11))
+    mols.append(("water5", w.numbers, _abi.angstrom_to_bohr(w.xyz)))
+    a = W.alkane(6, np.random.default_rng(12))
+    mols.append(("hexane", a.numbers, _abi.angstrom_to_bohr(a.xyz)))
+    for name, z, xyz in mols:
+        h, e = gpu.build_core(z, xyz)
+        ho, eo = oracle.build_core(z, xyz)
+        assert np.max(np.abs(h - ho)) < OP_TOL, (name, np.max(np.abs(h - ho)))
+        assert abs(e - eo) < 1e-9 * max(1.0, abs(eo)), name
+
+
+def test_fock_build(gpu, oracle, ref_values):
+    rng = np.random.default_rng(3)
+    for name, z, xyz in _golden_molecules(ref_values):
+        h, _ = oracle.build_core(z, xyz)
+        n = h.shape[0]
+        p = rng.standard_normal((n, n)) * 0.3
+        p = p + p.T
+        ps = rng.standard_normal((n, n)) * 0.2
+        ps = ps + ps.T
+        for pt, pspin, sc in ((p, p, 0.5), (p, ps, 1.0)):
+            f = gpu.build_fock(z, xyz, pt, pspin, sc)
+            fo = oracle.build_fock(z, xyz, pt, pspin, sc)
+            assert np.max(np.abs(f - fo)) < OP_TOL, (name, sc, np.max(np.abs(f - fo)))
+
+
+def test_scf_golden_molecules(gpu, oracle, ref_values):
+    for name, z, xyz in _golden_molecules(ref_values):
+        g = gpu.scf(z, xyz)
+        o = oracle.scf(z, xyz)
+        _compare_scf(g, o, name)
+
+
+def test_scf_recorded_heats_of_formation(gpu, ref_values):
+    # tests/auxiliary_integral_impact.rs:22-80 through the GPU path
+    for c in ref_values["auxiliary_integral_impact"]["cases"]:
+        z, xyz = atoms_to_arrays(c["atoms"])
+        g = gpu.scf(z, xyz)
+        assert abs(g["heat_of_formation_kcal"] - c["hof_kcal"]) < 6e-5, c["name"]
+
+
+@pytest.mark.parametrize("method,tag", [("am1", "AM1_CO2"), ("rm1", "RM1_CO2")])
+def test_co2_spectrum(gpu, ref_values, method, tag):
+    # tests/mopac_reference.rs: all 12 orbital energies (two degenerate pairs) and the carbon charge
+    from am1gpu import _abi
+
+    ref = ref_values["mopac_co2"][tag]
+    tol = ref_values["mopac_co2"]["tolerance"]
+    b = ref["bond"]
+    g = gpu.scf([6, 8, 8], _abi.angstrom_to_bohr([[0, 0, 0], [b, 0, 0], [-b, 0, 0]]), method=method)
+    assert g["converged"]
+    assert np.max(np.abs(g["mo_energies"] - np.array(ref["orbital_energies"]))) < tol["orbital"]
+    assert abs(g["charges"][0] - ref["charge_carbon"]) < tol["charge"]
+
+
+def test_uhf_radical_and_forced_references(gpu, oracle, ref_values):
+    m = ref_values["scf_methyl_radical"]
+    z, xyz = atoms_to_arrays(m["atoms"])
+    g = gpu.scf(z, xyz, multiplicity=2)
+    o = oracle.scf(z, xyz, multiplicity=2)
+    _compare_scf(g, o, "CH3 doublet")
+    assert g["unrestricted"]
+    assert abs(np.trace(g["spin_density"]) - 1.0) < 1e-6
+    assert np.max(np.abs(g["spin_density"] - o["spin_density"])) < P_TOL
+    zw, xw = atoms_to_arrays(ref_values["scf_water"]["atoms"])
+    rhf = gpu.scf(zw, xw, reference="rhf")
+    uhf = gpu.scf(zw, xw, reference="uhf")
+    auto = gpu.scf(zw, xw)
+    assert abs(uhf["energy_ev"] - rhf["energy_ev"]) < 1e-6
+    assert abs(auto["energy_ev"] - rhf["energy_ev"]) < 1e-12
+    # restricted open shell is refused (src/scf.rs:1442-1460)
+    r = gpu.scf(z, xyz, multiplicity=2, reference="rhf")
+    assert r["status"] == 1
+
+
+def test_accelerators(gpu, oracle, ref_values):
+    # src/scf.rs:1344-1369 on the GPU path, each against the oracle's same accelerator
+    z, xyz = atoms_to_arrays(ref_values["scf_formaldehyde"]["atoms"])
+    res = {}
+    for acc in ("adiis_cdiis", "cdiis", "none"):
+        g = gpu.scf(z, xyz, accelerator=acc, max_scf=500)
+        o = oracle.scf(z, xyz, accelerator=acc, max_scf=500)
+        _compare_scf(g, o, acc)
+        res[acc] = g
+    assert abs(res["adiis_cdiis"]["energy_ev"] - res["none"]["energy_ev"]) < 1e-6
+    assert res["adiis_cdiis"]["iterations"] < res["none"]["iterations"]
+
+
+def test_error_codes(gpu):
+    from am1gpu import _abi
+
+    r = gpu.scf([2, 1], [[0, 0, 0], [1.4, 0, 0]])
+    assert r["status"] == _abi.ELEMENT_NOT_PARAMETERIZED
+    r = gpu.scf([35, 1], [[0, 0, 0], [2.7, 0, 0]])
+    assert r["status"] == _abi.UNSUPPORTED
+    r = gpu.scf([8, 1, 1], [[0, 0, 0], [1.8, 0, 0], [-0.45, 1.75, 0]], multiplicity=2)
+    assert r["status"] == _abi.INVALID_INPUT
+    r = gpu.scf([8, 1, 1], [[0, 0, 0], [1.8, 0, 0], [-0.45, 1.75, 0]], max_scf=2)
+    assert r["status"] == _abi.SCF_NOT_CONVERGED and r["iterations"] == 2 and np.isfinite(r["residual"])
+
+
+def test_config0_water32(gpu, oracle):
+    from am1gpu import workloads as W, _abi
+
+    m = W.config0()
+    xyz = _abi.angstrom_to_bohr(m.xyz)
+    g = gpu.scf(m.numbers, xyz)
+    o = oracle.scf(m.numbers, xyz)
+    _compare_scf(g, o, "config0")
+
+
+def test_batch_matches_oracle_and_solo(gpu, oracle):
+    from am1gpu import workloads as W, _abi
+
+    rng = np.random.default_rng(21)
+    mols = []
+    for n in (1, 2, 3, 7, 12, 19):
+        a = W.alkane(n, rng)
+        mols.append((a.numbers, _abi.angstrom_to_bohr(a.xyz), 0.0, 1))
+    for k in (1, 2, 4, 9, 20, 33):
+        w = W.water_cluster(k, rng)
+        mols.append((w.numbers, _abi.angstrom_to_bohr(w.xyz), 0.0, 1))
+    for n in (1, 3, 6):
+        r = W.alkane(n, rng, radical=True)
+        mols.append((r.numbers, _abi.angstrom_to_bohr(r.xyz), 0.0, 2))
+    status, res = gpu.scf_batch(mols, want_matrices=True)
+    assert all(s == 0 for s in status), status
+    for i, (z, xyz, q, mult) in enumerate(mols):
+        o = oracle.scf(z, xyz, q, mult)
+        _compare_scf(res[i], o, f"batch[{i}]")
+        solo = gpu.scf(z, xyz, q, mult)
+        # same alone and in the mix
+        assert abs(solo["heat_of_formation_kcal"] - res[i]["heat_of_formation_kcal"]) < 1e-9
+        assert np.max(np.abs(solo["density"] - res[i]["density"])) < 1e-12
