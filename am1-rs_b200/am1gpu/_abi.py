@@ -107,6 +107,22 @@ class Result(ctypes.Structure):
     ]
 
 
+class CallStats(ctypes.Structure):
+    _fields_ = [
+        ("device_ms", ctypes.c_double),
+        ("phase_ms", ctypes.c_double * 8),
+        ("phase_launches", ctypes.c_int64 * 8),
+        ("kernel_launches", ctypes.c_int64),
+        ("h2d_bytes", ctypes.c_int64),
+        ("d2h_bytes", ctypes.c_int64),
+        ("scf_cycles", ctypes.c_int32),
+    ]
+
+
+PHASES = ["basis+core", "scf:fock", "scf:commutator", "scf:accel", "scf:eigen", "eigen:jacobi", "scf:density", "final"]
+
+_bp = ctypes.c_void_p
+
 # Every function the header declares, with its ctypes signature.
 SIGNATURES = {
     "am1gpu_default_options": (None, [ctypes.POINTER(Options)]),
@@ -123,7 +139,27 @@ SIGNATURES = {
     ),
     "am1gpu_symmetric_eigen": (ctypes.c_int, [ctypes.c_int32, _dp, _dp, _dp]),
     "am1gpu_last_error": (ctypes.c_char_p, []),
+    "am1gpu_batch_create": (
+        ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(_bp)]),
+    "am1gpu_batch_run": (ctypes.c_int, [_bp]),
+    "am1gpu_batch_results": (ctypes.c_int, [_bp, ctypes.POINTER(Result), _ip]),
+    "am1gpu_batch_destroy": (None, [_bp]),
+    "am1gpu_set_timing": (None, [ctypes.c_int32]),
+    "am1gpu_last_call_stats": (ctypes.c_int, [ctypes.POINTER(CallStats)]),
+    "am1gpu_batch_stats": (ctypes.c_int, [_bp, ctypes.POINTER(CallStats)]),
 }
+
+
+def stats_dict(st: CallStats) -> dict:
+    return {
+        "device_ms": st.device_ms,
+        "phase_ms": dict(zip(PHASES, list(st.phase_ms))),
+        "phase_launches": dict(zip(PHASES, list(st.phase_launches))),
+        "kernel_launches": int(st.kernel_launches),
+        "h2d_bytes": int(st.h2d_bytes),
+        "d2h_bytes": int(st.d2h_bytes),
+        "scf_cycles": int(st.scf_cycles),
+    }
 
 _lib = None
 _lock = threading.Lock()

@@ -90,7 +90,10 @@ def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, raise
     mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
     o = _abi.default_options(**opts)
     method = opts.get("method", "am1")
-    nao = _nao(mb.z, method) if mb.z.size else 0
+    try:
+        nao = _nao(mb.z, method) if mb.z.size else 0
+    except Am1GpuError:
+        nao, want_matrices = 0, False  # the library reports the element error itself
     rb = _abi.ResultBuffers(mb.z.shape[0], nao, want_matrices)
     rc = _abi.lib().am1gpu_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
     if raise_on_error:
@@ -123,6 +126,50 @@ class Batch:
             rb.res = self.res[i]
             out.append(_result_dict(rb, int(self.status[i]), self.want_matrices))
         return out
+
+
+def last_call_stats() -> dict:
+    st = _abi.CallStats()
+    _check(_abi.lib().am1gpu_last_call_stats(ctypes.byref(st)))
+    return _abi.stats_dict(st)
+
+
+def set_timing(enable: bool) -> None:
+    _abi.lib().am1gpu_set_timing(1 if enable else 0)
+
+
+class ResidentBatch:
+    """``am1gpu_batch_*``: molecules uploaded once, the SCF re-run on device-resident inputs."""
+
+    def __init__(self, mols, method="am1", want_matrices=False, **opts):
+        self.host = Batch(mols, method, want_matrices)
+        self.opts = _abi.default_options(method=method, **opts)
+        self.handle = ctypes.c_void_p()
+        _check(_abi.lib().am1gpu_batch_create(len(self.host.mbs), self.host.arr, ctypes.byref(self.opts),
+                                              ctypes.byref(self.handle)))
+
+    def run(self) -> None:
+        _check(_abi.lib().am1gpu_batch_run(self.handle))
+
+    def stats(self) -> dict:
+        st = _abi.CallStats()
+        _check(_abi.lib().am1gpu_batch_stats(self.handle, ctypes.byref(st)))
+        return _abi.stats_dict(st)
+
+    def results(self) -> tuple[list[int], list[dict]]:
+        _abi.lib().am1gpu_batch_results(self.handle, self.host.res, self.host.status)
+        return list(self.host.status), self.host.results()
+
+    def close(self) -> None:
+        if self.handle:
+            _abi.lib().am1gpu_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def scf_batch(mols, want_matrices=False, **opts):

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -57,7 +59,11 @@ struct DeviceCtx {
     std::string err;
     DevElem* d_params = nullptr;
     int sms = 0;
+    int jacobi_smem = 0;  // dynamic shared memory available to one eigensolver CTA
 };
+
+// Shared-memory budget the planner sizes eigensolver clusters for (set when a device is opened).
+int g_jacobi_budget = 232448 - 1024;
 
 DeviceCtx g_dev[64];
 
@@ -78,39 +84,43 @@ int device_ctx(DeviceCtx** out) {
         if ((err = cudaMalloc(&c.d_params, bytes)) != cudaSuccess) return bad("cudaMalloc params", err);
         if ((err = cudaMemcpy(c.d_params, host_param_table(), bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
             return bad("upload params", err);
-        if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448)) != cudaSuccess)
+        // dynamic shared memory of the eigensolver: the opt-in limit minus its static shared memory
+        int optin = 0;
+        if ((err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+            return bad("smem attr", err);
+        cudaFuncAttributes fa{};
+        if ((err = cudaFuncGetAttributes(&fa, k_jacobi)) != cudaSuccess) return bad("jacobi attributes", err);
+        c.jacobi_smem = optin - (int)fa.sharedSizeBytes;
+        if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, c.jacobi_smem)) != cudaSuccess)
             return bad("jacobi smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("jacobi cluster attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
+    g_jacobi_budget = c.jacobi_smem;
     *out = &c;
     return AM1GPU_OK;
 }
 
 // ---------------------------------------------------------------------------------------
-// Per-host-thread workspace: stream, grow-only device pool and pinned staging
+// Device memory: a grow-only device pool + pinned host staging + a stream.  One per host
+// thread (the ABI calls) and one per resident batch handle.
 // ---------------------------------------------------------------------------------------
-struct Workspace {
+struct Mem {
     int dev = -1;
     cudaStream_t stream = nullptr;
     char* dpool = nullptr;
     size_t dcap = 0;
     char* hpin = nullptr;
     size_t hcap = 0;
-    ~Workspace() {
-        // process exit: the driver frees everything with the context
-    }
+    std::vector<cudaEvent_t> events;  // timing events, reused across calls
 };
 
-thread_local Workspace tl_ws;
-
-int workspace(Workspace** out, size_t dbytes, size_t hbytes) {
-    Workspace& w = tl_ws;
+int mem_ensure(Mem& w, size_t dbytes, size_t hbytes) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
-    if (w.dev != dev) {  // first use on this device from this thread
-        w = Workspace();
+    if (w.dev != dev) {  // first use on this device
+        w = Mem();
         w.dev = dev;
         CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
     }
@@ -128,9 +138,97 @@ int workspace(Workspace** out, size_t dbytes, size_t hbytes) {
         CK(cudaMallocHost(&w.hpin, hbytes));
         w.hcap = hbytes;
     }
-    *out = &w;
     return AM1GPU_OK;
 }
+
+void mem_release(Mem& w) {
+    if (w.dpool) cudaFree(w.dpool);
+    if (w.hpin) cudaFreeHost(w.hpin);
+    for (auto e : w.events) cudaEventDestroy(e);
+    if (w.stream) cudaStreamDestroy(w.stream);
+    w = Mem();
+}
+
+thread_local Mem tl_mem;
+using Workspace = Mem;
+
+int workspace(Workspace** out, size_t dbytes, size_t hbytes) {
+    int rc = mem_ensure(tl_mem, dbytes, hbytes);
+    if (rc) return rc;
+    *out = &tl_mem;
+    return AM1GPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Call statistics and phase timing (the reference's AM1_TIMING phases, src/timing.rs)
+// ---------------------------------------------------------------------------------------
+std::atomic<int> g_timing{-1};  // -1: read AM1_TIMING on first use
+
+bool timing_on() {
+    int t = g_timing.load();
+    if (t < 0) {
+        const char* e = std::getenv("AM1_TIMING");
+        t = (e && *e && std::strcmp(e, "0") != 0) ? 1 : 0;
+        g_timing.store(t);
+    }
+    return t == 1;
+}
+
+thread_local am1gpu_call_stats tl_stats;
+
+constexpr int kSp2MaxSteps = 100;
+
+// How the SCF step forms P from F*: 0 purification (default), 1 eigenvectors every iteration.
+// AM1GPU_DENSITY=jacobi selects the eigensolver path (kept for comparison and testing).
+int density_mode() {
+    static const int mode = [] {
+        const char* e = std::getenv("AM1GPU_DENSITY");
+        return (e && std::strcmp(e, "jacobi") == 0) ? 1 : 0;
+    }();
+    return mode;
+}
+
+struct Run {
+    Mem* mem;
+    am1gpu_call_stats* stats;
+    bool timed;
+    size_t next_ev = 0;
+    std::vector<std::pair<int, std::pair<size_t, size_t>>> spans;  // phase, (start, stop) event slots
+    size_t t0 = 0, t1 = 0;
+
+    int event(size_t* slot) {
+        if (next_ev == mem->events.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            mem->events.push_back(e);
+        }
+        *slot = next_ev++;
+        CK(cudaEventRecord(mem->events[*slot], mem->stream));
+        return AM1GPU_OK;
+    }
+    int begin(size_t* slot) { return timed ? event(slot) : AM1GPU_OK; }
+    int end(int phase, size_t start) {
+        if (!timed) return AM1GPU_OK;
+        size_t stop;
+        int rc = event(&stop);
+        if (rc) return rc;
+        spans.push_back({phase, {start, stop}});
+        return AM1GPU_OK;
+    }
+    void launched(int phase, int k = 1) {
+        stats->kernel_launches += k;
+        stats->phase_launches[phase] += k;
+    }
+    // after the stream has been synchronized
+    int collect() {
+        for (auto& sp : spans) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, mem->events[sp.second.first], mem->events[sp.second.second]));
+            stats->phase_ms[sp.first] += ms;
+        }
+        return AM1GPU_OK;
+    }
+};
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -151,7 +249,7 @@ int choose_cluster(int n, int* npad_out, int* c_out) {
         const int npad = ((std::max(n, 2) + 2 * C - 1) / (2 * C)) * (2 * C);
         const int q = npad / 2 / C;
         if (C > 1 && q < 2) continue;
-        if (jacobi_smem_bytes(n, npad, C) <= 232448 - 1024) {  // leave room for static shared memory
+        if ((long long)jacobi_smem_bytes(n, npad, C) <= g_jacobi_budget) {
             *npad_out = npad;
             *c_out = C;
             return 1;
@@ -255,6 +353,13 @@ struct Batch {
     int neig = 0;
     struct Bucket { int off, count, C; size_t smem; };
     std::vector<Bucket> buckets;
+    Sp2Job* d_sp2;
+    GemmTile* d_sp2_tiles;
+    int nt_sp2 = 0, sp2_nblk = 1;
+    Sp2State* d_sp2_state;
+    TriJob* d_tri;
+    int* d_need_eigen;
+    int* d_sp2_active;
     MolState* d_st;
     int* d_status;
     double *d_wstore, *d_ecc, *d_arena, *d_res, *d_charges;
@@ -266,11 +371,12 @@ struct Batch {
     int* h_active;
     double* h_res;
     double* h_charges;
+    long long arena_doubles = 0;
 };
 
 // Lays out the batch in one device pool and one pinned staging area, copies inputs.
-int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<MolPlan>&& plans, Batch& b, Workspace** wsp,
-                double spin_scale_override = -1.0) {
+int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<MolPlan>&& plans, Batch& b, Mem& mem,
+                am1gpu_call_stats* stats, double spin_scale_override = -1.0) {
     b.plans = std::move(plans);
     b.nmol = (int)b.plans.size();
     const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
@@ -296,8 +402,13 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.nblk = std::max(1, std::min(32, (maxn + 15) / 16));
     const int nblk = b.nblk;
     // GEMM tile counts
-    int tiles_nn = 0;
-    for (auto& p : b.plans) tiles_nn += p.nch * ((p.nao + 63) / 64) * ((p.nao + 63) / 64);
+    int tiles_nn = 0, tiles_up = 0;
+    for (auto& p : b.plans) {
+        const int tn = (p.nao + 63) / 64;
+        tiles_nn += p.nch * tn * tn;
+        tiles_up += p.nch * tn * (tn + 1) / 2;
+    }
+    const int sp2_nblk = std::max(1, std::min(32, (maxn + 7) / 8));
     // ---- staged (host -> device) region layout
     size_t st = 0;
     auto take = [](size_t& cur, size_t bytes) {
@@ -320,18 +431,28 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_tgt = take(st, sizeof(GemmTile) * tiles_nn);
     const size_t o_tdn = take(st, sizeof(GemmTile) * tiles_nn);
     const size_t o_eig = take(st, sizeof(EigJob) * nch_total);
+    const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
+    const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
+    const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
     const size_t staged = align256(st);
     // ---- device-only region
     size_t dv = staged;
     const size_t o_status = take(dv, sizeof(int) * b.nmol);
+    const size_t o_need = take(dv, sizeof(int) * b.nmol);
+    const size_t o_sp2a = take(dv, sizeof(int) * 4);
+    const size_t o_sp2s = take(dv, sizeof(Sp2State) * nch_total);
     const size_t o_active = take(dv, sizeof(int) * 4);
     const size_t o_w = take(dv, sizeof(double) * std::max<long long>(wsize, 1));
     const size_t o_ecc = take(dv, sizeof(double) * std::max<long long>(npairs, 1));
     const size_t o_arena = take(dv, sizeof(double) * arena);
     const size_t o_hist = take(dv, sizeof(double) * hist);
     long long misc = 0;
-    for (auto& p : b.plans) misc += p.nch * (2LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + 64);
+    for (auto& p : b.plans) {
+        const long long tn = (p.nao + 63) / 64;
+        const long long sp2part = 2 * std::max<long long>(sp2_nblk, tn * (tn + 1) / 2);
+        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + 96);
+    }
     const size_t o_misc = take(dv, sizeof(double) * misc);
     const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
     const size_t o_res = take(dv, sizeof(double) * RES_N * b.nmol);
@@ -342,10 +463,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t h_o_active = take(hs, sizeof(int) * 4);
     const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
-    Workspace* ws;
-    int rc = workspace(&ws, dtotal, align256(hs));
+    int rc = mem_ensure(mem, dtotal, align256(hs));
     if (rc) return rc;
-    *wsp = ws;
+    Mem* ws = &mem;
     char* D = ws->dpool;
     char* Hs = ws->hpin;
     auto dptr = [D](size_t off) { return (void*)(D + off); };
@@ -363,6 +483,13 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_gt_gt = (GemmTile*)dptr(o_tgt);
     b.d_gt_dn = (GemmTile*)dptr(o_tdn);
     b.d_eig = (EigJob*)dptr(o_eig);
+    b.d_sp2 = (Sp2Job*)dptr(o_sp2);
+    b.d_sp2_tiles = (GemmTile*)dptr(o_sp2t);
+    b.d_tri = (TriJob*)dptr(o_tri);
+    b.d_need_eigen = (int*)dptr(o_need);
+    b.d_sp2_active = (int*)dptr(o_sp2a);
+    b.d_sp2_state = (Sp2State*)dptr(o_sp2s);
+    b.sp2_nblk = sp2_nblk;
     b.d_st = (MolState*)dptr(o_st);
     b.d_status = (int*)dptr(o_status);
     b.d_active = (int*)dptr(o_active);
@@ -392,6 +519,10 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     GemmTile* htgt = (GemmTile*)(Hs + o_tgt);
     GemmTile* htdn = (GemmTile*)(Hs + o_tdn);
     EigJob* heig = (EigJob*)(Hs + o_eig);
+    Sp2Job* hsp2 = (Sp2Job*)(Hs + o_sp2);
+    GemmTile* hsp2t = (GemmTile*)(Hs + o_sp2t);
+    TriJob* htri = (TriJob*)(Hs + o_tri);
+    int nsp2t = 0;
     MolState* hst = (MolState*)(Hs + o_st);
     long long a_off = 0, w_off = 0, ar_off = 0, hi_off = 0, mi_off = 0;
     int atom_base = 0, job = 0, ntile = 0, cid_off = 0;
@@ -460,8 +591,17 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             hi_off = (hi_off + 31) & ~31LL;
             cj.rowmin = d_misc + mi_off;
             mi_off += n;
+            cj.rowmax = d_misc + mi_off;
+            mi_off += n;
             cj.eps = d_misc + mi_off;
             mi_off += n;
+            double* tri_d = d_misc + mi_off;
+            mi_off += n;
+            double* tri_e = d_misc + mi_off;
+            mi_off += n;
+            const long long tn_ = (n + 63) / 64;
+            double* sp2part = d_misc + mi_off;
+            mi_off += 2 * std::max<long long>(sp2_nblk, tn_ * (tn_ + 1) / 2);
             double* lam = d_misc + mi_off;
             mi_off += p.npad;
             cj.red = d_misc + mi_off;
@@ -470,6 +610,32 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             mi_off += nblk;
             mi_off = (mi_off + 31) & ~31LL;
             hj[job] = cj;
+            Sp2Job sj{};
+            sj.F = cj.FP;
+            sj.rowmin = cj.rowmin;
+            sj.rowmax = cj.rowmax;
+            sj.X0 = base + SLOT_GT * nn;
+            sj.X1 = base + SLOT_VS * nn;
+            sj.P = cj.Pnew;
+            sj.part = sp2part;
+            sj.nocc = (double)p.n_occ[c];
+            sj.weight = md.occ_weight;
+            sj.n = (int)n;
+            sj.mol = mi;
+            sj.tile0 = nsp2t;
+            for (int x = 0; x < (int)tn_; ++x)
+                for (int y = x; y < (int)tn_; ++y) hsp2t[nsp2t++] = GemmTile{job, x, y};
+            sj.ntiles = nsp2t - sj.tile0;
+            hsp2[job] = sj;
+            TriJob tj{};
+            tj.A = cj.FP;
+            tj.W = base + SLOT_VS * nn;
+            tj.d = tri_d;
+            tj.e = tri_e;
+            tj.eps = cj.eps;
+            tj.n = (int)n;
+            tj.mol = mi;
+            htri[job] = tj;
             // GEMMs: F.P, C^T F*, w C_occ^T C_occ
             hgfp[job] = GemmJob{cj.F, cj.P, cj.FP, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
             hggt[job] = GemmJob{cj.Ct, cj.FP, base + SLOT_GT * nn, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
@@ -509,6 +675,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     }
     hpp[b.nmol] = a_off;
     b.nt_fp = b.nt_gt = b.nt_dn = ntile;
+    b.nt_sp2 = nsp2t;
     // eigen jobs grouped by cluster size, largest first inside a group
     std::vector<int> idx(eig_all.size());
     for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
@@ -529,7 +696,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.mols.assign(hm, hm + b.nmol);
     b.jobs.assign(hj, hj + job);
     b.job0.assign(hj0, hj0 + b.nmol);
+    b.arena_doubles = arena;
     CK(cudaMemcpyAsync(D, Hs, staged, cudaMemcpyHostToDevice, ws->stream));
+    if (stats) stats->h2d_bytes += (int64_t)staged;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, ws->stream));
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * arena, ws->stream));
     return AM1GPU_OK;
@@ -537,19 +706,26 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
 
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
-int launch_core(Batch& b, Workspace* ws, const DevElem* dp) {
+int launch_core(Batch& b, Mem* ws, const DevElem* dp, Run* run) {
     cudaStream_t s = ws->stream;
-    if (b.npairs > 0)
+    int k = 0;
+    if (b.npairs > 0) {
         k_pair_integrals<<<cdiv(b.npairs, 128), 128, 0, s>>>(b.d_mols, b.nmol, b.d_pair_prefix, b.npairs, dp, b.d_atom_z,
                                                             b.d_atom_xyz, b.d_wstore, b.d_arena, b.d_ecc, b.d_status);
-    if (b.natoms > 0)
+        ++k;
+    }
+    if (b.natoms > 0) {
         k_core_diag<<<cdiv(b.natoms, 128), 128, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena);
+        ++k;
+    }
     k_core_energy<<<b.nmol, 256, 0, s>>>(b.d_mols, b.d_ecc, b.d_st);
+    ++k;
     CK(cudaGetLastError());
+    if (run) run->launched(AM1GPU_PHASE_CORE, k);
     return AM1GPU_OK;
 }
 
-int launch_jacobi(Batch& b, Workspace* ws, int force) {
+int launch_jacobi(Batch& b, Mem* ws, int force, const int* mask = nullptr) {
     for (auto& bk : b.buckets) {
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(bk.count * bk.C, 1, 1);
@@ -563,19 +739,38 @@ int launch_jacobi(Batch& b, Workspace* ws, int force) {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CK(cudaLaunchKernelEx(&cfg, k_jacobi, (const EigJob*)(b.d_eig + bk.off), (const MolState*)b.d_st, b.d_status, force));
+        CK(cudaLaunchKernelEx(&cfg, k_jacobi, (const EigJob*)(b.d_eig + bk.off), (const MolState*)b.d_st, b.d_status, force,
+                              mask));
     }
     return AM1GPU_OK;
 }
 
-int run_scf(Batch& b, Workspace* ws, const DevElem* dp, const am1gpu_options& o) {
+// The whole solve on the device: state reset, integrals, SCF iterations, final energy and the
+// result records.  Inputs must already be resident (build_batch); nothing but the count of
+// molecules still iterating is read back.
+int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, am1gpu_call_stats* stats) {
+    Mem* ws = &mem;
     cudaStream_t s = ws->stream;
-    int rc = launch_core(b, ws, dp);
+    Run run{ws, stats, timing_on()};
+    int rc;
+    size_t t0, ph;
+    if ((rc = run.event(&t0))) return rc;
+    if ((rc = run.begin(&ph))) return rc;
+    CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, s));
+    CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * b.arena_doubles, s));
+    k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.nmol);
+    run.launched(AM1GPU_PHASE_CORE);
+    rc = launch_core(b, ws, dp, &run);
     if (rc) return rc;
     const int njobs = (int)b.jobs.size();
-    if (b.natoms > 0) k_sad_init<<<cdiv(b.natoms, 128), 128, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_arena);
+    if (b.natoms > 0) {
+        k_sad_init<<<cdiv(b.natoms, 128), 128, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_arena);
+        run.launched(AM1GPU_PHASE_CORE);
+    }
     k_identity<<<dim3(cdiv(b.maxn, 256), njobs), 256, 0, s>>>(b.d_jobs);
+    run.launched(AM1GPU_PHASE_CORE);
     CK(cudaGetLastError());
+    if ((rc = run.end(AM1GPU_PHASE_CORE, ph))) return rc;
     ScfParams prm{o.max_scf, o.use_diis, o.accelerator, o.e_tol, o.p_tol, o.adiis_switch};
     const int nblk = b.nblk;
     const int rowblk = std::max(1, std::min(64, (b.maxn + 7) / 8));
@@ -584,49 +779,122 @@ int run_scf(Batch& b, Workspace* ws, const DevElem* dp, const am1gpu_options& o)
     while (done < o.max_scf) {
         for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
             CK(cudaMemsetAsync(b.d_active, 0, sizeof(int), s));
+            if ((rc = run.begin(&ph))) return rc;
             k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena,
                                                       b.d_st, 0);
-            k_gemm_nn<<<b.nt_fp, 256, 0, s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0);
+            run.launched(AM1GPU_PHASE_FOCK);
+            if ((rc = run.end(AM1GPU_PHASE_FOCK, ph)) || (rc = run.begin(&ph))) return rc;
+            k_gemm_nn<<<b.nt_fp, 256, 0, s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0, nullptr);
             k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
+            run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
+            if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, ph)) || (rc = run.begin(&ph))) return rc;
             k_diis_solve<<<cdiv(b.nmol, 64), 64, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm);
             k_combine<<<dim3(rowblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, 0);
-            k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0);
-            CK(cudaGetLastError());
-            rc = launch_jacobi(b, ws, 0);
-            if (rc) return rc;
-            k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0);
-            k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0);
+            run.launched(AM1GPU_PHASE_ACCEL, 2);
+            if ((rc = run.end(AM1GPU_PHASE_ACCEL, ph)) || (rc = run.begin(&ph))) return rc;
+            if (density_mode() == 0) {
+                // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
+                k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
+                k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
+                CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
+                run.launched(AM1GPU_PHASE_EIGEN, 2);
+                for (int step = 0; step < kSp2MaxSteps; ++step) {
+                    k_sp2_step<<<b.nt_sp2, 128, 0, s>>>(b.d_sp2, b.d_sp2_tiles, b.nt_sp2, b.d_sp2_state);
+                    CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
+                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, kSp2MaxSteps, b.d_sp2_active);
+                    run.launched(AM1GPU_PHASE_EIGEN, 2);
+                    if (step >= 12 && (step % 6) == 5) {
+                        CK(cudaMemcpyAsync(b.h_active + 1, b.d_sp2_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+                        CK(cudaStreamSynchronize(s));
+                        if (b.h_active[1] == 0) break;
+                    }
+                }
+                k_sp2_finish<<<dim3(8, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen);
+                run.launched(AM1GPU_PHASE_EIGEN);
+                // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
+                k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
+                size_t pj;
+                if ((rc = run.begin(&pj))) return rc;
+                if ((rc = launch_jacobi(b, ws, 0, b.d_need_eigen))) return rc;
+                run.launched(AM1GPU_PHASE_JACOBI, (int)b.buckets.size());
+                if ((rc = run.end(AM1GPU_PHASE_JACOBI, pj))) return rc;
+                k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
+                k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
+                run.launched(AM1GPU_PHASE_EIGEN, 3);
+                if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
+            } else {
+                k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, nullptr);
+                CK(cudaGetLastError());
+                size_t pj;
+                if ((rc = run.begin(&pj))) return rc;
+                if ((rc = launch_jacobi(b, ws, 0))) return rc;
+                run.launched(AM1GPU_PHASE_JACOBI, (int)b.buckets.size());
+                if ((rc = run.end(AM1GPU_PHASE_JACOBI, pj))) return rc;
+                k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
+                run.launched(AM1GPU_PHASE_EIGEN, 2);
+                if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
+                k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, nullptr);
+                run.launched(AM1GPU_PHASE_DENSITY);
+            }
             k_density_post<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, nblk);
             k_converge<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm,
                                                          b.d_active);
+            run.launched(AM1GPU_PHASE_DENSITY, 2);
+            if ((rc = run.end(AM1GPU_PHASE_DENSITY, ph))) return rc;
             CK(cudaGetLastError());
         }
         CK(cudaMemcpyAsync(b.h_active, b.d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         if (*b.h_active == 0) break;
     }
-    // final energy at the final density (src/scf.rs:698-701, 835-839)
+    stats->scf_cycles = done;
+    // final energy at the final density (src/scf.rs:698-701, 835-839) and the result records
+    if ((rc = run.begin(&ph))) return rc;
     k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena, b.d_st, 1);
     k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 1, 1);
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
+    // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
+    k_tridiag<<<njobs, 256, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);
+    k_bisect<<<njobs, 128, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
+    run.launched(AM1GPU_PHASE_FINAL, 6);
     CK(cudaGetLastError());
+    if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
+    size_t t1;
+    if ((rc = run.event(&t1))) return rc;
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, mem.events[t0], mem.events[t1]));
+    stats->device_ms += ms;
+    return run.collect();
+}
+
+int fetch_results(Batch& b, Mem& mem, am1gpu_call_stats* stats) {
+    cudaStream_t s = mem.stream;
     CK(cudaMemcpyAsync(b.h_res, b.d_res, sizeof(double) * RES_N * b.nmol, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(b.h_charges, b.d_charges, sizeof(double) * std::max(b.natoms, 1), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    stats->d2h_bytes += (int64_t)(sizeof(double) * RES_N * b.nmol + sizeof(double) * std::max(b.natoms, 1));
     return AM1GPU_OK;
 }
 
 // Copies one device matrix (internal AO order) out to the caller's order.
-int fetch_matrix(Workspace* ws, const double* dsrc, int n, std::vector<double>& tmp) {
+int fetch_matrix(Mem* ws, const double* dsrc, int n, std::vector<double>& tmp, am1gpu_call_stats* stats = nullptr) {
     tmp.resize((size_t)n * n);
     CK(cudaMemcpyAsync(tmp.data(), dsrc, sizeof(double) * n * n, cudaMemcpyDeviceToHost, ws->stream));
     CK(cudaStreamSynchronize(ws->stream));
+    if (stats) stats->d2h_bytes += (int64_t)sizeof(double) * n * n;
     return AM1GPU_OK;
 }
 
-int write_result(Batch& b, Workspace* ws, int mi, am1gpu_result* r) {
+}  // namespace
+int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_override);
+namespace {
+thread_local Mem tl_mem_eig;  // on-demand eigenvectors: separate from the batch's memory
+int density_mode();
+
+int write_result(Batch& b, Mem* ws, int mi, am1gpu_result* r, am1gpu_call_stats* stats) {
     const MolPlan& p = b.plans[mi];
     const double* rec = b.h_res + (size_t)mi * RES_N;
     r->electronic_ev = rec[RES_ELEC];
@@ -654,10 +922,10 @@ int write_result(Batch& b, Workspace* ws, int mi, am1gpu_result* r) {
     std::vector<double> t0, t1;
     const ChanJob& j0 = b.jobs[b.job0[mi]];
     if (r->density || r->spin_density) {
-        int rc = fetch_matrix(ws, j0.P, n, t0);
+        int rc = fetch_matrix(ws, j0.P, n, t0, stats);
         if (rc) return rc;
         if (p.nch == 2) {
-            rc = fetch_matrix(ws, b.jobs[b.job0[mi] + 1].P, n, t1);
+            rc = fetch_matrix(ws, b.jobs[b.job0[mi] + 1].P, n, t1, stats);
             if (rc) return rc;
         }
         for (int i = 0; i < n; ++i)
@@ -674,12 +942,24 @@ int write_result(Batch& b, Workspace* ws, int mi, am1gpu_result* r) {
         if (e_out) {
             CK(cudaMemcpyAsync(e_out, jc.eps, sizeof(double) * n, cudaMemcpyDeviceToHost, ws->stream));
             CK(cudaStreamSynchronize(ws->stream));
+            stats->d2h_bytes += (int64_t)sizeof(double) * n;
         }
         if (c_out) {
-            int rc = fetch_matrix(ws, jc.Ct, n, t0);
-            if (rc) return rc;
-            for (int k = 0; k < n; ++k)
-                for (int mu = 0; mu < n; ++mu) c_out[(size_t)map[mu] * n + k] = t0[(size_t)k * n + mu];
+            if (density_mode() == 0) {
+                // the purification path has no eigenvectors: diagonalise the last F* now
+                int rc = fetch_matrix(ws, jc.FP, n, t0, stats);
+                if (rc) return rc;
+                std::vector<double> wv(n), vv((size_t)n * n);
+                rc = symmetric_eigen_one(n, t0.data(), wv.data(), vv.data(), &tl_mem_eig);
+                if (rc) return rc;
+                for (int mu = 0; mu < n; ++mu)
+                    for (int k = 0; k < n; ++k) c_out[(size_t)map[mu] * n + k] = vv[(size_t)mu * n + k];
+            } else {
+                int rc = fetch_matrix(ws, jc.Ct, n, t0, stats);
+                if (rc) return rc;
+                for (int k = 0; k < n; ++k)
+                    for (int mu = 0; mu < n; ++mu) c_out[(size_t)map[mu] * n + k] = t0[(size_t)k * n + mu];
+            }
         }
     }
     const int status = (int)rec[RES_STATUS];
@@ -712,6 +992,7 @@ void fill_empty(am1gpu_result* r) {
 
 int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* res, int* status) {
     g_err.clear();
+    tl_stats = am1gpu_call_stats{};
     if (nmol < 0 || (nmol > 0 && (!mols || !res)) || !opts) return fail(AM1GPU_INVALID_INPUT, "null argument");
     DeviceCtx* ctx;
     int rc = device_ctx(&ctx);
@@ -741,8 +1022,10 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
     if (!plans.empty()) {
         Batch b;
         Workspace* ws;
-        rc = build_batch(mols, *opts, std::move(plans), b, &ws);
-        if (!rc) rc = run_scf(b, ws, ctx->d_params, *opts);
+        rc = workspace(&ws, 0, 0);
+        if (!rc) rc = build_batch(mols, *opts, std::move(plans), b, *ws, &tl_stats);
+        if (!rc) rc = run_device(b, *ws, ctx->d_params, *opts, &tl_stats);
+        if (!rc) rc = fetch_results(b, *ws, &tl_stats);
         if (rc) {
             for (auto& p : b.plans)
                 if (status) status[p.user] = rc;
@@ -750,7 +1033,7 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
         }
         for (int mi = 0; mi < b.nmol; ++mi) {
             const int u = b.plans[mi].user;
-            int r = write_result(b, ws, mi, &res[u]);
+            int r = write_result(b, ws, mi, &res[u], &tl_stats);
             if (status) status[u] = r;
             if (r && !first) {
                 first = r;
@@ -786,9 +1069,11 @@ int build_core_one(const am1gpu_molecule* mol, int method, double* h_core, doubl
     std::vector<MolPlan> plans{std::move(p)};
     Batch b;
     Workspace* ws;
-    rc = build_batch(&m, o, std::move(plans), b, &ws);
+    tl_stats = am1gpu_call_stats{};
+    rc = workspace(&ws, 0, 0);
+    if (!rc) rc = build_batch(&m, o, std::move(plans), b, *ws, &tl_stats);
     if (rc) return rc;
-    rc = launch_core(b, ws, ctx->d_params);
+    rc = launch_core(b, ws, ctx->d_params, nullptr);
     if (rc) return rc;
     MolState st;
     CK(cudaMemcpyAsync(&st, b.d_st, sizeof(MolState), cudaMemcpyDeviceToHost, ws->stream));
@@ -827,9 +1112,11 @@ int build_fock_one(const am1gpu_molecule* mol, int method, const double* p_tot, 
     std::vector<MolPlan> plans{std::move(p)};
     Batch b;
     Workspace* ws;
-    rc = build_batch(&m, o, std::move(plans), b, &ws, spin_scale);
+    tl_stats = am1gpu_call_stats{};
+    rc = workspace(&ws, 0, 0);
+    if (!rc) rc = build_batch(&m, o, std::move(plans), b, *ws, &tl_stats, spin_scale);
     if (rc) return rc;
-    rc = launch_core(b, ws, ctx->d_params);
+    rc = launch_core(b, ws, ctx->d_params, nullptr);
     if (rc) return rc;
     const int n = b.plans[0].nao;
     const auto& map = b.plans[0].ao_map;
@@ -853,7 +1140,7 @@ int build_fock_one(const am1gpu_molecule* mol, int method, const double* p_tot, 
     return AM1GPU_OK;
 }
 
-int symmetric_eigen_one(int n, const double* a, double* w, double* v) {
+int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_override = nullptr) {
     g_err.clear();
     if (n < 0 || (n > 0 && (!a || !w || !v))) return fail(AM1GPU_INVALID_INPUT, "null argument");
     if (n == 0) return AM1GPU_OK;
@@ -882,7 +1169,12 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v) {
                  o_id = take(npad * 4), o_e = take(n * 8), o_r = take(n * 8), o_st = take(sizeof(MolState)),
                  o_status = take(16), o_job = take(sizeof(EigJob));
     Workspace* ws;
-    rc = workspace(&ws, align256(off), align256(off));
+    if (mem_override) {
+        rc = mem_ensure(*mem_override, align256(off), align256(off));
+        ws = mem_override;
+    } else {
+        rc = workspace(&ws, align256(off), align256(off));
+    }
     if (rc) return rc;
     char* D = ws->dpool;
     char* Hh = ws->hpin;
@@ -925,7 +1217,7 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v) {
     b.neig = 1;
     rc = launch_jacobi(b, ws, 1);
     if (rc) return rc;
-    k_eig_sort<<<1, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1);
+    k_eig_sort<<<1, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1, nullptr);
     CK(cudaGetLastError());
     std::vector<double> ct(nn);
     int st = 0;
@@ -940,6 +1232,19 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v) {
 }
 
 }  // namespace am1
+
+// A resident batch: inputs uploaded once, device memory and stream owned by the handle.
+struct am1gpu_batch {
+    am1::Mem mem;
+    am1::Batch b;
+    am1gpu_options opts;
+    std::vector<int> status;   // validation result per caller molecule
+    std::vector<int> planned;  // caller index -> batch index, or -1
+    int nmol = 0;
+    am1gpu_call_stats stats{};
+    const am1::DevElem* dp = nullptr;
+    bool ran = false;
+};
 
 // ---------------------------------------------------------------------------------------
 // C ABI
@@ -996,5 +1301,97 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {
 }
 
 const char* am1gpu_last_error(void) { return am1::g_err.c_str(); }
+
+int am1gpu_batch_create(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_batch** out) {
+    using namespace am1;
+    g_err.clear();
+    if (!out || !opts || nmol < 0 || (nmol > 0 && !mols)) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    *out = nullptr;
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    auto* h = new am1gpu_batch();
+    h->opts = *opts;
+    h->nmol = nmol;
+    h->status.assign(nmol, AM1GPU_OK);
+    h->planned.assign(nmol, -1);
+    h->dp = ctx->d_params;
+    std::vector<MolPlan> plans;
+    for (int i = 0; i < nmol; ++i) {
+        MolPlan p;
+        const int r = plan_molecule(mols[i], *opts, i, p);
+        h->status[i] = r;
+        if (r == AM1GPU_OK) {
+            h->planned[i] = (int)plans.size();
+            plans.push_back(std::move(p));
+        }
+    }
+    if (!plans.empty()) {
+        rc = build_batch(mols, *opts, std::move(plans), h->b, h->mem, &h->stats);
+        if (!rc && cudaStreamSynchronize(h->mem.stream) != cudaSuccess) rc = fail(AM1GPU_DEVICE_ERROR, "upload failed");
+        if (rc) {
+            mem_release(h->mem);
+            delete h;
+            return rc;
+        }
+    }
+    *out = h;
+    return AM1GPU_OK;
+}
+
+int am1gpu_batch_run(am1gpu_batch* h) {
+    using namespace am1;
+    g_err.clear();
+    if (!h) return fail(AM1GPU_INVALID_INPUT, "null batch");
+    h->stats = am1gpu_call_stats{};
+    if (h->b.nmol == 0) return AM1GPU_OK;
+    int rc = run_device(h->b, h->mem, h->dp, h->opts, &h->stats);
+    tl_stats = h->stats;
+    h->ran = rc == AM1GPU_OK;
+    return rc;
+}
+
+int am1gpu_batch_results(am1gpu_batch* h, am1gpu_result* results, int32_t* status) {
+    using namespace am1;
+    g_err.clear();
+    if (!h || (h->nmol > 0 && !results)) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (h->b.nmol > 0 && !h->ran) return fail(AM1GPU_INVALID_INPUT, "am1gpu_batch_run has not completed");
+    int rc = h->b.nmol > 0 ? fetch_results(h->b, h->mem, &h->stats) : AM1GPU_OK;
+    if (rc) return rc;
+    int first = AM1GPU_OK;
+    std::string msg;
+    for (int i = 0; i < h->nmol; ++i) {
+        int r = h->status[i];
+        if (r == AM1GPU_OK) r = write_result(h->b, &h->mem, h->planned[i], &results[i], &h->stats);
+        if (status) status[i] = r;
+        if (r && !first) {
+            first = r;
+            msg = g_err;
+        }
+    }
+    tl_stats = h->stats;
+    if (first) g_err = msg;
+    return first;
+}
+
+void am1gpu_batch_destroy(am1gpu_batch* h) {
+    if (!h) return;
+    am1::mem_release(h->mem);
+    delete h;
+}
+
+void am1gpu_set_timing(int32_t enable) { am1::g_timing.store(enable ? 1 : 0); }
+
+int am1gpu_last_call_stats(am1gpu_call_stats* out) {
+    if (!out) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    *out = am1::tl_stats;
+    return AM1GPU_OK;
+}
+
+int am1gpu_batch_stats(const am1gpu_batch* h, am1gpu_call_stats* out) {
+    if (!h || !out) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    *out = h->stats;
+    return AM1GPU_OK;
+}
 
 }  // extern "C"

@@ -32,7 +32,7 @@ constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
 
 template <bool TA>
 __device__ __forceinline__ void gemm_tile(const GemmJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
-                                          const MolState* __restrict__ st, int force) {
+                                          const MolState* __restrict__ st, int force, const int* __restrict__ mask) {
     __shared__ double As[GB_K][GB_M + 1];
     __shared__ double Bs[GB_K][GB_N + 1];
     const int t = blockIdx.x;
@@ -40,6 +40,7 @@ __device__ __forceinline__ void gemm_tile(const GemmJob* __restrict__ jobs, cons
     const GemmTile tl = tiles[t];
     const GemmJob jb = jobs[tl.job];
     if (!force && !st[jb.mol].active) return;
+    if (mask && !mask[jb.mol]) return;
     const int m0 = tl.tm * GB_M, n0 = tl.tn * GB_N;
     const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
     double acc[4][4];
@@ -92,13 +93,13 @@ __device__ __forceinline__ void gemm_tile(const GemmJob* __restrict__ jobs, cons
 }
 
 __global__ void __launch_bounds__(256) k_gemm_nn(const GemmJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                 int ntiles, const MolState* __restrict__ st, int force) {
-    gemm_tile<false>(jobs, tiles, ntiles, st, force);
+                                                 int ntiles, const MolState* __restrict__ st, int force, const int* __restrict__ mask) {
+    gemm_tile<false>(jobs, tiles, ntiles, st, force, mask);
 }
 
 __global__ void __launch_bounds__(256) k_gemm_tn(const GemmJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                 int ntiles, const MolState* __restrict__ st, int force) {
-    gemm_tile<true>(jobs, tiles, ntiles, st, force);
+                                                 int ntiles, const MolState* __restrict__ st, int force, const int* __restrict__ mask) {
+    gemm_tile<true>(jobs, tiles, ntiles, st, force, mask);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -144,13 +145,14 @@ constexpr int JAC_MAX_SWEEPS = 60;
 
 // Shared memory: nbuf = 2q + 2 buffers of 2n doubles ([g | v]), then int metadata.
 __global__ void __launch_bounds__(JAC_THREADS) k_jacobi(const EigJob* __restrict__ jobs, const MolState* __restrict__ st,
-                                                        int* __restrict__ mol_status, int force) {
+                                                        int* __restrict__ mol_status, int force, const int* __restrict__ mask) {
     extern __shared__ double smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
     const int crank = (int)cluster.block_rank();
     const EigJob jb = jobs[blockIdx.x / C];
     if (!force && !st[jb.mol].active) return;  // uniform over the cluster
+    if (mask && !mask[jb.mol]) return;
     const int n = jb.n, npad = jb.npad, m = npad / 2, q = m / C;
     const int nbuf = 2 * q + 2;
     const int LAND_TOP = 2 * q, LAND_BOT = 2 * q + 1;
@@ -368,9 +370,11 @@ __global__ void __launch_bounds__(JAC_THREADS) k_jacobi(const EigJob* __restrict
 // ---------------------------------------------------------------------------------------
 // Sort eigenpairs ascending (bitonic sort of up to 1024 keys per job) and gather rows.
 // ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_eig_sort(const EigJob* __restrict__ jobs, const MolState* __restrict__ st, int force) {
+__global__ void __launch_bounds__(512) k_eig_sort(const EigJob* __restrict__ jobs, const MolState* __restrict__ st, int force,
+                                                  const int* __restrict__ mask) {
     const EigJob jb = jobs[blockIdx.x];
     if (!force && !st[jb.mol].active) return;
+    if (mask && !mask[jb.mol]) return;
     __shared__ double key[1024];
     __shared__ int val[1024];
     int P2 = 1;

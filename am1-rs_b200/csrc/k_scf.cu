@@ -49,6 +49,16 @@ __global__ void k_sad_init(const MolDesc* __restrict__ mols, const int* __restri
     }
 }
 
+// Fresh SCF state for every molecule of a batch (each run starts from the SAD guess).
+__global__ void k_state_init(MolState* __restrict__ st, int nmol) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nmol) return;
+    MolState s{};
+    s.active = 1;
+    s.residual = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    st[i] = s;
+}
+
 // Identity warm start for the eigensolver (C^T = I; the slot is zero-filled beforehand).
 __global__ void k_identity(const ChanJob* __restrict__ jobs) {
     const ChanJob jb = jobs[blockIdx.y];
@@ -353,7 +363,10 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
             bound += __shfl_xor_sync(0xffffffffu, bound, o);
             diag += __shfl_xor_sync(0xffffffffu, diag, o);
         }
-        if (lane == 0) jb.rowmin[r] = diag - bound;
+        if (lane == 0) {
+            jb.rowmin[r] = diag - bound;
+            jb.rowmax[r] = diag + bound;
+        }
     }
 }
 

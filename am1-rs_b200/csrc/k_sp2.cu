@@ -1,0 +1,262 @@
+// Density matrix of the SCF step by trace-correcting purification (SP2), batched.
+//
+// The SCF needs only P = w * (projector onto the n_occ lowest eigenvectors of F*), which is what
+// am1-rs builds from the eigenvectors (src/scf.rs:654-661: symmetric_eigen then
+// density_from_coeff).  SP2 (Niklasson, Phys. Rev. B 66, 155115 (2002)) reaches the same
+// projector with matrix products only:
+//     X0 = (e_max I - F*) / (e_max - e_min)         (Gershgorin bounds, spectrum mapped into [0,1])
+//     X <- X^2  or  X <- 2X - X^2                   (whichever brings tr X closer to n_occ)
+// until X is idempotent to rounding.  Each step is one symmetric FP64 product X.X on the tensor
+// cores (mma.sync m8n8k4 f64), upper-triangle tiles only, mirrored in the epilogue, which also
+// folds in the choice of branch and the tile's share of tr X and ||X||_F^2 (= tr X^2 for the
+// next step's decision).  No eigenvectors, no fine-grained synchronisation: every step is one
+// launch over all (molecule, channel) tiles of the batch.
+#include <cuda_runtime.h>
+
+#include "am1gpu_internal.h"
+#include "kernels.h"
+
+namespace am1 {
+
+constexpr int SP_TILE = 64;
+constexpr int SP_BK = 16;
+constexpr int SP_AS = SP_BK + 4;    // row stride of the A tile (conflict-free 8-byte fragment loads)
+constexpr int SP_BS = SP_TILE + 4;  // row stride of the B tile
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// X0 = (e_max I - F*) / (e_max - e_min); per-block partial sums of tr X0 and ||X0||_F^2.
+__global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, const MolState* __restrict__ st, int nblk) {
+    const Sp2Job jb = jobs[blockIdx.y];
+    if (!st[jb.mol].active) return;
+    const int n = jb.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    __shared__ double red[2][32];
+    // spectral bounds (every block reduces the row bounds itself)
+    double lo = 1e300, hi = -1e300;
+    for (int i = tid; i < n; i += blockDim.x) {
+        lo = fmin(lo, jb.rowmin[i]);
+        hi = fmax(hi, jb.rowmax[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+        red[0][warp] = lo;
+        red[1][warp] = hi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < nw; ++w) {
+            red[0][0] = fmin(red[0][0], red[0][w]);
+            red[1][0] = fmax(red[1][0], red[1][w]);
+        }
+    }
+    __syncthreads();
+    const double emin = red[0][0], emax = red[1][0];
+    const double inv = 1.0 / fmax(emax - emin, 1e-300);
+    __syncthreads();
+    double tr = 0.0, fr = 0.0;
+    for (int r = blockIdx.x * nw + warp; r < n; r += nblk * nw) {
+        const double* Fr = jb.F + (long long)r * n;
+        double* Xr = jb.X0 + (long long)r * n;
+        for (int c = lane; c < n; c += 32) {
+            const double x = ((c == r ? emax : 0.0) - Fr[c]) * inv;
+            Xr[c] = x;
+            fr += x * x;
+            if (c == r) tr += x;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_xor_sync(0xffffffffu, tr, o);
+        fr += __shfl_xor_sync(0xffffffffu, fr, o);
+    }
+    if (lane == 0) {
+        red[0][warp] = tr;
+        red[1][warp] = fr;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < nw; ++w) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        jb.part[2 * blockIdx.x] = a;
+        jb.part[2 * blockIdx.x + 1] = b;
+        if (blockIdx.x == 0) {
+            Sp2State& s = sst[blockIdx.y];
+            s.emin = emin;
+            s.emax = emax;
+        }
+    }
+}
+
+// Reduce the init partials: state of step 0.
+__global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, const MolState* __restrict__ st, int njobs,
+                            int nblk) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const Sp2Job jb = jobs[j];
+    Sp2State& s = sst[j];
+    s.active = st[jb.mol].active;
+    s.steps = 0;
+    s.cur = 0;
+    s.converged = 0;
+    double tr = 0.0, fr = 0.0;
+    for (int b = 0; b < nblk; ++b) {
+        tr += jb.part[2 * b];
+        fr += jb.part[2 * b + 1];
+    }
+    s.trX = tr;
+    s.trX2 = fr;
+    s.idem[0] = s.idem[1] = 1e300;
+    s.square = fabs(fr - jb.nocc) < fabs(2.0 * tr - fr - jb.nocc) ? 1 : 0;
+}
+
+// One SP2 step over all upper-triangle 64x64 tiles of every active channel.
+__global__ void __launch_bounds__(128) k_sp2_step(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
+                                                  const Sp2State* __restrict__ sst) {
+    __shared__ double As[SP_TILE * SP_AS];
+    __shared__ double Bs[SP_BK * SP_BS];
+    __shared__ double red[2][4];
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const Sp2State s = sst[tl.job];
+    if (!s.active) return;
+    const Sp2Job jb = jobs[tl.job];
+    const int n = jb.n;
+    const double* X = s.cur ? jb.X1 : jb.X0;
+    double* Y = s.cur ? jb.X0 : jb.X1;
+    const int m0 = tl.tm * SP_TILE, n0 = tl.tn * SP_TILE;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // warp tile origin inside the CTA tile
+    const int g = lane >> 2, tq = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int k0 = 0; k0 < n; k0 += SP_BK) {
+        // A tile: rows m0.., cols k0.. ; B tile: rows k0.., cols n0..  (X symmetric)
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            const int idx = tid + l * 128;
+            const int ar = idx >> 4, ak = idx & 15;
+            const int gi = m0 + ar, gk = k0 + ak;
+            As[ar * SP_AS + ak] = (gi < n && gk < n) ? X[(long long)gi * n + gk] : 0.0;
+            const int bk = idx >> 6, bc = idx & 63;
+            const int gbk = k0 + bk, gj = n0 + bc;
+            Bs[bk * SP_BS + bc] = (gbk < n && gj < n) ? X[(long long)gbk * n + gj] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < SP_BK; kk += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[(wr + i * 8 + g) * SP_AS + kk + tq];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * SP_BS + wc + j * 8 + g];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+    // epilogue: Y = X^2 or 2X - X^2, mirrored; partial trace / Frobenius sums
+    const bool diag_tile = tl.tm == tl.tn;
+    double tr = 0.0, fr = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int r = m0 + wr + i * 8 + g;
+                const int c = n0 + wc + j * 8 + tq * 2 + e;
+                if (r < n && c < n) {
+                    const double x2 = acc[i][j][e];
+                    const double y = s.square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
+                    Y[(long long)r * n + c] = y;
+                    if (!diag_tile) Y[(long long)c * n + r] = y;
+                    fr += (diag_tile ? 1.0 : 2.0) * y * y;
+                    if (r == c) tr += y;
+                }
+            }
+    for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_xor_sync(0xffffffffu, tr, o);
+        fr += __shfl_xor_sync(0xffffffffu, fr, o);
+    }
+    if (lane == 0) {
+        red[0][warp] = tr;
+        red[1][warp] = fr;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double* p = jb.part + 2 * (t - jb.tile0);
+        p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
+        p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
+    }
+}
+
+// After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
+__global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs, int max_steps,
+                             int* __restrict__ active_count) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    Sp2State& s = sst[j];
+    if (!s.active) return;
+    const Sp2Job jb = jobs[j];
+    double tr = 0.0, fr = 0.0;
+    for (int t = 0; t < jb.ntiles; ++t) {
+        tr += jb.part[2 * t];
+        fr += jb.part[2 * t + 1];
+    }
+    s.cur ^= 1;
+    s.steps += 1;
+    s.trX = tr;
+    s.trX2 = fr;
+    // idempotency error tr X - tr X^2 (sum of x(1-x) over the spectrum, >= 0)
+    const double idem = fabs(tr - fr);
+    const bool floor_reached = idem < 1.0e-6 && idem >= s.idem[0];  // stagnation at the rounding floor
+    s.idem[0] = s.idem[1];
+    s.idem[1] = idem;
+    if (floor_reached || idem < 1.0e-15 * fmax(1.0, (double)jb.n)) {
+        s.active = 0;
+        s.converged = 1;
+        return;
+    }
+    if (s.steps >= max_steps) {
+        s.active = 0;
+        s.converged = 0;
+        return;
+    }
+    s.square = fabs(fr - jb.nocc) < fabs(2.0 * tr - fr - jb.nocc) ? 1 : 0;
+    atomicAdd(active_count, 1);
+}
+
+// P_new = w X (the converged X); molecules whose purification stalled are flagged for the
+// eigensolver path.
+__global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __restrict__ sst, const MolState* __restrict__ st,
+                             int* __restrict__ need_eigen) {
+    const Sp2Job jb = jobs[blockIdx.y];
+    if (!st[jb.mol].active) return;
+    const Sp2State& s = sst[blockIdx.y];
+    if (!s.converged) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) need_eigen[jb.mol] = 1;
+        return;
+    }
+    const double* X = s.cur ? jb.X1 : jb.X0;
+    const long long nn = (long long)jb.n * jb.n;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x)
+        jb.P[i] = jb.weight * X[i];
+}
+
+}  // namespace am1

@@ -48,9 +48,39 @@ struct ChanJob {
     double* hF;       // packed history of F  [8][n(n+1)/2]
     double* hE;       // packed history of [F,P] [8][n(n-1)/2]
     double* hD;       // packed history of P  [8][n(n+1)/2] (A-DIIS) or nullptr
-    double* rowmin;   // n
+    double* rowmin;   // n: Gershgorin lower bound of each row of F*
+    double* rowmax;   // n: Gershgorin upper bound
     double* red;      // per-block partial sums [nblk][RED_N]
     double* red2;     // per-block partial sums of (P_new - P)^2 [nblk]
+};
+
+// One purification problem (a channel of a molecule).
+struct Sp2Job {
+    const double* F;        // the extrapolated Fock matrix F*
+    const double* rowmin;   // Gershgorin bounds of F*
+    const double* rowmax;
+    double* X0;             // ping-pong iterates, n x n each
+    double* X1;
+    double* P;              // output density (w X), n x n (may alias X0)
+    double* part;           // partial sums [max(nblk, ntiles)][2]
+    double nocc, weight;
+    int n, mol, tile0, ntiles;
+};
+
+struct Sp2State {
+    int active, steps, cur, square, converged;
+    double trX, trX2, emin, emax;
+    double idem[2];
+};
+
+// One tridiagonalisation + bisection problem.
+struct TriJob {
+    const double* A;   // symmetric input, n x n
+    double* W;         // scratch copy, n x n
+    double* d;         // diagonal, n
+    double* e;         // off-diagonal, n
+    double* eps;       // ascending eigenvalues, n
+    int n, mol;
 };
 
 struct ScfParams {
@@ -67,15 +97,24 @@ __global__ void k_core_energy(const MolDesc* mols, const double* ecc, MolState* 
 __global__ void k_fock(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                        const int* atom_z, const double* wstore, double* arena, const MolState* st, int force);
 // C = alpha A B (A row-major M x K) and C = alpha A^T B (A stored K x M)
-__global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force);
-__global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force);
-__global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force);
-__global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force);
+// mask (optional): only molecules with mask[mol] != 0 take part
+__global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
+__global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
+__global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force, const int* mask);
+__global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, const int* mask);
+__global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
+__global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
+__global__ void k_sp2_step(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+__global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count);
+__global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen);
+__global__ void k_tridiag(const TriJob* jobs, const int* mask);
+__global__ void k_bisect(const TriJob* jobs, const int* mask);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
 __global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                            const int* atom_z, double* arena);
 __global__ void k_identity(const ChanJob* jobs);
+__global__ void k_state_init(MolState* st, int nmol);
 __global__ void k_post_fock(const ChanJob* jobs, const MolDesc* mols, const MolState* st, int nblk, int energy_only,
                             int force);
 __global__ void k_diis_solve(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,

@@ -151,6 +151,52 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 /* Message of the last failing call on this host thread ("" if none). */
 const char* am1gpu_last_error(void);
 
+/*
+ * Resident batch: the molecules are uploaded once and stay in device memory, so the SCF can be
+ * re-run (and its results fetched) without moving inputs again -- the form a serving loop or a
+ * benchmark of the device path uses.  The handle owns its device memory and CUDA stream; it is
+ * not thread-safe (one handle per host thread at a time).  Inputs are copied at creation.
+ * No counterpart in the reference: am1-rs keeps all state in host memory.
+ */
+typedef struct am1gpu_batch am1gpu_batch;
+int am1gpu_batch_create(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
+                        am1gpu_batch** out);
+/* Runs integrals + SCF + result records on the device; no host<->device copy of inputs or
+ * results (only the 4-byte count of molecules still iterating is read back). */
+int am1gpu_batch_run(am1gpu_batch* batch);
+/* Copies the results of the last run into caller-owned records (same semantics as
+ * am1gpu_scf_batch's results/status). */
+int am1gpu_batch_results(am1gpu_batch* batch, am1gpu_result* results, int32_t* status);
+void am1gpu_batch_destroy(am1gpu_batch* batch);
+
+/* Phases of a call, named after the reference's AM1_TIMING scopes (src/scf.rs:315-659). */
+enum {
+    AM1GPU_PHASE_CORE = 0,        /* "basis+core": integrals, overlap, H_core, core-core, guess */
+    AM1GPU_PHASE_FOCK = 1,        /* "scf:fock" */
+    AM1GPU_PHASE_COMMUTATOR = 2,  /* "scf:commutator": F.P, [F,P], energy, DIIS history */
+    AM1GPU_PHASE_ACCEL = 3,       /* "scf:accel": CDIIS / A-DIIS solve and extrapolation */
+    AM1GPU_PHASE_EIGEN = 4,       /* "scf:eigen": warm-start product, Jacobi, sort */
+    AM1GPU_PHASE_JACOBI = 5,      /* the Jacobi kernel alone (inside scf:eigen) */
+    AM1GPU_PHASE_DENSITY = 6,     /* "scf:density": C_occ C_occ^T, dP, convergence */
+    AM1GPU_PHASE_FINAL = 7        /* final Fock, energy and result records */
+};
+
+/* Statistics of the last call on this host thread (or of a batch handle's last run). */
+typedef struct {
+    double device_ms;            /* the call's device time (CUDA events on the library's stream) */
+    double phase_ms[8];          /* per phase, when timing is on (else 0) */
+    int64_t phase_launches[8];   /* kernel launches per phase */
+    int64_t kernel_launches;     /* all kernels the call launched */
+    int64_t h2d_bytes;           /* host->device bytes the call copied */
+    int64_t d2h_bytes;           /* device->host bytes the call copied */
+    int32_t scf_cycles;          /* batched SCF iterations run (the slowest molecule's count) */
+} am1gpu_call_stats;
+
+/* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */
+void am1gpu_set_timing(int32_t enable);
+int am1gpu_last_call_stats(am1gpu_call_stats* out);
+int am1gpu_batch_stats(const am1gpu_batch* batch, am1gpu_call_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -209,3 +209,63 @@ def test_batch_matches_oracle_and_solo(gpu, oracle):
         # same alone and in the mix
         assert abs(solo["heat_of_formation_kcal"] - res[i]["heat_of_formation_kcal"]) < 1e-9
         assert np.max(np.abs(solo["density"] - res[i]["density"])) < 1e-12
+
+
+def test_orbital_energies_match_oracle(gpu, oracle, ref_values):
+    # mo_energies are the eigenvalues of the last extrapolated Fock matrix (src/scf.rs:654-689)
+    for name, z, xyz in _golden_molecules(ref_values):
+        g = gpu.scf(z, xyz)
+        o = oracle.scf(z, xyz)
+        assert np.max(np.abs(g["mo_energies"] - o["mo_energies"])) < 1e-7, name
+        assert abs(g["homo_ev"] - o["homo_ev"]) < 1e-7 and abs(g["lumo_ev"] - o["lumo_ev"]) < 1e-7, name
+
+
+def test_mo_coefficients_reproduce_the_density(gpu, ref_values):
+    # columns are MOs (src/scf.rs:200-240); P = 2 C_occ C_occ^T (RHF), P = Ca Ca^T + Cb Cb^T (UHF)
+    for name, z, xyz in _golden_molecules(ref_values)[:3]:
+        g = gpu.scf(z, xyz)
+        c = g["mo_coeff"]
+        k = g["n_occ"]
+        assert np.max(np.abs(c.T @ c - np.eye(c.shape[0]))) < 1e-10, name
+        assert np.max(np.abs(2.0 * c[:, :k] @ c[:, :k].T - g["density"])) < 1e-8, name
+    m = ref_values["scf_methyl_radical"]
+    z, xyz = atoms_to_arrays(m["atoms"])
+    g = gpu.scf(z, xyz, multiplicity=2)
+    ca, cb = g["mo_coeff"], g["beta_coeff"]
+    pa = ca[:, : g["n_occ"]] @ ca[:, : g["n_occ"]].T
+    pb = cb[:, : g["n_occ_beta"]] @ cb[:, : g["n_occ_beta"]].T
+    assert np.max(np.abs(pa + pb - g["density"])) < 1e-8
+    assert np.max(np.abs(pa - pb - g["spin_density"])) < 1e-8
+
+
+def test_eigensolver_density_path(tmp_path):
+    # AM1GPU_DENSITY=jacobi forms P from eigenvectors every iteration instead of purification;
+    # both paths must land on the oracle's answer
+    import subprocess
+    import sys
+    import textwrap
+
+    from conftest import ROOT
+
+    script = textwrap.dedent(f"""
+        import sys
+        sys.path[:0] = [{str(ROOT / 'am1-rs_b200')!r}, {str(ROOT / 'oracle')!r}]
+        import numpy as np
+        from am1gpu import native, workloads as W, _abi
+        import oracle
+        rng = np.random.default_rng(5)
+        mols = [W.alkane(n, rng) for n in (2, 9)] + [W.water_cluster(k, rng) for k in (3, 22)]
+        for m in mols:
+            xyz = _abi.angstrom_to_bohr(m.xyz)
+            g = native.scf(m.numbers, xyz)
+            o = oracle.scf(m.numbers, xyz)
+            assert g["status"] == 0, g.get("error")
+            assert abs(g["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < 1e-6
+            assert np.max(np.abs(g["density"] - o["density"])) < 1e-8
+        print("ok")
+    """)
+    f = tmp_path / "jac.py"
+    f.write_text(script)
+    env = dict(__import__("os").environ, AM1GPU_DENSITY="jacobi")
+    r = subprocess.run([sys.executable, str(f)], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
