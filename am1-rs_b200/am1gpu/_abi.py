@@ -116,10 +116,13 @@ class CallStats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_int64),
         ("d2h_bytes", ctypes.c_int64),
         ("scf_cycles", ctypes.c_int32),
+        ("eigen_fallbacks", ctypes.c_int32),
+        ("purification_steps", ctypes.c_double),
+        ("purification_flops", ctypes.c_double),
     ]
 
 
-PHASES = ["basis+core", "scf:fock", "scf:commutator", "scf:accel", "scf:eigen", "eigen:jacobi", "scf:density", "final"]
+PHASES = ["basis+core", "scf:fock", "scf:commutator", "scf:accel", "scf:eigen", "eigen:inner", "scf:density", "final"]
 
 _bp = ctypes.c_void_p
 
@@ -159,6 +162,9 @@ def stats_dict(st: CallStats) -> dict:
         "h2d_bytes": int(st.h2d_bytes),
         "d2h_bytes": int(st.d2h_bytes),
         "scf_cycles": int(st.scf_cycles),
+        "eigen_fallbacks": int(st.eigen_fallbacks),
+        "purification_steps": float(st.purification_steps),
+        "purification_flops": float(st.purification_flops),
     }
 
 _lib = None

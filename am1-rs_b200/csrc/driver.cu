@@ -360,6 +360,7 @@ struct Batch {
     TriJob* d_tri;
     int* d_need_eigen;
     int* d_sp2_active;
+    double* d_work;  // [0] purification steps, [1] their flops, [2] eigensolver fallbacks
     MolState* d_st;
     int* d_status;
     double *d_wstore, *d_ecc, *d_arena, *d_res, *d_charges;
@@ -369,6 +370,7 @@ struct Batch {
     std::vector<ChanJob> jobs;
     std::vector<int> job0;
     int* h_active;
+    double* h_work;
     double* h_res;
     double* h_charges;
     long long arena_doubles = 0;
@@ -441,6 +443,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_status = take(dv, sizeof(int) * b.nmol);
     const size_t o_need = take(dv, sizeof(int) * b.nmol);
     const size_t o_sp2a = take(dv, sizeof(int) * 4);
+    const size_t o_work = take(dv, sizeof(double) * 4);
     const size_t o_sp2s = take(dv, sizeof(Sp2State) * nch_total);
     const size_t o_active = take(dv, sizeof(int) * 4);
     const size_t o_w = take(dv, sizeof(double) * std::max<long long>(wsize, 1));
@@ -461,6 +464,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     // pinned staging also receives the outputs
     size_t hs = staged;
     const size_t h_o_active = take(hs, sizeof(int) * 4);
+    const size_t h_o_work = take(hs, sizeof(double) * 4);
     const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
     int rc = mem_ensure(mem, dtotal, align256(hs));
@@ -488,6 +492,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_tri = (TriJob*)dptr(o_tri);
     b.d_need_eigen = (int*)dptr(o_need);
     b.d_sp2_active = (int*)dptr(o_sp2a);
+    b.d_work = (double*)dptr(o_work);
     b.d_sp2_state = (Sp2State*)dptr(o_sp2s);
     b.sp2_nblk = sp2_nblk;
     b.d_st = (MolState*)dptr(o_st);
@@ -502,6 +507,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_res = (double*)dptr(o_res);
     b.d_charges = (double*)dptr(o_chg);
     b.h_active = (int*)(Hs + h_o_active);
+    b.h_work = (double*)(Hs + h_o_work);
     b.h_res = (double*)(Hs + h_o_res);
     b.h_charges = (double*)(Hs + h_o_chg);
     // ---- fill the staged region
@@ -757,6 +763,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.event(&t0))) return rc;
     if ((rc = run.begin(&ph))) return rc;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, s));
+    CK(cudaMemsetAsync(b.d_work, 0, sizeof(double) * 4, s));
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * b.arena_doubles, s));
     k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.nmol);
     run.launched(AM1GPU_PHASE_CORE);
@@ -799,25 +806,27 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
                 run.launched(AM1GPU_PHASE_EIGEN, 2);
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
+                    size_t pc;
+                    if ((rc = run.begin(&pc))) return rc;
                     k_sp2_step<<<b.nt_sp2, 128, 0, s>>>(b.d_sp2, b.d_sp2_tiles, b.nt_sp2, b.d_sp2_state);
+                    run.launched(AM1GPU_PHASE_DENSITY_CORE);
+                    if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
                     CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
-                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, kSp2MaxSteps, b.d_sp2_active);
-                    run.launched(AM1GPU_PHASE_EIGEN, 2);
+                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, kSp2MaxSteps, b.d_sp2_active,
+                                                                  b.d_work);
+                    run.launched(AM1GPU_PHASE_EIGEN);
                     if (step >= 12 && (step % 6) == 5) {
                         CK(cudaMemcpyAsync(b.h_active + 1, b.d_sp2_active, sizeof(int), cudaMemcpyDeviceToHost, s));
                         CK(cudaStreamSynchronize(s));
                         if (b.h_active[1] == 0) break;
                     }
                 }
-                k_sp2_finish<<<dim3(8, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen);
+                k_sp2_finish<<<dim3(8, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_work);
                 run.launched(AM1GPU_PHASE_EIGEN);
                 // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
                 k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
-                size_t pj;
-                if ((rc = run.begin(&pj))) return rc;
                 if ((rc = launch_jacobi(b, ws, 0, b.d_need_eigen))) return rc;
-                run.launched(AM1GPU_PHASE_JACOBI, (int)b.buckets.size());
-                if ((rc = run.end(AM1GPU_PHASE_JACOBI, pj))) return rc;
+                run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
                 k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
                 k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
                 run.launched(AM1GPU_PHASE_EIGEN, 3);
@@ -828,8 +837,8 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 size_t pj;
                 if ((rc = run.begin(&pj))) return rc;
                 if ((rc = launch_jacobi(b, ws, 0))) return rc;
-                run.launched(AM1GPU_PHASE_JACOBI, (int)b.buckets.size());
-                if ((rc = run.end(AM1GPU_PHASE_JACOBI, pj))) return rc;
+                run.launched(AM1GPU_PHASE_DENSITY_CORE, (int)b.buckets.size());
+                if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pj))) return rc;
                 k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
                 run.launched(AM1GPU_PHASE_EIGEN, 2);
                 if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
@@ -863,7 +872,11 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;
     if ((rc = run.event(&t1))) return rc;
+    CK(cudaMemcpyAsync(b.h_work, b.d_work, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    stats->purification_steps += b.h_work[0];
+    stats->purification_flops += b.h_work[1];
+    stats->eigen_fallbacks += (int32_t)b.h_work[2];
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, mem.events[t0], mem.events[t1]));
     stats->device_ms += ms;

@@ -208,12 +208,15 @@ __global__ void __launch_bounds__(128) k_sp2_step(const Sp2Job* __restrict__ job
 
 // After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
 __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs, int max_steps,
-                             int* __restrict__ active_count) {
+                             int* __restrict__ active_count, double* __restrict__ work) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     Sp2State& s = sst[j];
     if (!s.active) return;
     const Sp2Job jb = jobs[j];
+    // algorithmic work of the product just taken: a symmetric X.X, n^3 flops
+    atomicAdd(&work[0], 1.0);
+    atomicAdd(&work[1], (double)jb.n * jb.n * jb.n);
     double tr = 0.0, fr = 0.0;
     for (int t = 0; t < jb.ntiles; ++t) {
         tr += jb.part[2 * t];
@@ -245,12 +248,15 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
 // P_new = w X (the converged X); molecules whose purification stalled are flagged for the
 // eigensolver path.
 __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __restrict__ sst, const MolState* __restrict__ st,
-                             int* __restrict__ need_eigen) {
+                             int* __restrict__ need_eigen, double* __restrict__ work) {
     const Sp2Job jb = jobs[blockIdx.y];
     if (!st[jb.mol].active) return;
     const Sp2State& s = sst[blockIdx.y];
     if (!s.converged) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) need_eigen[jb.mol] = 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            need_eigen[jb.mol] = 1;
+            atomicAdd(&work[2], 1.0);
+        }
         return;
     }
     const double* X = s.cur ? jb.X1 : jb.X0;

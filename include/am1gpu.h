@@ -175,8 +175,9 @@ enum {
     AM1GPU_PHASE_FOCK = 1,        /* "scf:fock" */
     AM1GPU_PHASE_COMMUTATOR = 2,  /* "scf:commutator": F.P, [F,P], energy, DIIS history */
     AM1GPU_PHASE_ACCEL = 3,       /* "scf:accel": CDIIS / A-DIIS solve and extrapolation */
-    AM1GPU_PHASE_EIGEN = 4,       /* "scf:eigen": warm-start product, Jacobi, sort */
-    AM1GPU_PHASE_JACOBI = 5,      /* the Jacobi kernel alone (inside scf:eigen) */
+    AM1GPU_PHASE_EIGEN = 4,       /* "scf:eigen": P from F* (purification, or eigensolver) */
+    AM1GPU_PHASE_DENSITY_CORE = 5,/* the inner kernel of scf:eigen alone: the purification
+                                     steps, or the Jacobi kernel on the eigensolver path */
     AM1GPU_PHASE_DENSITY = 6,     /* "scf:density": C_occ C_occ^T, dP, convergence */
     AM1GPU_PHASE_FINAL = 7        /* final Fock, energy and result records */
 };
@@ -190,6 +191,9 @@ typedef struct {
     int64_t h2d_bytes;           /* host->device bytes the call copied */
     int64_t d2h_bytes;           /* device->host bytes the call copied */
     int32_t scf_cycles;          /* batched SCF iterations run (the slowest molecule's count) */
+    int32_t eigen_fallbacks;     /* molecule-iterations whose purification stalled (eigensolver used) */
+    double purification_steps;   /* purification steps summed over molecules, channels, iterations */
+    double purification_flops;   /* their algorithmic work: n^3 per symmetric product X.X */
 } am1gpu_call_stats;
 
 /* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */
