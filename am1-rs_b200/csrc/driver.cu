@@ -95,6 +95,12 @@ int device_ctx(DeviceCtx** out) {
             return bad("jacobi smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("jacobi cluster attribute", err);
+        if ((err = cudaFuncSetAttribute(k_sp2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
+            cudaSuccess)
+            return bad("sp2 smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_dgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
+            cudaSuccess)
+            return bad("dgemm smem attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
@@ -791,7 +797,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                                                       b.d_st, 0);
             run.launched(AM1GPU_PHASE_FOCK);
             if ((rc = run.end(AM1GPU_PHASE_FOCK, ph)) || (rc = run.begin(&ph))) return rc;
-            k_gemm_nn<<<b.nt_fp, 256, 0, s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0, nullptr);
+            k_dgemm_nn<<<b.nt_fp, 128, dgemm_smem_bytes(), s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0, nullptr);
             k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
             run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
             if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, ph)) || (rc = run.begin(&ph))) return rc;
@@ -808,7 +814,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
-                    k_sp2_step<<<b.nt_sp2, 128, 0, s>>>(b.d_sp2, b.d_sp2_tiles, b.nt_sp2, b.d_sp2_state);
+                    k_sp2_step<<<b.nt_sp2, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, b.d_sp2_tiles, b.nt_sp2, b.d_sp2_state);
                     run.launched(AM1GPU_PHASE_DENSITY_CORE);
                     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
                     CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));

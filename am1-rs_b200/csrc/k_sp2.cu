@@ -14,20 +14,11 @@
 #include <cuda_runtime.h>
 
 #include "am1gpu_internal.h"
+#include "dmma_gemm.cuh"
 #include "kernels.h"
 
 namespace am1 {
 
-constexpr int SP_TILE = 64;
-constexpr int SP_BK = 16;
-constexpr int SP_AS = SP_BK + 4;    // row stride of the A tile (conflict-free 8-byte fragment loads)
-constexpr int SP_BS = SP_TILE + 4;  // row stride of the B tile
-
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
 
 // X0 = (e_max I - F*) / (e_max - e_min); per-block partial sums of tr X0 and ||X0||_F^2.
 __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, const MolState* __restrict__ st, int nblk) {
@@ -120,10 +111,9 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
 }
 
 // One SP2 step over all upper-triangle 64x64 tiles of every active channel.
-__global__ void __launch_bounds__(128) k_sp2_step(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
-                                                  const Sp2State* __restrict__ sst) {
-    __shared__ double As[SP_TILE * SP_AS];
-    __shared__ double Bs[SP_BK * SP_BS];
+__global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                            int ntiles, const Sp2State* __restrict__ sst) {
+    extern __shared__ double dsm[];
     __shared__ double red[2][4];
     const int t = blockIdx.x;
     if (t >= ntiles) return;
@@ -134,42 +124,12 @@ __global__ void __launch_bounds__(128) k_sp2_step(const Sp2Job* __restrict__ job
     const int n = jb.n;
     const double* X = s.cur ? jb.X1 : jb.X0;
     double* Y = s.cur ? jb.X0 : jb.X1;
-    const int m0 = tl.tm * SP_TILE, n0 = tl.tn * SP_TILE;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // warp tile origin inside the CTA tile
-    const int g = lane >> 2, tq = lane & 3;
+    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
     double acc[4][4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    for (int k0 = 0; k0 < n; k0 += SP_BK) {
-        // A tile: rows m0.., cols k0.. ; B tile: rows k0.., cols n0..  (X symmetric)
-#pragma unroll
-        for (int l = 0; l < 8; ++l) {
-            const int idx = tid + l * 128;
-            const int ar = idx >> 4, ak = idx & 15;
-            const int gi = m0 + ar, gk = k0 + ak;
-            As[ar * SP_AS + ak] = (gi < n && gk < n) ? X[(long long)gi * n + gk] : 0.0;
-            const int bk = idx >> 6, bc = idx & 63;
-            const int gbk = k0 + bk, gj = n0 + bc;
-            Bs[bk * SP_BS + bc] = (gbk < n && gj < n) ? X[(long long)gbk * n + gj] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < SP_BK; kk += 4) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[(wr + i * 8 + g) * SP_AS + kk + tq];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * SP_BS + wc + j * 8 + g];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-        }
-        __syncthreads();
-    }
+    dg_mainloop(dsm, X, n, X, n, n, n, n, m0, n0, acc);  // X symmetric: X[rows m0..] . X[:, n0..]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    const int g = lane >> 2, tq = lane & 3;
     // epilogue: Y = X^2 or 2X - X^2, mirrored; partial trace / Frobenius sums
     const bool diag_tile = tl.tm == tl.tn;
     double tr = 0.0, fr = 0.0;
@@ -204,6 +164,36 @@ __global__ void __launch_bounds__(128) k_sp2_step(const Sp2Job* __restrict__ job
         p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
         p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
     }
+}
+
+// C = alpha A.B for every (molecule, channel) job of a tile list, on the FP64 tensor cores
+// (the commutator product F.P, src/scf.rs:531-544).
+__global__ void __launch_bounds__(DG_THREADS, 4) k_dgemm_nn(const GemmJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                            int ntiles, const MolState* __restrict__ st, int force,
+                                                            const int* __restrict__ mask) {
+    extern __shared__ double dsm[];
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const GemmJob jb = jobs[tl.job];
+    if (!force && !st[jb.mol].active) return;
+    if (mask && !mask[jb.mol]) return;
+    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
+    double acc[4][4][2];
+    dg_mainloop(dsm, jb.A, jb.lda, jb.B, jb.ldb, jb.M, jb.N, jb.K, m0, n0, acc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int r = m0 + wr + i * 8 + g;
+                const int c = n0 + wc + j * 8 + tq * 2 + e;
+                if (r < jb.M && c < jb.N) jb.C[(long long)r * jb.ldc + c] = jb.alpha * acc[i][j][e];
+            }
 }
 
 // After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
@@ -264,5 +254,7 @@ __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x)
         jb.P[i] = jb.weight * X[i];
 }
+
+size_t dgemm_smem_bytes() { return DG_SMEM; }
 
 }  // namespace am1

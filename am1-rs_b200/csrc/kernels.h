@@ -105,6 +105,8 @@ __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, co
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 __global__ void k_sp2_step(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+__global__ void k_dgemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
+size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work);
 __global__ void k_tridiag(const TriJob* jobs, const int* mask);
