@@ -142,6 +142,8 @@ SIGNATURES = {
     ),
     "am1gpu_symmetric_eigen": (ctypes.c_int, [ctypes.c_int32, _dp, _dp, _dp]),
     "am1gpu_last_error": (ctypes.c_char_p, []),
+    "am1gpu_symmetric_eigen_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
     "am1gpu_batch_create": (
         ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(_bp)]),
     "am1gpu_batch_run": (ctypes.c_int, [_bp]),

@@ -15,6 +15,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 
 #ifdef __CUDACC__
 #define AM1_HD __host__ __device__
@@ -88,5 +89,8 @@ constexpr int RED_B = 3;              // 8 entries: <e_new, e_j> (packed, x2 app
 constexpr int RED_GROW = 11;          // 8 entries: <D_new, F_j>
 constexpr int RED_GCOL = 19;          // 8 entries: <D_i, F_new>
 constexpr int RED_N = 27;
+
+// Message returned by am1gpu_last_error for the calling host thread.
+void set_last_error(const std::string& msg);
 
 }  // namespace am1

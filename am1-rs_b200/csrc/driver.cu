@@ -1265,6 +1265,8 @@ struct am1gpu_batch {
     bool ran = false;
 };
 
+void am1::set_last_error(const std::string& msg) { am1::g_err = msg; }
+
 // ---------------------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------------------

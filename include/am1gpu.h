@@ -152,6 +152,23 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 const char* am1gpu_last_error(void);
 
 /*
+ * Allocation-free symmetric eigensolver, for callers that may not allocate device memory
+ * (code running beside a framework that owns the whole device memory pool, real-time loops
+ * where an allocation is an unbounded stall, hosts that only hand out device buffers).  No
+ * counterpart in the reference: am1-rs has no device memory to allocate.
+ * a (n*n), w (n) and v (n*n) are DEVICE pointers owned by the caller; a is read (lower
+ * triangle, as symmetric_eigen does), w receives ascending eigenvalues, v (row-major) the
+ * eigenvectors as columns.  stream is a cudaStream_t (NULL: the default stream); the call
+ * returns when the results are in w and v.  Scratch is a fixed 512 KiB device array inside
+ * the library, so n <= 128 (larger n returns AM1GPU_INVALID_INPUT) and no cudaMalloc/cudaFree
+ * is ever called.  The first call on a device sets up (fetches the array's address) and must
+ * come before any stream capture on that device.  Calls share the array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller.  Non-finite input returns
+ * AM1GPU_LINALG (w and v are then unspecified).
+ */
+int am1gpu_symmetric_eigen_noalloc(int32_t n, const double* a, double* w, double* v, void* stream);
+
+/*
  * Resident batch: the molecules are uploaded once and stay in device memory, so the SCF can be
  * re-run (and its results fetched) without moving inputs again -- the form a serving loop or a
  * benchmark of the device path uses.  The handle owns its device memory and CUDA stream; it is
