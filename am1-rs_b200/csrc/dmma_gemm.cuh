@@ -1,8 +1,13 @@
 // FP64 tensor-core GEMM main loop for 64x64 output tiles: C_tile = A[m0:m0+64, :K] . B[:K, n0:n0+64]
-// with mma.sync.m8n8k4.f64 (4 warps, each a 32x32 sub-tile of 4x4 MMA blocks) and a
+// with mma.sync.m16n8k8.f64 (4 warps, each a 32x32 sub-tile of 2x4 MMA blocks) and a
 // STAGES-deep cp.async pipeline feeding shared memory, so global (L2) latency is overlapped
 // with the MMAs.  Row-major operands with arbitrary leading dimensions; out-of-range elements
 // are zero-filled by the copy itself (src-size 0).
+//
+// Fragment layout of m16n8k8 f64 (g = lane/4, t = lane%4):
+//   A (16x8, row): a0 (g, t)  a1 (g+8, t)  a2 (g, t+4)  a3 (g+8, t+4)
+//   B (8x8, col):  b0 (t, g)  b1 (t+4, g)
+//   C (16x8):      c0 (g, 2t)  c1 (g, 2t+1)  c2 (g+8, 2t)  c3 (g+8, 2t+1)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,10 +23,20 @@ constexpr int DG_STAGES = 3;
 constexpr int DG_THREADS = 128;
 constexpr size_t DG_SMEM = sizeof(double) * DG_STAGE * DG_STAGES;
 
-__device__ __forceinline__ void dg_mma(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
+__device__ __forceinline__ void dg_mma(double c[4], const double a[4], const double b[2]) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// Row and column (inside the 64x64 tile) of accumulator element acc[i][j][e].
+__device__ __forceinline__ int dg_row(int i, int e) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    return (warp >> 1) * 32 + i * 16 + (lane >> 2) + (e >= 2 ? 8 : 0);
+}
+__device__ __forceinline__ int dg_col(int j, int e) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    return (warp & 1) * 32 + j * 8 + (lane & 3) * 2 + (e & 1);
 }
 
 // 8-byte asynchronous copy; an invalid element reads nothing (src-size 0) from the operand's
@@ -56,16 +71,21 @@ __device__ __forceinline__ void dg_load(double* smem, int st, const double* __re
     }
 }
 
-// acc[i][j][e]: row wr + 8i + (lane>>2), column wc + 8j + 2(lane&3) + e of the 64x64 tile.
+// acc[i][j][e]: element (dg_row(i, e), dg_col(j, e)) of the 64x64 tile.  A warp with
+// compute == false still takes part in the copies and barriers but issues no MMAs (its 32x32
+// quarter of the tile is padding, or redundant by symmetry); the SM gives its issue slots to
+// other CTAs' warps.
 __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restrict__ A, int lda, const double* __restrict__ B, int ldb,
-                                            int M, int N, int K, int m0, int n0, double acc[4][4][2]) {
+                                            int M, int N, int K, int m0, int n0, double acc[2][4][4], bool compute = true) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
     const int g = lane >> 2, tq = lane & 3;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     const int KT = (K + DG_BK - 1) / DG_BK;
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {
@@ -80,17 +100,28 @@ __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restri
         dg_commit();
         const double* As = smem + (kt % DG_STAGES) * DG_STAGE;
         const double* Bs = As + DG_TILE * DG_AS;
+        if (!compute) continue;
 #pragma unroll
-        for (int kk = 0; kk < DG_BK; kk += 4) {
-            double a[4], b[4];
+        for (int kk = 0; kk < DG_BK; kk += 8) {
+            double a[2][4], b[4][2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[(wr + i * 8 + g) * DG_AS + kk + tq];
+            for (int i = 0; i < 2; ++i) {
+                const double* ar = As + (wr + i * 16 + g) * DG_AS + kk + tq;
+                a[i][0] = ar[0];
+                a[i][1] = ar[8 * DG_AS];
+                a[i][2] = ar[4];
+                a[i][3] = ar[8 * DG_AS + 4];
+            }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * DG_BS + wc + j * 8 + g];
+            for (int j = 0; j < 4; ++j) {
+                const double* br = Bs + (kk + tq) * DG_BS + wc + j * 8 + g;
+                b[j][0] = br[0];
+                b[j][1] = br[4 * DG_BS];
+            }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) dg_mma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                for (int j = 0; j < 4; ++j) dg_mma(acc[i][j], a[i], b[j]);
         }
     }
     dg_wait<0>();

@@ -7,7 +7,7 @@
 //     X0 = (e_max I - F*) / (e_max - e_min)         (Gershgorin bounds, spectrum mapped into [0,1])
 //     X <- X^2  or  X <- 2X - X^2                   (whichever brings tr X closer to n_occ)
 // until X is idempotent to rounding.  Each step is one symmetric FP64 product X.X on the tensor
-// cores (mma.sync m8n8k4 f64), upper-triangle tiles only, mirrored in the epilogue, which also
+// cores (mma.sync m16n8k8 f64), upper-triangle tiles only, mirrored in the epilogue, which also
 // folds in the choice of branch and the tile's share of tr X and ||X||_F^2 (= tr X^2 for the
 // next step's decision).  No eigenvectors, no fine-grained synchronisation: every step is one
 // launch over all (molecule, channel) tiles of the batch.
@@ -125,28 +125,32 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __rest
     const double* X = s.cur ? jb.X1 : jb.X0;
     double* Y = s.cur ? jb.X0 : jb.X1;
     const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
-    double acc[4][4][2];
-    dg_mainloop(dsm, X, n, X, n, n, n, n, m0, n0, acc);  // X symmetric: X[rows m0..] . X[:, n0..]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-    const int g = lane >> 2, tq = lane & 3;
-    // epilogue: Y = X^2 or 2X - X^2, mirrored; partial trace / Frobenius sums
     const bool diag_tile = tl.tm == tl.tn;
+    // this warp's 32x32 quarter: skip it when it is padding, or the lower-left quarter of a
+    // diagonal tile (the upper-right quarter computes and mirrors it)
+    const int qr = (warp >> 1) * 32, qc = (warp & 1) * 32;
+    const bool lower_quarter = diag_tile && qr > qc;
+    const bool compute = m0 + qr < n && n0 + qc < n && !lower_quarter;
+    double acc[2][4][4];
+    dg_mainloop(dsm, X, n, X, n, n, n, n, m0, n0, acc, compute);  // X symmetric: X[rows m0..] . X[:, n0..]
+    // epilogue: Y = X^2 or 2X - X^2, mirrored; partial trace / Frobenius sums
+    const bool mirror = !diag_tile || qr < qc;  // off-diagonal content: write the transpose too
     double tr = 0.0, fr = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int r = m0 + wr + i * 8 + g;
-                const int c = n0 + wc + j * 8 + tq * 2 + e;
-                if (r < n && c < n) {
+            for (int e = 0; e < 4; ++e) {
+                const int r = m0 + dg_row(i, e);
+                const int c = n0 + dg_col(j, e);
+                if (compute && r < n && c < n) {
                     const double x2 = acc[i][j][e];
                     const double y = s.square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
                     Y[(long long)r * n + c] = y;
-                    if (!diag_tile) Y[(long long)c * n + r] = y;
-                    fr += (diag_tile ? 1.0 : 2.0) * y * y;
+                    if (mirror) Y[(long long)c * n + r] = y;
+                    fr += (mirror ? 2.0 : 1.0) * y * y;
                     if (r == c) tr += y;
                 }
             }
@@ -179,19 +183,18 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_dgemm_nn(const GemmJob* __res
     if (!force && !st[jb.mol].active) return;
     if (mask && !mask[jb.mol]) return;
     const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
-    double acc[4][4][2];
-    dg_mainloop(dsm, jb.A, jb.lda, jb.B, jb.ldb, jb.M, jb.N, jb.K, m0, n0, acc);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-    const int g = lane >> 2, tq = lane & 3;
+    const int warp = threadIdx.x >> 5;
+    const bool compute = m0 + (warp >> 1) * 32 < jb.M && n0 + (warp & 1) * 32 < jb.N;  // skip pure padding
+    double acc[2][4][4];
+    dg_mainloop(dsm, jb.A, jb.lda, jb.B, jb.ldb, jb.M, jb.N, jb.K, m0, n0, acc, compute);
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int r = m0 + wr + i * 8 + g;
-                const int c = n0 + wc + j * 8 + tq * 2 + e;
+            for (int e = 0; e < 4; ++e) {
+                const int r = m0 + dg_row(i, e);
+                const int c = n0 + dg_col(j, e);
                 if (r < jb.M && c < jb.N) jb.C[(long long)r * jb.ldc + c] = jb.alpha * acc[i][j][e];
             }
 }

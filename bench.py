@@ -343,7 +343,7 @@ def run_ours(args):
             "parity": {"sample": len(par_idx), "max_abs_dHf_kcal_vs_oracle": dhf, "bar": 1e-4},
             "e2e": {"value": world * nmol * args.steps / e2e_s, "unit": "solves/s",
                     "h2d_bytes_per_step": e2e_stats["h2d_bytes"], "d2h_bytes_per_step": e2e_stats["d2h_bytes"]},
-            "roofline": {"kernel": "k_sp2_step (density purification: symmetric FP64 X.X on mma.sync m8n8k4 f64)",
+            "roofline": {"kernel": "k_sp2_step (density purification: symmetric FP64 X.X on mma.sync m16n8k8 f64)",
                          "bound": "tensor", "achieved": achieved_tf, "peak": peak_fp64, "unit": "TFLOP/s",
                          "frac": achieved_tf / peak_fp64 if peak_fp64 else None, "traffic": None,
                          "peak_source": "FP64 cuBLAS DGEMM (torch.matmul float64 8192^3) measured in this run; "
