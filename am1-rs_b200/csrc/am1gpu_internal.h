@@ -57,7 +57,7 @@ struct MolDesc {
 };
 
 // Matrix slots of one channel, each n*n doubles, at ch_base + slot*n*n (VS holds npad*n).
-enum ChSlot { SLOT_F = 0, SLOT_FP = 1, SLOT_P = 2, SLOT_CT = 3, SLOT_GT = 4, SLOT_VS = 5, NUM_SLOTS = 6 };
+enum ChSlot { SLOT_F = 0, SLOT_FX = 1, SLOT_P = 2, SLOT_CT = 3, SLOT_GT = 4, SLOT_VS = 5, NUM_SLOTS = 6 };
 
 // Packed history of one channel: MAX_DIIS entries each of F (n(n+1)/2), E (n(n-1)/2) and,
 // for A-DIIS, D (n(n+1)/2); laid out [F x8][E x8][D x8].

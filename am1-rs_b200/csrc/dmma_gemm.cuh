@@ -128,4 +128,85 @@ __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restri
     __syncthreads();
 }
 
+// acc = A1[m0:, :K] . B1[:K, n0:] - A2[m0:, :K] . B2[:K, n0:], as one pipelined k-loop over 2K:
+// the k-tiles of the second product follow those of the first, and the accumulator is negated
+// between the two (so the pipeline never drains in the middle).  All four operands share M = N = K
+// and the leading dimension ld.  Same fragment layout and `compute` rule as dg_mainloop.
+__device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __restrict__ A1, const double* __restrict__ B1,
+                                                 const double* __restrict__ A2, const double* __restrict__ B2, int ld,
+                                                 int n, int m0, int n0, double acc[2][4][4], bool compute) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+    const int KT = (n + DG_BK - 1) / DG_BK;  // k-tiles per product
+    auto load = [&](int st, int kt) {
+        if (kt < KT)
+            dg_load(smem, st, A1, ld, B1, ld, n, n, n, m0, n0, kt);
+        else
+            dg_load(smem, st, A2, ld, B2, ld, n, n, n, m0, n0, kt - KT);
+    };
+#pragma unroll
+    for (int s = 0; s < DG_STAGES - 1; ++s) {
+        if (s < 2 * KT) load(s, s);
+        dg_commit();
+    }
+    for (int kt = 0; kt < 2 * KT; ++kt) {
+        dg_wait<DG_STAGES - 2>();
+        __syncthreads();
+        const int nk = kt + DG_STAGES - 1;
+        if (nk < 2 * KT) load(nk % DG_STAGES, nk);
+        dg_commit();
+        const double* As = smem + (kt % DG_STAGES) * DG_STAGE;
+        const double* Bs = As + DG_TILE * DG_AS;
+        if (!compute) continue;
+        if (kt == KT) {  // first product done: acc = -A1.B1, then accumulate A2.B2
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
+        }
+#pragma unroll
+        for (int kk = 0; kk < DG_BK; kk += 8) {
+            double a[2][4], b[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const double* ar = As + (wr + i * 16 + g) * DG_AS + kk + tq;
+                a[i][0] = ar[0];
+                a[i][1] = ar[8 * DG_AS];
+                a[i][2] = ar[4];
+                a[i][3] = ar[8 * DG_AS + 4];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double* br = Bs + (kk + tq) * DG_BS + wc + j * 8 + g;
+                b[j][0] = br[0];
+                b[j][1] = br[4 * DG_BS];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dg_mma(acc[i][j], a[i], b[j]);
+        }
+    }
+    dg_wait<0>();
+    __syncthreads();
+    // acc = A2.B2 - A1.B1: flip to A1.B1 - A2.B2
+    if (compute) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
+    }
+}
+
 }  // namespace am1

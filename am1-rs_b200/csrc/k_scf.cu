@@ -1,10 +1,13 @@
 // The per-iteration SCF bookkeeping kernels (am1-rs src/scf.rs:475-1204), batched over
 // molecules and spin channels:
 //   k_sad_init     superposition-of-atomic-densities guess            scf.rs:475-494, 730-740
-//   k_post_fock    one pass over the upper triangle of F, F.P, P, H:
-//                  energy traces (scf.rs:595, 767), the commutator e = FP - (FP)^T and its norm
-//                  (scf.rs:531-544, 600), the packed history push (scf.rs:603-614, 877-952) and
-//                  the new row/column of the CDIIS and A-DIIS Gram matrices (only those change)
+//   k_commutator   the commutator e = FP - (FP)^T = F.P - P.F (scf.rs:531-544) straight from F and
+//                  P on the FP64 tensor cores, upper-triangle tiles only; its epilogue pushes e
+//                  into the packed history and forms |e|^2 (scf.rs:600) and the new row of the
+//                  CDIIS Gram matrix, so F.P is never stored
+//   k_post_fock    one pass over the upper triangle of F, P, H: energy traces (scf.rs:595, 767),
+//                  the packed history push of F and P (scf.rs:603-614, 877-952) and the new
+//                  row/column of the A-DIIS Gram matrix (only those change)
 //   k_diis_solve   one thread per molecule: history bookkeeping, divergence guard
 //                  (scf.rs:621-625), CDIIS bordered solve with the 1e-12 pivot guard
 //                  (scf.rs:966-988, 1095-1141), A-DIIS simplex (scf.rs:1061-1091, 1144-1204)
@@ -14,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "am1gpu_internal.h"
+#include "dmma_gemm.cuh"
 #include "kernels.h"
 
 namespace am1 {
@@ -90,7 +94,7 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
     int newslot = 0;
     unsigned live = 0;
     live_slots(s, newslot, live);
-    const long long ls = packed_sym_len(n), la = packed_anti_len(n);
+    const long long ls = packed_sym_len(n);
     double acc[RED_N];
 #pragma unroll
     for (int k = 0; k < RED_N; ++k) acc[k] = 0.0;
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
         const double* Fr = jb.F + (long long)r * n;
         const double* Pr = jb.P + (long long)r * n;
         const double* Hr = jb.H + (long long)r * n;
-        const long long rs = sym_row(r, n), ra = anti_row(r, n);
+        const long long rs = sym_row(r, n);
         for (int c = r + lane; c < n; c += 32) {
             const double f = Fr[c], p = Pr[c], hh = Hr[c];
             const double wgt = c == r ? 1.0 : 2.0;
@@ -110,23 +114,14 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
             jb.hF[newslot * ls + si] = f;
             if (adiis) {
                 jb.hD[newslot * ls + si] = p;
-                acc[RED_GROW + newslot] += wgt * p * f;
 #pragma unroll
-                for (int j = 0; j < MAX_DIIS; ++j)
-                    if (live >> j & 1u) {
+                for (int j = 0; j < MAX_DIIS; ++j)  // unrolled: no dynamic index into acc
+                    if (j == newslot) {
+                        acc[RED_GROW + j] += wgt * p * f;
+                    } else if (live >> j & 1u) {
                         acc[RED_GROW + j] += wgt * p * jb.hF[j * ls + si];
                         acc[RED_GCOL + j] += wgt * jb.hD[j * ls + si] * f;
                     }
-            }
-            if (c > r) {
-                const double e = jb.FP[(long long)r * n + c] - jb.FP[(long long)c * n + r];
-                const long long ai = ra + (c - r - 1);
-                jb.hE[newslot * la + ai] = e;
-                acc[RED_ERR2] += 2.0 * e * e;
-                acc[RED_B + newslot] += e * e;
-#pragma unroll
-                for (int j = 0; j < MAX_DIIS; ++j)
-                    if (live >> j & 1u) acc[RED_B + j] += e * jb.hE[j * la + ai];
             }
         }
     }
@@ -143,6 +138,74 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
         double v = 0.0;
         for (int w = 0; w < POST_WARPS; ++w) v += part[w][threadIdx.x];
         jb.red[(long long)blockIdx.x * RED_N + threadIdx.x] = v;
+    }
+}
+
+// The DIIS error e = FP - (FP)^T of the new Fock matrix (scf.rs:531-544).  F and P are symmetric,
+// so (FP)^T = P.F and e = F.P - P.F: tile (I, J) of e is F[I,:].P[:,J] - P[I,:].F[:,J], one
+// pipelined FP64 tensor-core k-loop over both products, and e is antisymmetric, so only the
+// upper-triangle tiles are computed.  The epilogue takes the strict upper triangle: it stores e in
+// the packed history slot of this iteration and forms this tile's share of |e|_F^2 and of
+// <e, e_slot> for every live slot (the new CDIIS Gram row).
+__global__ void __launch_bounds__(DG_THREADS, 4) k_commutator(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                              int ntiles, const MolState* __restrict__ st) {
+    extern __shared__ double dsm[];
+    __shared__ double red[CP_N][4];
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const ChanJob jb = jobs[tl.job];
+    const MolState& s = st[jb.mol];
+    if (!s.active) return;
+    const int n = jb.n;
+    int newslot = 0;
+    unsigned live = 0;
+    live_slots(s, newslot, live);
+    const long long la = packed_anti_len(n);
+    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // this warp's 32x32 quarter: skip it when it is padding or lies below the diagonal
+    const int qr = (warp >> 1) * 32, qc = (warp & 1) * 32;
+    const bool compute = m0 + qr < n && n0 + qc < n && !(tl.tm == tl.tn && qr > qc);
+    double acc[2][4][4];
+    dg_mainloop_diff(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
+    double v[CP_N];
+#pragma unroll
+    for (int k = 0; k < CP_N; ++k) v[k] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = m0 + dg_row(i, e);
+                const int c = n0 + dg_col(j, e);
+                if (compute && r < c && c < n) {
+                    const double ev = acc[i][j][e];
+                    const long long ai = anti_row(r, n) + (c - r - 1);
+                    jb.hE[newslot * la + ai] = ev;
+                    v[CP_ERR2] += 2.0 * ev * ev;
+#pragma unroll
+                    for (int q = 0; q < MAX_DIIS; ++q)
+                        if (q == newslot)
+                            v[CP_B + q] += ev * ev;
+                        else if (live >> q & 1u)
+                            v[CP_B + q] += ev * jb.hE[q * la + ai];
+                }
+            }
+#pragma unroll
+    for (int k = 0; k < CP_N; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[k][warp] = x;
+    }
+    __syncthreads();
+    if (tid < CP_N) {
+        // index of tile (tm, tn), tm <= tn, in the channel's row-major upper-triangle tile list
+        const int T = (n + DG_TILE - 1) / DG_TILE;
+        const int local = tl.tm * T - tl.tm * (tl.tm - 1) / 2 + (tl.tn - tl.tm);
+        jb.cpart[(long long)local * CP_N + tid] = red[tid][0] + red[tid][1] + red[tid][2] + red[tid][3];
     }
 }
 
@@ -246,6 +309,10 @@ __global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __
         const ChanJob& jb = jobs[mol_job0[mi] + c];
         for (int b = 0; b < nblk; ++b)
             for (int k = 0; k < RED_N; ++k) tot[k] += jb.red[(long long)b * RED_N + k];
+        for (int t = 0; t < jb.ntiles; ++t) {  // the commutator pass, in tile order
+            tot[RED_ERR2] += jb.cpart[(long long)t * CP_N + CP_ERR2];
+            for (int k = 0; k < MAX_DIIS; ++k) tot[RED_B + k] += jb.cpart[(long long)t * CP_N + CP_B + k];
+        }
     }
     const double e_elec = 0.5 * (tot[RED_E_H] + tot[RED_E_F]);
     const double err = sqrt(tot[RED_ERR2]);
@@ -342,7 +409,7 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
     const long long ls = packed_sym_len(n);
     const int m = s.hist_count;
     for (int r = blockIdx.x * nw + warp; r < n; r += gridDim.x * nw) {
-        double* out = jb.FP + (long long)r * n;
+        double* out = jb.Fx + (long long)r * n;
         double bound = 0.0, diag = 0.0;
         for (int c = lane; c < n; c += 32) {
             double v;

@@ -39,7 +39,7 @@ struct EigJob {
 struct ChanJob {
     int mol, ch, n;
     double* F;
-    double* FP;       // F.P, then reused for the extrapolated Fock
+    double* Fx;       // the extrapolated Fock matrix F* (DIIS combination)
     double* P;
     double* Pnew;
     double* Ct;       // eigenvector rows (C^T), n x n
@@ -52,7 +52,13 @@ struct ChanJob {
     double* rowmax;   // n: Gershgorin upper bound
     double* red;      // per-block partial sums [nblk][RED_N]
     double* red2;     // per-block partial sums of (P_new - P)^2 [nblk]
+    double* cpart;    // per-tile partial sums of the commutator pass [ntiles][CP_N]
+    int ntiles;       // upper-triangle 64x64 tiles of the channel
 };
+
+// Partial sums of k_commutator per tile: CP_ERR2 = sum of e^2 over the full matrix,
+// CP_B + slot = <e_new, e_slot> over the strict upper triangle (slot = physical history slot).
+constexpr int CP_ERR2 = 0, CP_B = 1, CP_N = 1 + MAX_DIIS;
 
 // One purification problem (a channel of a molecule).
 struct Sp2Job {
@@ -76,7 +82,6 @@ struct Sp2State {
 // One tridiagonalisation + bisection problem.
 struct TriJob {
     const double* A;   // symmetric input, n x n
-    double* W;         // scratch copy, n x n
     double* d;         // diagonal, n
     double* e;         // off-diagonal, n
     double* eps;       // ascending eigenvalues, n
@@ -105,11 +110,15 @@ __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, co
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 __global__ void k_sp2_step(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+// E = F.P - P.F over the upper-triangle tiles: history push of E and its CDIIS Gram row
+__global__ void k_commutator(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 __global__ void k_dgemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work);
+// launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each
 __global__ void k_tridiag(const TriJob* jobs, const int* mask);
+size_t tridiag_smem_bytes(int n, int C);
 __global__ void k_bisect(const TriJob* jobs, const int* mask);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
