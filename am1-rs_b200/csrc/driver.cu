@@ -60,10 +60,21 @@ struct DeviceCtx {
     DevElem* d_params = nullptr;
     int sms = 0;
     int jacobi_smem = 0;  // dynamic shared memory available to one eigensolver CTA
+    int tridiag_smem = 0;  // ... and to one tridiagonalisation CTA
 };
 
-// Shared-memory budget the planner sizes eigensolver clusters for (set when a device is opened).
+// Shared-memory budgets the planner sizes eigensolver and tridiagonalisation clusters for (set
+// when a device is opened).
 int g_jacobi_budget = 232448 - 1024;
+int g_tridiag_budget = 232448 - 1024;
+
+// Smallest cluster (1, 2, 4, 8, 16 CTAs) whose row share of an n x n matrix fits one CTA's
+// shared memory; 0 when none does.
+int tridiag_cluster(int n) {
+    for (int C = 1; C <= 16; C *= 2)
+        if (tridiag_smem_bytes(n, C) <= (size_t)g_tridiag_budget) return C;
+    return 0;
+}
 
 DeviceCtx g_dev[64];
 
@@ -95,15 +106,25 @@ int device_ctx(DeviceCtx** out) {
             return bad("jacobi smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("jacobi cluster attribute", err);
+        if ((err = cudaFuncGetAttributes(&fa, k_tridiag)) != cudaSuccess) return bad("tridiag attributes", err);
+        c.tridiag_smem = optin - (int)fa.sharedSizeBytes;
+        if ((err = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, c.tridiag_smem)) != cudaSuccess)
+            return bad("tridiag smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+            return bad("tridiag cluster attribute", err);
         if ((err = cudaFuncSetAttribute(k_sp2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
             cudaSuccess)
             return bad("sp2 smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_dgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
             cudaSuccess)
             return bad("dgemm smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_commutator, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
+            cudaSuccess)
+            return bad("commutator smem attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
+    g_tridiag_budget = c.tridiag_smem;
     *out = &c;
     return AM1GPU_OK;
 }
@@ -352,13 +373,14 @@ struct Batch {
     long long* d_pair_prefix;
     ChanJob* d_jobs;
     int* d_job0;
-    GemmJob *d_gj_fp, *d_gj_gt, *d_gj_dn;
-    GemmTile *d_gt_fp, *d_gt_gt, *d_gt_dn;
-    int nt_fp = 0, nt_gt = 0, nt_dn = 0;
+    GemmJob *d_gj_gt, *d_gj_dn;
+    GemmTile *d_gt_gt, *d_gt_dn;
+    int nt_gt = 0, nt_dn = 0;
     EigJob* d_eig;
     int neig = 0;
     struct Bucket { int off, count, C; size_t smem; };
-    std::vector<Bucket> buckets;
+    std::vector<Bucket> buckets;      // eigensolver jobs by cluster size
+    std::vector<Bucket> tri_buckets;  // tridiagonalisation jobs by cluster size
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;
     int nt_sp2 = 0, sp2_nblk = 1;
@@ -432,10 +454,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_pp = take(st, sizeof(long long) * (b.nmol + 1));
     const size_t o_jobs = take(st, sizeof(ChanJob) * nch_total);
     const size_t o_job0 = take(st, sizeof(int) * b.nmol);
-    const size_t o_gfp = take(st, sizeof(GemmJob) * nch_total);
     const size_t o_ggt = take(st, sizeof(GemmJob) * nch_total);
     const size_t o_gdn = take(st, sizeof(GemmJob) * nch_total);
-    const size_t o_tfp = take(st, sizeof(GemmTile) * tiles_nn);
     const size_t o_tgt = take(st, sizeof(GemmTile) * tiles_nn);
     const size_t o_tdn = take(st, sizeof(GemmTile) * tiles_nn);
     const size_t o_eig = take(st, sizeof(EigJob) * nch_total);
@@ -460,7 +480,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     for (auto& p : b.plans) {
         const long long tn = (p.nao + 63) / 64;
         const long long sp2part = 2 * std::max<long long>(sp2_nblk, tn * (tn + 1) / 2);
-        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + 96);
+        const long long cpart = CP_N * tn * (tn + 1) / 2;
+        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 128);
     }
     const size_t o_misc = take(dv, sizeof(double) * misc);
     const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
@@ -486,10 +507,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_pair_prefix = (long long*)dptr(o_pp);
     b.d_jobs = (ChanJob*)dptr(o_jobs);
     b.d_job0 = (int*)dptr(o_job0);
-    b.d_gj_fp = (GemmJob*)dptr(o_gfp);
     b.d_gj_gt = (GemmJob*)dptr(o_ggt);
     b.d_gj_dn = (GemmJob*)dptr(o_gdn);
-    b.d_gt_fp = (GemmTile*)dptr(o_tfp);
     b.d_gt_gt = (GemmTile*)dptr(o_tgt);
     b.d_gt_dn = (GemmTile*)dptr(o_tdn);
     b.d_eig = (EigJob*)dptr(o_eig);
@@ -524,10 +543,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     long long* hpp = (long long*)(Hs + o_pp);
     ChanJob* hj = (ChanJob*)(Hs + o_jobs);
     int* hj0 = (int*)(Hs + o_job0);
-    GemmJob* hgfp = (GemmJob*)(Hs + o_gfp);
     GemmJob* hggt = (GemmJob*)(Hs + o_ggt);
     GemmJob* hgdn = (GemmJob*)(Hs + o_gdn);
-    GemmTile* htfp = (GemmTile*)(Hs + o_tfp);
     GemmTile* htgt = (GemmTile*)(Hs + o_tgt);
     GemmTile* htdn = (GemmTile*)(Hs + o_tdn);
     EigJob* heig = (EigJob*)(Hs + o_eig);
@@ -540,6 +557,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     int atom_base = 0, job = 0, ntile = 0, cid_off = 0;
     std::vector<EigJob> eig_all;
     std::vector<int> eig_cluster;
+    std::vector<TriJob> tri_all;
     for (int mi = 0; mi < b.nmol; ++mi) {
         MolPlan& p = b.plans[mi];
         const am1gpu_molecule& m = in[p.user];
@@ -585,7 +603,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             cj.ch = c;
             cj.n = (int)n;
             cj.F = base + SLOT_F * nn;
-            cj.FP = base + SLOT_FP * nn;
+            cj.Fx = base + SLOT_FX * nn;
             cj.P = base + SLOT_P * nn;
             cj.Ct = base + SLOT_CT * nn;
             cj.Pnew = base + SLOT_GT * nn;
@@ -620,10 +638,13 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             mi_off += (long long)nblk * RED_N;
             cj.red2 = d_misc + mi_off;
             mi_off += nblk;
+            cj.ntiles = (int)(tn_ * (tn_ + 1) / 2);
+            cj.cpart = d_misc + mi_off;
+            mi_off += (long long)CP_N * cj.ntiles;
             mi_off = (mi_off + 31) & ~31LL;
             hj[job] = cj;
             Sp2Job sj{};
-            sj.F = cj.FP;
+            sj.F = cj.Fx;
             sj.rowmin = cj.rowmin;
             sj.rowmax = cj.rowmax;
             sj.X0 = base + SLOT_GT * nn;
@@ -640,22 +661,19 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.ntiles = nsp2t - sj.tile0;
             hsp2[job] = sj;
             TriJob tj{};
-            tj.A = cj.FP;
-            tj.W = base + SLOT_VS * nn;
+            tj.A = cj.Fx;
             tj.d = tri_d;
             tj.e = tri_e;
             tj.eps = cj.eps;
             tj.n = (int)n;
             tj.mol = mi;
-            htri[job] = tj;
-            // GEMMs: F.P, C^T F*, w C_occ^T C_occ
-            hgfp[job] = GemmJob{cj.F, cj.P, cj.FP, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
-            hggt[job] = GemmJob{cj.Ct, cj.FP, base + SLOT_GT * nn, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
+            tri_all.push_back(tj);
+            // GEMMs of the eigensolver path: C^T F*, w C_occ^T C_occ
+            hggt[job] = GemmJob{cj.Ct, cj.Fx, base + SLOT_GT * nn, (int)n, (int)n, (int)n, (int)n, (int)n, (int)n, 1.0, mi};
             hgdn[job] = GemmJob{cj.Ct, cj.Ct, cj.Pnew, (int)n, (int)n, p.n_occ[c], (int)n, (int)n, (int)n, md.occ_weight, mi};
             const int tn = (int)((n + 63) / 64);
             for (int x = 0; x < tn; ++x)
                 for (int y = 0; y < tn; ++y) {
-                    htfp[ntile] = GemmTile{job, x, y};
                     htgt[ntile] = GemmTile{job, x, y};
                     htdn[ntile] = GemmTile{job, x, y};
                     ++ntile;
@@ -686,7 +704,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         hst[mi] = s;
     }
     hpp[b.nmol] = a_off;
-    b.nt_fp = b.nt_gt = b.nt_dn = ntile;
+    b.nt_gt = b.nt_dn = ntile;
     b.nt_sp2 = nsp2t;
     // eigen jobs grouped by cluster size, largest first inside a group
     std::vector<int> idx(eig_all.size());
@@ -705,6 +723,20 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         b.buckets.back().smem = std::max(b.buckets.back().smem, sm);
     }
     b.neig = (int)idx.size();
+    // tridiagonalisation jobs grouped by cluster size, largest first
+    std::vector<int> tix(tri_all.size());
+    for (size_t i = 0; i < tix.size(); ++i) tix[i] = (int)i;
+    std::stable_sort(tix.begin(), tix.end(), [&](int x, int y) { return tri_all[x].n > tri_all[y].n; });
+    b.tri_buckets.clear();
+    for (size_t i = 0; i < tix.size(); ++i) {
+        const TriJob& tj = tri_all[tix[i]];
+        htri[i] = tj;
+        const int C = tridiag_cluster(tj.n);
+        if (!C) return fail(AM1GPU_UNSUPPORTED, "matrix too large for the on-chip tridiagonalisation");
+        if (b.tri_buckets.empty() || b.tri_buckets.back().C != C) b.tri_buckets.push_back({(int)i, 0, C, 0});
+        b.tri_buckets.back().count++;
+        b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tj.n, C));
+    }
     b.mols.assign(hm, hm + b.nmol);
     b.jobs.assign(hj, hj + job);
     b.job0.assign(hj0, hj0 + b.nmol);
@@ -734,6 +766,26 @@ int launch_core(Batch& b, Mem* ws, const DevElem* dp, Run* run) {
     ++k;
     CK(cudaGetLastError());
     if (run) run->launched(AM1GPU_PHASE_CORE, k);
+    return AM1GPU_OK;
+}
+
+// One cluster of C CTAs per matrix, one launch per cluster size.
+int launch_tridiag(Batch& b, Mem* ws) {
+    for (auto& bk : b.tri_buckets) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(bk.count * bk.C, 1, 1);
+        cfg.blockDim = dim3(512, 1, 1);
+        cfg.dynamicSmemBytes = bk.smem;
+        cfg.stream = ws->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = bk.C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_tridiag, (const TriJob*)(b.d_tri + bk.off), (const int*)nullptr));
+    }
     return AM1GPU_OK;
 }
 
@@ -797,7 +849,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                                                       b.d_st, 0);
             run.launched(AM1GPU_PHASE_FOCK);
             if ((rc = run.end(AM1GPU_PHASE_FOCK, ph)) || (rc = run.begin(&ph))) return rc;
-            k_dgemm_nn<<<b.nt_fp, 128, dgemm_smem_bytes(), s>>>(b.d_gj_fp, b.d_gt_fp, b.nt_fp, b.d_st, 0, nullptr);
+            k_commutator<<<b.nt_sp2, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, b.d_sp2_tiles, b.nt_sp2, b.d_st);
             k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
             run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
             if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, ph)) || (rc = run.begin(&ph))) return rc;
@@ -869,11 +921,11 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 1, 1);
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
     // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
-    k_tridiag<<<njobs, 256, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);
+    if ((rc = launch_tridiag(b, ws))) return rc;
     k_bisect<<<njobs, 128, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
-    run.launched(AM1GPU_PHASE_FINAL, 6);
+    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size());
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;
@@ -966,7 +1018,7 @@ int write_result(Batch& b, Mem* ws, int mi, am1gpu_result* r, am1gpu_call_stats*
         if (c_out) {
             if (density_mode() == 0) {
                 // the purification path has no eigenvectors: diagonalise the last F* now
-                int rc = fetch_matrix(ws, jc.FP, n, t0, stats);
+                int rc = fetch_matrix(ws, jc.Fx, n, t0, stats);
                 if (rc) return rc;
                 std::vector<double> wv(n), vv((size_t)n * n);
                 rc = symmetric_eigen_one(n, t0.data(), wv.data(), vv.data(), &tl_mem_eig);
