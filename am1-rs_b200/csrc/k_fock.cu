@@ -1,15 +1,15 @@
 // Fock G(P) build: F^s = H_core + J(P_tot) - K(spin_scale * P^s), am1-rs src/fock.rs:249-511.
 //
-// One warp per atom A.  The warp walks every partner B of its molecule in order and
-//   * accumulates the Coulomb term of A's diagonal block, J_A = sum_B (A A | B B) . P_BB
-//     (the reference's ja/jb, src/fock.rs:427-448) in registers -- a gather, so the sum is
-//     deterministic and needs no atomics;
-//   * for B > A (A is then the pair's first, heavier atom) computes the exchange block
-//     K_AB = -s sum P^s_ab (mu nu | lambda sigma) (src/fock.rs:449-466) for every spin channel
-//     and writes F_AB = H_AB + K_AB into both triangles; each off-diagonal block has exactly one
-//     writer.
-// Each pair's integral block is staged through shared memory once per visit with coalesced
-// loads; lanes 0..15 own the 16 exchange outputs, lanes 16..25 the 10 Coulomb outputs.
+// One warp per atom A; every off-diagonal block has exactly one writer and every sum is a
+// gather in a fixed order, so the result is deterministic and needs no atomics.
+//   * heavy partners B of a heavy A (100-integral blocks, src/fock.rs:427-466): one pair at a
+//     time, the block staged through shared memory with coalesced loads; lanes 16..25 gather the
+//     Coulomb term J_A = sum_B (A A | B B) . P_BB, lanes 0..15 the 16 exchange outputs
+//     K_AB = -s sum P^s_ab (mu nu | lambda sigma) when B > A, written to F_AB and F_BA;
+//   * every other partner (a hydrogen B, or any B of a hydrogen A: blocks of 10 or 1 integrals)
+//     is handled lane-parallel, 32 partners at a time: each lane gathers its partner's share of
+//     J_A in registers (reduced over the warp once per atom) and writes the exchange column
+//     F_AB, F_BA of its partner when A is the pair's first atom.
 // The one-centre terms (oc_two_electron, src/fock.rs:27-65 and 321-344) finish the diagonal.
 #include <cuda_runtime.h>
 
@@ -18,10 +18,9 @@
 
 namespace am1 {
 
-__device__ __forceinline__ int pack2(int a, int b) {
-    const int hi = a > b ? a : b, lo = a > b ? b : a;
-    return hi * (hi + 1) / 2 + lo;
-}
+// packed index of the AO pair (a, b) of one atom (0..9); constexpr, so unrolled loops index
+// register arrays with it at compile time
+__host__ __device__ constexpr int pack2(int a, int b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; }
 
 // One-centre integral (a b | c d) of one atom (src/fock.rs:27-65).
 __device__ __forceinline__ double oc_integral(int a, int b, int c, int d, const DevElem& e) {
@@ -37,6 +36,10 @@ __device__ __forceinline__ double oc_integral(int a, int b, int c, int d, const 
 }
 
 constexpr int FOCK_WARPS = 8;
+
+// the AO pair of packed index q (inverse of pack2)
+__host__ __device__ constexpr int pair_hi(int q) { return q < 1 ? 0 : q < 3 ? 1 : q < 6 ? 2 : 3; }
+__host__ __device__ constexpr int pair_lo(int q) { return q - pair_hi(q) * (pair_hi(q) + 1) / 2; }
 
 __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restrict__ mols, const int* __restrict__ atom_mol,
                                                          int natoms_total, const DevElem* __restrict__ params,
@@ -57,6 +60,8 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
     const double* H0 = arena + md.h_base;
     const double* P0 = arena + md.ch_base[0] + SLOT_P * nn;
     const double* P1 = md.nch == 2 ? arena + md.ch_base[1] + SLOT_P * nn : nullptr;
+    double* F0 = arena + md.ch_base[0] + SLOT_F * nn;
+    double* F1 = md.nch == 2 ? arena + md.ch_base[1] + SLOT_F * nn : nullptr;
     const double sc = md.spin_scale;
     const long long xxsz = 100LL * h * (h - 1) / 2, xhsz = 10LL * h * Hn;
     const double* w = wstore + md.w_base;
@@ -65,83 +70,141 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
     const int naA = aheavy ? 4 : 1;
     const int npA = aheavy ? 10 : 1;
     double* wb = s_w[warp];
-    double jacc = 0.0;  // lane 16 + k owns J_A[k]
-
     auto ptot = [&](long long idx) { return P1 ? P0[idx] + P1[idx] : P0[idx]; };
 
-    for (int B = 0; B < N; ++B) {
-        if (B == A) continue;
-        const bool bheavy = B < h;
-        const int oB = bheavy ? 4 * B : 4 * h + (B - h);
-        const int naB = bheavy ? 4 : 1, npB = bheavy ? 10 : 1;
-        const int i = min(A, B), j = max(A, B);
-        const double* blk;
-        int sz;
-        if (j < h) {
-            blk = w + 100LL * ((long long)i * h - (long long)i * (i + 1) / 2 + (j - i - 1));
-            sz = 100;
-        } else if (i < h) {
-            blk = w + xxsz + 10LL * ((long long)i * Hn + (j - h));
-            sz = 10;
-        } else {
-            const int i2 = i - h, j2 = j - h;
-            blk = w + xxsz + xhsz + ((long long)i2 * Hn - (long long)i2 * (i2 + 1) / 2 + (j2 - i2 - 1));
-            sz = 1;
-        }
-        for (int l = lane; l < sz; l += 32) wb[l] = blk[l];
-        if (lane < npB) {
-            // packed P_BB with the off-diagonal pairs counted twice
-            int hi = 0;
-            while ((hi + 1) * (hi + 2) / 2 <= lane) ++hi;
-            const int lo = lane - hi * (hi + 1) / 2;
-            const double v = ptot((long long)(oB + hi) * n + oB + lo);
-            s_q[warp][lane] = hi == lo ? v : 2.0 * v;
-        }
-        const bool do_k = B > A;
-        if (do_k && lane < 16) {
-            const int nu = lane >> 2, sg = lane & 3;
-            if (nu < naA && sg < naB) {
-                const long long idx = (long long)(oA + nu) * n + oB + sg;
+    double jacc = 0.0;  // heavy-heavy part: lane 16 + k owns J_A[k]
+    if (aheavy) {
+        for (int B = 0; B < h; ++B) {
+            if (B == A) continue;
+            const int oB = 4 * B;
+            const int i = min(A, B), j = max(A, B);
+            const double* blk = w + 100LL * ((long long)i * h - (long long)i * (i + 1) / 2 + (j - i - 1));
+            for (int l = lane; l < 100; l += 32) wb[l] = blk[l];
+            if (lane < 10) {  // packed P_BB, off-diagonal pairs counted twice
+                const int hi = pair_hi(lane), lo = pair_lo(lane);
+                const double v = ptot((long long)(oB + hi) * n + oB + lo);
+                s_q[warp][lane] = hi == lo ? v : 2.0 * v;
+            }
+            const bool do_k = B > A;
+            if (do_k && lane < 16) {
+                const long long idx = (long long)(oA + (lane >> 2)) * n + oB + (lane & 3);
                 s_pab[warp][0][lane] = P0[idx];
                 if (P1) s_pab[warp][1][lane] = P1[idx];
             }
-        }
-        __syncwarp();
-        // Coulomb: the A-side of the block is its rows when A is the first atom, else its columns
-        if (lane >= 16 && lane < 16 + npA) {
-            const int k = lane - 16;
-            double acc = 0.0;
-            if (A == i) {
-                for (int q = 0; q < npB; ++q) acc += wb[k * npB + q] * s_q[warp][q];
-            } else {
-                for (int q = 0; q < npB; ++q) acc += wb[q * npA + k] * s_q[warp][q];
+            __syncwarp();
+            if (lane >= 16 && lane < 26) {
+                // Coulomb: A's side of the block is its rows when A is the first atom, else its columns
+                const int k = lane - 16;
+                double acc = 0.0;
+                if (A == i) {
+#pragma unroll
+                    for (int q = 0; q < 10; ++q) acc += wb[k * 10 + q] * s_q[warp][q];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 10; ++q) acc += wb[q * 10 + k] * s_q[warp][q];
+                }
+                jacc += acc;
             }
-            jacc += acc;
-        }
-        // Exchange block (A = first atom, B = second)
-        if (do_k && lane < 16) {
-            const int mu = lane >> 2, la = lane & 3;
-            if (mu < naA && la < naB) {
-                const int ncol = npB;
+            if (do_k && lane < 16) {  // exchange block (A = first atom, B = second)
+                const int mu = lane >> 2, la = lane & 3;
+                const long long ab = (long long)(oA + mu) * n + oB + la;
+                const long long ba = (long long)(oB + la) * n + oA + mu;
+                const double hab = H0[ab];
                 for (int c = 0; c < md.nch; ++c) {
                     double acc = 0.0;
-                    for (int nu = 0; nu < naA; ++nu) {
-                        const double* row = wb + pack2(mu, nu) * ncol;
-                        for (int sg = 0; sg < naB; ++sg) acc += s_pab[warp][c][nu * 4 + sg] * row[pack2(la, sg)];
+#pragma unroll
+                    for (int nu = 0; nu < 4; ++nu) {
+                        const double* row = wb + pack2(mu, nu) * 10;
+#pragma unroll
+                        for (int sg = 0; sg < 4; ++sg) acc += s_pab[warp][c][nu * 4 + sg] * row[pack2(la, sg)];
                     }
-                    const double kval = -(acc * sc);
-                    double* F = arena + md.ch_base[c] + SLOT_F * nn;
-                    const long long ab = (long long)(oA + mu) * n + oB + la;
-                    const long long ba = (long long)(oB + la) * n + oA + mu;
-                    const double v = H0[ab] + kval;
+                    const double v = hab - acc * sc;
+                    double* F = c == 0 ? F0 : F1;
+                    F[ab] = v;
+                    F[ba] = v;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    // every other partner, lane-parallel
+    double jl[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) jl[k] = 0.0;
+    if (aheavy) {
+        // hydrogen partners B (XH blocks: A's 10 packed pairs x B's ss); A is the first atom
+        for (int B = h + lane; B < N; B += 32) {
+            const int oB = 4 * h + (B - h);
+            const double* blk = w + xxsz + 10LL * ((long long)A * Hn + (B - h));
+            double wv[10];
+#pragma unroll
+            for (int k = 0; k < 10; ++k) wv[k] = blk[k];
+            const double pbb = ptot((long long)oB * n + oB);
+#pragma unroll
+            for (int k = 0; k < 10; ++k) jl[k] += wv[k] * pbb;
+            const double* Hrow = H0 + (long long)oB * n + oA;
+            for (int c = 0; c < md.nch; ++c) {
+                const double* Pr = (c == 0 ? P0 : P1) + (long long)oB * n + oA;  // P_BA = P_AB (symmetric)
+                const double p0 = Pr[0], p1 = Pr[1], p2 = Pr[2], p3 = Pr[3];
+                double* F = c == 0 ? F0 : F1;
+#pragma unroll
+                for (int mu = 0; mu < 4; ++mu) {
+                    const double acc = p0 * wv[pack2(mu, 0)] + p1 * wv[pack2(mu, 1)] + p2 * wv[pack2(mu, 2)] + p3 * wv[pack2(mu, 3)];
+                    const double v = Hrow[mu] - acc * sc;
+                    F[(long long)oB * n + oA + mu] = v;
+                    F[(long long)(oA + mu) * n + oB] = v;
+                }
+            }
+        }
+    } else {
+        const int A2 = A - h;
+        // heavy partners B (XH block of (B, A): B's 10 packed pairs x A's ss); B is the first atom
+        for (int B = lane; B < h; B += 32) {
+            const int oB = 4 * B;
+            const double* blk = w + xxsz + 10LL * ((long long)B * Hn + A2);
+            double acc = 0.0;
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                const int hi = pair_hi(q), lo = pair_lo(q);
+                const double v = ptot((long long)(oB + hi) * n + oB + lo);
+                acc += blk[q] * (hi == lo ? v : 2.0 * v);
+            }
+            jl[0] += acc;
+        }
+        // hydrogen partners B (HH blocks); exchange when A is the first atom (B > A)
+        for (int B = h + lane; B < N; B += 32) {
+            if (B == A) continue;
+            const int B2 = B - h;
+            const int i2 = min(A2, B2), j2 = max(A2, B2);
+            const double wv = w[xxsz + xhsz + ((long long)i2 * Hn - (long long)i2 * (i2 + 1) / 2 + (j2 - i2 - 1))];
+            const int oB = 4 * h + B2;
+            jl[0] += wv * ptot((long long)oB * n + oB);
+            if (B > A) {
+                const long long ab = (long long)oA * n + oB, ba = (long long)oB * n + oA;
+                const double hab = H0[ab];
+                for (int c = 0; c < md.nch; ++c) {
+                    const double v = hab - sc * (c == 0 ? P0 : P1)[ab] * wv;
+                    double* F = c == 0 ? F0 : F1;
                     F[ab] = v;
                     F[ba] = v;
                 }
             }
         }
-        __syncwarp();
     }
-    if (lane >= 16 && lane < 16 + npA) s_j[warp][lane - 16] = jacc;
+    // J_A = heavy-heavy part (lanes 16..25) + the lane-parallel part (reduced over the warp)
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        double v = jl[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        jl[k] = v;
+    }
+    if (lane == 0) {  // s_q is free after the heavy-heavy loop
+#pragma unroll
+        for (int k = 0; k < 10; ++k) s_q[warp][k] = jl[k];
+    }
+    __syncwarp();
+    if (lane >= 16 && lane < 16 + npA) s_j[warp][lane - 16] = jacc + s_q[warp][lane - 16];
     __syncwarp();
     // one-centre terms and the diagonal block
     if (lane < 16) {
@@ -158,7 +221,7 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
                         acc -= sc * Pc[idx] * oc_integral(mu, la, nu, sg, e);
                     }
                 const long long d = (long long)(oA + mu) * n + oA + nu;
-                double* F = arena + md.ch_base[c] + SLOT_F * nn;
+                double* F = c == 0 ? F0 : F1;
                 F[d] = H0[d] + acc + s_j[warp][pack2(mu, nu)];
             }
         }
