@@ -17,32 +17,47 @@ namespace cg = cooperative_groups;
 // Householder reduction of one symmetric matrix held on chip.  The n x n matrix is distributed by
 // rows over a thread-block cluster of C CTAs (row r lives in CTA r % C, at local row r / C, full
 // length n), so the whole reduction runs out of shared memory; C is the smallest cluster whose
-// share fits one CTA.  Step k (GVL Alg. 8.3.1; the reflector zeroes row/column k below the
-// subdiagonal):
-//   owner of row k:  x = A[k, k+1:], alpha = |x|, v = x + sign(x0) alpha e1, beta = 1/(alpha(alpha+|x0|))
-//   cluster sync #1; every CTA copies v and beta from the owner (distributed shared memory)
-//   every CTA:       p_r = beta A[r, k+1:] . v for its rows, sent to every CTA; its share of p.v
-//   cluster sync #2; w = p - (beta/2)(p.v) v;  A[r, k+1:] -= v_r w + w_r v for its rows
-// All control flow is uniform over the cluster (alpha = 0 gives beta = 0 and a no-op update),
-// so every CTA takes the same cluster barriers.
+// share fits one CTA.  Step k (GVL Alg. 8.3.1: the reflector I - beta v v^T zeroes row/column k
+// below the subdiagonal):
+//   sync #1   the owner of row k has v_k, beta_k ready; every other CTA copies them (distributed
+//             shared memory)
+//   p_r = beta A[r, k+1:] . v for the CTA's rows r > k, sent to every CTA with the warp's share of p.v
+//   sync #2   A[r, k+1:] -= v_r w + w_r v with w = p - (beta/2)(p.v) v, formed on the fly
+// Look-ahead: the warp that updates row k+1 (warp 0 of its owner) derives v_{k+1}, beta_{k+1}, d, e
+// from it at once, into the other half of the double-buffered v, so a step costs two cluster
+// barriers and one CTA barrier.  All control flow is uniform over the cluster (alpha = 0 gives
+// beta = 0 and a no-op update), so every CTA takes the same barriers.
 constexpr int TRI_THREADS = 512;
 constexpr int TRI_WARPS = TRI_THREADS / 32;
 
-// Dynamic shared memory of one CTA: local rows, v, p/w and the C partial sums of p.v.
+// Dynamic shared memory of one CTA: local rows, v (two buffers), p, the per-warp shares of p.v
+// from every CTA, beta (two buffers).
 size_t tridiag_smem_bytes(int n, int C) {
     const size_t rows = (size_t)(n + C - 1) / C;
-    return sizeof(double) * (rows * n + 2 * (size_t)n + 1 + 16);
+    return sizeof(double) * (rows * n + 3 * (size_t)n + (size_t)C * TRI_WARPS + 2);
 }
 
-__device__ __forceinline__ double tri_block_sum(double v, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    double s = 0.0;
-    for (int w = 0; w < TRI_WARPS; ++w) s += red[w];
-    return s;
+// Householder vector of row `row` (the trailing part from column c0 = k + 1), computed by one
+// warp: v = x + sign(x0) |x| e1 into vbuf, beta into *beta, and d[k], e[k].
+__device__ __forceinline__ void tri_reflector(const double* row, int k, int n, double* vbuf, double* beta, double* d, double* e) {
+    const int lane = threadIdx.x & 31, c0 = k + 1;
+    double nrm = 0.0;
+    for (int c = c0 + lane; c < n; c += 32) {
+        const double x = row[c];
+        vbuf[c] = x;
+        nrm += x * x;
+    }
+    for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    const double alpha = sqrt(nrm);
+    const double x0 = row[c0];
+    const double sg = x0 >= 0.0 ? 1.0 : -1.0;
+    __syncwarp();
+    if (lane == 0) {
+        d[k] = row[k];
+        e[k] = alpha == 0.0 ? 0.0 : -sg * alpha;
+        *beta = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x0)));
+        if (alpha != 0.0) vbuf[c0] = x0 + sg * alpha;
+    }
 }
 
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restrict__ jobs, const int* __restrict__ mask) {
@@ -54,11 +69,11 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
     const int n = jb.n;
     const int R = (n + C - 1) / C;
     extern __shared__ double sh[];
-    double* A = sh;            // R x n: global row lr * C + crank at local row lr
-    double* v = A + (size_t)R * n;
-    double* pw = v + n;        // p, then w (global column index)
-    double* sc = pw + n;       // sc[0] = beta, sc[1 + q] = CTA q's share of p.v
-    __shared__ double red[TRI_WARPS];
+    double* A = sh;                     // R x n: global row lr * C + crank at local row lr
+    double* vb = A + (size_t)R * n;     // v, two buffers of n (global column index)
+    double* p = vb + 2 * (size_t)n;     // p (global index)
+    double* part = p + n;               // [C * TRI_WARPS] shares of p.v
+    double* bb = part + C * TRI_WARPS;  // beta, two buffers
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     auto csync = [&]() {
         if (C > 1) cluster.sync();
@@ -70,39 +85,20 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
         for (int c = lane; c < n; c += 32) A[(size_t)lr * n + c] = jb.A[(size_t)r * n + c];
     }
     __syncthreads();
+    if (n >= 3 && crank == 0 && warp == 0) tri_reflector(A, 0, n, vb, bb, jb.d, jb.e);
     for (int k = 0; k + 2 < n; ++k) {
-        const int owner = k % C;
-        const int c0 = k + 1;  // trailing block: rows and columns c0 .. n-1
-        if (crank == owner) {
-            const double* rowk = A + (size_t)(k / C) * n;
-            double nrm = 0.0;
-            for (int c = c0 + tid; c < n; c += TRI_THREADS) {
-                const double x = rowk[c];
-                v[c] = x;
-                nrm += x * x;
-            }
-            nrm = tri_block_sum(nrm, red);
-            const double alpha = sqrt(nrm);
-            const double x0 = rowk[c0];
-            const double sg = x0 >= 0.0 ? 1.0 : -1.0;
-            if (tid == 0) {
-                jb.d[k] = rowk[k];
-                jb.e[k] = alpha == 0.0 ? 0.0 : -sg * alpha;
-                sc[0] = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x0)));
-                if (alpha != 0.0) v[c0] = x0 + sg * alpha;
-            }
-        }
-        csync();  // #1: v and beta are ready in the owner
+        const int par = k & 1, owner = k % C, c0 = k + 1;
+        double* v = vb + (size_t)par * n;
+        csync();  // #1: v_k and beta_k are ready in the owner
         if (crank != owner) {
             const double* rv = cluster.map_shared_rank(v, owner);
             for (int c = c0 + tid; c < n; c += TRI_THREADS) v[c] = rv[c];
-            if (tid == 0) sc[0] = *cluster.map_shared_rank(sc, owner);
+            if (tid == 0) bb[par] = *cluster.map_shared_rank(bb + par, owner);
+            __syncthreads();
         }
-        __syncthreads();
-        const double beta = sc[0];
-        // p_r = beta * A[r, c0:] . v for this CTA's rows r >= c0, one warp per row
+        const double beta = bb[par];
         const int lr0 = (c0 - crank + C - 1) / C;  // first local row with global index >= c0
-        double part = 0.0;
+        double wpart = 0.0;
         for (int lr = lr0 + warp; lr < R; lr += TRI_WARPS) {
             const int r = lr * C + crank;
             if (r >= n) break;
@@ -110,27 +106,30 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
             double acc = 0.0;
             for (int c = c0 + lane; c < n; c += 32) acc = fma(row[c], v[c], acc);
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            const double p = beta * acc;
-            if (lane < C) *cluster.map_shared_rank(&pw[r], lane) = p;  // to every CTA, itself included
-            part += p * v[r];
+            const double pr = beta * acc;
+            if (lane < C) *cluster.map_shared_rank(&p[r], lane) = pr;  // to every CTA, itself included
+            wpart += pr * v[r];
         }
-        part = tri_block_sum(lane == 0 ? part : 0.0, red);
-        if (tid < C) *cluster.map_shared_rank(&sc[1 + crank], tid) = part;
-        csync();  // #2: p and the shares of p.v are complete everywhere
+        if (lane < C) *cluster.map_shared_rank(&part[crank * TRI_WARPS + warp], lane) = wpart;
+        csync();  // #2: p and every share of p.v are complete everywhere
         double pv = 0.0;
-        for (int q = 0; q < C; ++q) pv += sc[1 + q];
+        for (int q = lane; q < C * TRI_WARPS; q += 32) pv += part[q];
+        for (int o = 16; o > 0; o >>= 1) pv += __shfl_xor_sync(0xffffffffu, pv, o);
         const double kk = 0.5 * beta * pv;
-        for (int c = c0 + tid; c < n; c += TRI_THREADS) pw[c] -= kk * v[c];  // pw <- w
-        __syncthreads();
         for (int lr = lr0 + warp; lr < R; lr += TRI_WARPS) {
             const int r = lr * C + crank;
             if (r >= n) break;
             double* row = A + (size_t)lr * n;
-            const double vr = v[r], wr = pw[r];
-            for (int c = c0 + lane; c < n; c += 32) row[c] -= vr * pw[c] + wr * v[c];
+            const double vr = v[r], wr = p[r] - kk * vr;
+            for (int c = c0 + lane; c < n; c += 32) row[c] -= vr * (p[c] - kk * v[c]) + wr * v[c];
+            // look-ahead: row k+1 is final now; its reflector is the next step's
+            if (r == c0 && c0 + 2 < n) {
+                __syncwarp();
+                tri_reflector(row, c0, n, vb + (size_t)(par ^ 1) * n, bb + (par ^ 1), jb.d, jb.e);
+            }
         }
-        __syncthreads();
     }
+    __syncthreads();
     // the last 2 x 2 block (or the 1 x 1 matrix)
     if (tid == 0) {
         if (n >= 2) {
