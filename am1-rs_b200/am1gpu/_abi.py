@@ -119,6 +119,7 @@ class CallStats(ctypes.Structure):
         ("eigen_fallbacks", ctypes.c_int32),
         ("purification_steps", ctypes.c_double),
         ("purification_flops", ctypes.c_double),
+        ("purification_bytes", ctypes.c_double),
     ]
 
 
@@ -167,6 +168,7 @@ def stats_dict(st: CallStats) -> dict:
         "eigen_fallbacks": int(st.eigen_fallbacks),
         "purification_steps": float(st.purification_steps),
         "purification_flops": float(st.purification_flops),
+        "purification_bytes": float(st.purification_bytes),
     }
 
 _lib = None

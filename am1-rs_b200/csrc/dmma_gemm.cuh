@@ -2,7 +2,8 @@
 // with mma.sync.m16n8k8.f64 (4 warps, each a 32x32 sub-tile of 2x4 MMA blocks) and a
 // STAGES-deep cp.async pipeline feeding shared memory, so global (L2) latency is overlapped
 // with the MMAs.  Row-major operands with arbitrary leading dimensions; out-of-range elements
-// are zero-filled by the copy itself (src-size 0).
+// are zero-filled by the copy itself (src-size 0).  Operands with even shapes and 16-byte
+// aligned rows are copied in 16-byte pairs (half the copy instructions), others element-wise.
 //
 // Fragment layout of m16n8k8 f64 (g = lane/4, t = lane%4):
 //   A (16x8, row): a0 (g, t)  a1 (g+8, t)  a2 (g, t+4)  a3 (g+8, t+4)
@@ -39,12 +40,24 @@ __device__ __forceinline__ int dg_col(int j, int e) {
     return (warp & 1) * 32 + j * 8 + (lane & 3) * 2 + (e & 1);
 }
 
-// 8-byte asynchronous copy; an invalid element reads nothing (src-size 0) from the operand's
-// base address and is zero-filled.
+// 8- and 16-byte asynchronous copies; an invalid element reads nothing (src-size 0) from the
+// operand's base address and is zero-filled.
 __device__ __forceinline__ void dg_cp8(double* smem_dst, const double* gsrc, const double* base, bool valid) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     const int bytes = valid ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(valid ? gsrc : base), "r"(bytes));
+}
+__device__ __forceinline__ void dg_cp16(double* smem_dst, const double* gsrc, const double* base, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    const int bytes = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(valid ? gsrc : base), "r"(bytes));
+}
+
+// True when both operands can be copied in 16-byte pairs: 16-byte aligned bases, even leading
+// dimensions (every row starts on a pair), and even K and N (a pair never straddles an edge).
+__device__ __forceinline__ bool dg_pairs_ok(const double* A, int lda, const double* B, int ldb, int N, int K) {
+    return ((reinterpret_cast<unsigned long long>(A) | reinterpret_cast<unsigned long long>(B)) & 15ull) == 0 &&
+           ((lda | ldb | N | K) & 1) == 0;
 }
 __device__ __forceinline__ void dg_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -52,13 +65,26 @@ __device__ __forceinline__ void dg_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Issue the copies of k-tile kt into pipeline stage `st`.
+// Issue the copies of k-tile kt into pipeline stage `st` (16-byte pairs when `pairs`).
 __device__ __forceinline__ void dg_load(double* smem, int st, const double* __restrict__ A, int lda, const double* __restrict__ B,
-                                        int ldb, int M, int N, int K, int m0, int n0, int kt) {
+                                        int ldb, int M, int N, int K, int m0, int n0, int kt, bool pairs) {
     double* As = smem + st * DG_STAGE;
     double* Bs = As + DG_TILE * DG_AS;
     const int k0 = kt * DG_BK;
     const int tid = threadIdx.x;
+    if (pairs) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int idx = tid + l * DG_THREADS;
+            const int ar = idx >> 3, ak = (idx & 7) * 2;
+            const int gi = m0 + ar, gk = k0 + ak;
+            dg_cp16(&As[ar * DG_AS + ak], A + (long long)gi * lda + gk, A, gi < M && gk < K);
+            const int bk = idx >> 5, bc = (idx & 31) * 2;
+            const int gbk = k0 + bk, gj = n0 + bc;
+            dg_cp16(&Bs[bk * DG_BS + bc], B + (long long)gbk * ldb + gj, B, gbk < K && gj < N);
+        }
+        return;
+    }
 #pragma unroll
     for (int l = 0; l < 8; ++l) {
         const int idx = tid + l * DG_THREADS;
@@ -87,16 +113,17 @@ __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restri
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     const int KT = (K + DG_BK - 1) / DG_BK;
+    const bool pairs = dg_pairs_ok(A, lda, B, ldb, N, K);
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {
-        if (s < KT) dg_load(smem, s, A, lda, B, ldb, M, N, K, m0, n0, s);
+        if (s < KT) dg_load(smem, s, A, lda, B, ldb, M, N, K, m0, n0, s, pairs);
         dg_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
         dg_wait<DG_STAGES - 2>();
         __syncthreads();
         const int nk = kt + DG_STAGES - 1;
-        if (nk < KT) dg_load(smem, nk % DG_STAGES, A, lda, B, ldb, M, N, K, m0, n0, nk);
+        if (nk < KT) dg_load(smem, nk % DG_STAGES, A, lda, B, ldb, M, N, K, m0, n0, nk, pairs);
         dg_commit();
         const double* As = smem + (kt % DG_STAGES) * DG_STAGE;
         const double* Bs = As + DG_TILE * DG_AS;
@@ -145,11 +172,12 @@ __device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __r
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     const int KT = (n + DG_BK - 1) / DG_BK;  // k-tiles per product
+    const bool pairs = dg_pairs_ok(A1, ld, B1, ld, n, n) && dg_pairs_ok(A2, ld, B2, ld, n, n);
     auto load = [&](int st, int kt) {
         if (kt < KT)
-            dg_load(smem, st, A1, ld, B1, ld, n, n, n, m0, n0, kt);
+            dg_load(smem, st, A1, ld, B1, ld, n, n, n, m0, n0, kt, pairs);
         else
-            dg_load(smem, st, A2, ld, B2, ld, n, n, n, m0, n0, kt - KT);
+            dg_load(smem, st, A2, ld, B2, ld, n, n, n, m0, n0, kt - KT, pairs);
     };
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {

@@ -115,9 +115,6 @@ int device_ctx(DeviceCtx** out) {
         if ((err = cudaFuncSetAttribute(k_sp2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
             cudaSuccess)
             return bad("sp2 smem attribute", err);
-        if ((err = cudaFuncSetAttribute(k_dgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
-            cudaSuccess)
-            return bad("dgemm smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_commutator, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
             cudaSuccess)
             return bad("commutator smem attribute", err);
@@ -388,7 +385,7 @@ struct Batch {
     TriJob* d_tri;
     int* d_need_eigen;
     int* d_sp2_active;
-    double* d_work;  // [0] purification steps, [1] their flops, [2] eigensolver fallbacks
+    double* d_work;  // [0] purification steps, [1] their flops, [2] eigensolver fallbacks, [3] their bytes
     MolState* d_st;
     int* d_status;
     double *d_wstore, *d_ecc, *d_arena, *d_res, *d_charges;
@@ -481,7 +478,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         const long long tn = (p.nao + 63) / 64;
         const long long sp2part = 2 * std::max<long long>(sp2_nblk, tn * (tn + 1) / 2);
         const long long cpart = CP_N * tn * (tn + 1) / 2;
-        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 128);
+        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 2 + 128);
     }
     const size_t o_misc = take(dv, sizeof(double) * misc);
     const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
@@ -632,6 +629,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             const long long tn_ = (n + 63) / 64;
             double* sp2part = d_misc + mi_off;
             mi_off += 2 * std::max<long long>(sp2_nblk, tn_ * (tn_ + 1) / 2);
+            double* sp2bounds = d_misc + mi_off;
+            mi_off += 2;
             double* lam = d_misc + mi_off;
             mi_off += p.npad;
             cj.red = d_misc + mi_off;
@@ -651,6 +650,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.X1 = base + SLOT_VS * nn;
             sj.P = cj.Pnew;
             sj.part = sp2part;
+            sj.bounds = sp2bounds;
             sj.nocc = (double)p.n_occ[c];
             sj.weight = md.occ_weight;
             sj.n = (int)n;
@@ -859,10 +859,11 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
             if ((rc = run.end(AM1GPU_PHASE_ACCEL, ph)) || (rc = run.begin(&ph))) return rc;
             if (density_mode() == 0) {
                 // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
+                k_sp2_bounds<<<njobs, 256, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
                 k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
                 k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
                 CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
-                run.launched(AM1GPU_PHASE_EIGEN, 2);
+                run.launched(AM1GPU_PHASE_EIGEN, 3);
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
@@ -934,6 +935,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     CK(cudaStreamSynchronize(s));
     stats->purification_steps += b.h_work[0];
     stats->purification_flops += b.h_work[1];
+    stats->purification_bytes += b.h_work[3];
     stats->eigen_fallbacks += (int32_t)b.h_work[2];
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, mem.events[t0], mem.events[t1]));

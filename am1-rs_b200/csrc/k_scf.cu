@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
 // <e, e_slot> for every live slot (the new CDIIS Gram row).
 __global__ void __launch_bounds__(DG_THREADS, 4) k_commutator(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
                                                               int ntiles, const MolState* __restrict__ st) {
-    extern __shared__ double dsm[];
+    extern __shared__ __align__(16) double dsm[];
     __shared__ double red[CP_N][4];
     const int t = blockIdx.x;
     if (t >= ntiles) return;

@@ -20,6 +20,191 @@
 namespace am1 {
 
 
+// Spectral bounds [e_min, e_max] of F* for the SP2 mapping.  The number of purification steps
+// grows with the width of the interval, and the Gershgorin interval of an NDDO Fock matrix is
+// about twice the true spectral width (the row sums over the many small long-range elements), so
+// the bounds come from a short Lanczos run (SP2_LANCZOS steps from a fixed start vector, no
+// reorthogonalisation: only the extreme Ritz values are used):
+//     e_max = min(Gershgorin max, theta_max + r_max + 0.005 w)
+//     e_min = max(Gershgorin min, theta_min - r_min - 0.005 w)
+// with r = |beta_m s_m| the residual of the extreme Ritz pair (s from inverse iteration on the
+// Lanczos tridiagonal T) and w = theta_max - theta_min.  An eigenvalue left slightly outside
+// the interval maps just outside [0, 1], where the trace-correcting steps pull it back; a run
+// that still fails to converge falls back to the eigensolver.  One CTA per channel.
+constexpr int SP2_LANCZOS = 12;
+constexpr int SP2_BOUND_THREADS = 256;
+
+__device__ double bounds_block_sum(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < SP2_BOUND_THREADS / 32; ++w) t += red[w];
+    return t;
+}
+
+// Eigenvalues of T (m x m, diagonal a, off-diagonal b) below x.
+__device__ int lz_count(const double* a, const double* b, int m, double x) {
+    int c = 0;
+    double q = a[0] - x;
+    if (q < 0.0) ++c;
+    for (int i = 1; i < m; ++i) {
+        q = a[i] - x - b[i - 1] * b[i - 1] / (q == 0.0 ? 1e-300 : q);
+        if (q < 0.0) ++c;
+    }
+    return c;
+}
+
+// k-th smallest eigenvalue of T by bisection inside [lo, hi].
+__device__ double lz_eig(const double* a, const double* b, int m, int k, double lo, double hi) {
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (!(mid > lo && mid < hi)) break;
+        if (lz_count(a, b, m, mid) <= k) lo = mid;
+        else hi = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+
+// |last component| of the unit eigenvector of T for an exterior eigenvalue: inverse iteration
+// with the shift sigma just outside the spectrum, so T - sigma I is definite and the
+// tridiagonal solve needs no pivoting.
+__device__ double lz_last_component(const double* a, const double* b, int m, double sigma) {
+    double x[SP2_LANCZOS], cp[SP2_LANCZOS], rp[SP2_LANCZOS];
+    for (int i = 0; i < m; ++i) x[i] = 1.0;
+    for (int it = 0; it < 3; ++it) {
+        double den = a[0] - sigma;
+        cp[0] = m > 1 ? b[0] / den : 0.0;
+        rp[0] = x[0] / den;
+        for (int i = 1; i < m; ++i) {
+            den = a[i] - sigma - b[i - 1] * cp[i - 1];
+            cp[i] = i + 1 < m ? b[i] / den : 0.0;
+            rp[i] = (x[i] - b[i - 1] * rp[i - 1]) / den;
+        }
+        x[m - 1] = rp[m - 1];
+        for (int i = m - 2; i >= 0; --i) x[i] = rp[i] - cp[i] * x[i + 1];
+        double nrm = 0.0;
+        for (int i = 0; i < m; ++i) nrm += x[i] * x[i];
+        nrm = sqrt(nrm);
+        if (!(nrm > 0.0) || !isfinite(nrm)) return 1.0;
+        for (int i = 0; i < m; ++i) x[i] /= nrm;
+    }
+    return fabs(x[m - 1]);
+}
+
+__global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* __restrict__ jobs, const MolState* __restrict__ st) {
+    const Sp2Job jb = jobs[blockIdx.x];
+    if (!st[jb.mol].active) return;
+    const int n = jb.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = SP2_BOUND_THREADS / 32;
+    extern __shared__ double lz[];
+    double* q = lz;        // current Lanczos vector
+    double* qp = lz + n;   // previous one
+    double* w = lz + 2 * n;
+    __shared__ double red[NW];
+    __shared__ double alpha[SP2_LANCZOS], beta[SP2_LANCZOS];
+    // Gershgorin interval (rows of F*)
+    __shared__ double gred[2][NW];
+    double glo = 1e300, ghi = -1e300;
+    for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
+        glo = fmin(glo, jb.rowmin[i]);
+        ghi = fmax(ghi, jb.rowmax[i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+        ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+    }
+    if (lane == 0) {
+        gred[0][warp] = glo;
+        gred[1][warp] = ghi;
+    }
+    // fixed start vector, normalised
+    double nq = 0.0;
+    for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
+        const double x = cos(0.7 * i + 0.3) + 0.5;
+        q[i] = x;
+        qp[i] = 0.0;
+        nq += x * x;
+    }
+    nq = bounds_block_sum(nq, red);  // its barriers also publish gred
+    glo = gred[0][0];
+    ghi = gred[1][0];
+    for (int v = 1; v < NW; ++v) {
+        glo = fmin(glo, gred[0][v]);
+        ghi = fmax(ghi, gred[1][v]);
+    }
+    const double inq = 1.0 / sqrt(nq);
+    for (int i = tid; i < n; i += SP2_BOUND_THREADS) q[i] *= inq;
+    __syncthreads();
+    const int K = min(SP2_LANCZOS, n);
+    int m = 0;
+    double bprev = 0.0;
+    for (int j = 0; j < K; ++j) {
+        for (int r = warp; r < n; r += NW) {
+            const double* Fr = jb.F + (long long)r * n;
+            double acc = 0.0;
+            for (int c = lane; c < n; c += 32) acc = fma(Fr[c], q[c], acc);
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) w[r] = acc;
+        }
+        __syncthreads();
+        double part = 0.0;
+        for (int i = tid; i < n; i += SP2_BOUND_THREADS) part += q[i] * w[i];
+        const double a = bounds_block_sum(part, red);
+        part = 0.0;
+        for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
+            const double x = w[i] - a * q[i] - bprev * qp[i];
+            w[i] = x;
+            part += x * x;
+        }
+        const double bnorm = sqrt(bounds_block_sum(part, red));
+        if (tid == 0) {
+            alpha[j] = a;
+            beta[j] = bnorm;
+        }
+        m = j + 1;
+        if (!(bnorm > 1e-12 * fmax(fabs(a), 1.0))) break;  // invariant subspace: T is exact
+        const double ib = 1.0 / bnorm;
+        for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
+            qp[i] = q[i];
+            q[i] = w[i] * ib;
+        }
+        bprev = bnorm;
+        __syncthreads();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // Gershgorin interval of T contains its spectrum
+        double tlo = 1e300, thi = -1e300;
+        for (int i = 0; i < m; ++i) {
+            const double rad = (i > 0 ? fabs(beta[i - 1]) : 0.0) + (i + 1 < m ? fabs(beta[i]) : 0.0);
+            tlo = fmin(tlo, alpha[i] - rad);
+            thi = fmax(thi, alpha[i] + rad);
+        }
+        const double pad = 1e-12 * (fabs(tlo) + fabs(thi)) + 1e-300;
+        tlo -= pad;
+        thi += pad;
+        const double th_min = lz_eig(alpha, beta, m, 0, tlo, thi);
+        const double th_max = lz_eig(alpha, beta, m, m - 1, tlo, thi);
+        const double width = fmax(th_max - th_min, 1e-6);
+        const double eps = 1e-8 * (fabs(th_min) + fabs(th_max) + 1.0);
+        const double bm = beta[m - 1];
+        const double r_min = fabs(bm) * lz_last_component(alpha, beta, m, th_min - eps);
+        const double r_max = fabs(bm) * lz_last_component(alpha, beta, m, th_max + eps);
+        double lo = th_min - r_min - 0.005 * width;
+        double hi = th_max + r_max + 0.005 * width;
+        if (!isfinite(lo) || !isfinite(hi) || !(hi > lo)) {
+            lo = glo;
+            hi = ghi;
+        }
+        jb.bounds[0] = fmax(lo, glo);
+        jb.bounds[1] = fmin(hi, ghi);
+    }
+}
+
 // X0 = (e_max I - F*) / (e_max - e_min); per-block partial sums of tr X0 and ||X0||_F^2.
 __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, const MolState* __restrict__ st, int nblk) {
     const Sp2Job jb = jobs[blockIdx.y];
@@ -27,31 +212,8 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
     const int n = jb.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     __shared__ double red[2][32];
-    // spectral bounds (every block reduces the row bounds itself)
-    double lo = 1e300, hi = -1e300;
-    for (int i = tid; i < n; i += blockDim.x) {
-        lo = fmin(lo, jb.rowmin[i]);
-        hi = fmax(hi, jb.rowmax[i]);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    if (lane == 0) {
-        red[0][warp] = lo;
-        red[1][warp] = hi;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int w = 1; w < nw; ++w) {
-            red[0][0] = fmin(red[0][0], red[0][w]);
-            red[1][0] = fmax(red[1][0], red[1][w]);
-        }
-    }
-    __syncthreads();
-    const double emin = red[0][0], emax = red[1][0];
+    const double emin = jb.bounds[0], emax = jb.bounds[1];  // from k_sp2_bounds
     const double inv = 1.0 / fmax(emax - emin, 1e-300);
-    __syncthreads();
     double tr = 0.0, fr = 0.0;
     for (int r = blockIdx.x * nw + warp; r < n; r += nblk * nw) {
         const double* Fr = jb.F + (long long)r * n;
@@ -113,7 +275,7 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
 // One SP2 step over all upper-triangle 64x64 tiles of every active channel.
 __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
                                                             int ntiles, const Sp2State* __restrict__ sst) {
-    extern __shared__ double dsm[];
+    extern __shared__ __align__(16) double dsm[];
     __shared__ double red[2][4];
     const int t = blockIdx.x;
     if (t >= ntiles) return;
@@ -170,35 +332,6 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __rest
     }
 }
 
-// C = alpha A.B for every (molecule, channel) job of a tile list, on the FP64 tensor cores
-// (the commutator product F.P, src/scf.rs:531-544).
-__global__ void __launch_bounds__(DG_THREADS, 4) k_dgemm_nn(const GemmJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                            int ntiles, const MolState* __restrict__ st, int force,
-                                                            const int* __restrict__ mask) {
-    extern __shared__ double dsm[];
-    const int t = blockIdx.x;
-    if (t >= ntiles) return;
-    const GemmTile tl = tiles[t];
-    const GemmJob jb = jobs[tl.job];
-    if (!force && !st[jb.mol].active) return;
-    if (mask && !mask[jb.mol]) return;
-    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
-    const int warp = threadIdx.x >> 5;
-    const bool compute = m0 + (warp >> 1) * 32 < jb.M && n0 + (warp & 1) * 32 < jb.N;  // skip pure padding
-    double acc[2][4][4];
-    dg_mainloop(dsm, jb.A, jb.lda, jb.B, jb.ldb, jb.M, jb.N, jb.K, m0, n0, acc, compute);
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int r = m0 + dg_row(i, e);
-                const int c = n0 + dg_col(j, e);
-                if (r < jb.M && c < jb.N) jb.C[(long long)r * jb.ldc + c] = jb.alpha * acc[i][j][e];
-            }
-}
-
 // After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
 __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs, int max_steps,
                              int* __restrict__ active_count, double* __restrict__ work) {
@@ -210,6 +343,7 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
     // algorithmic work of the product just taken: a symmetric X.X, n^3 flops
     atomicAdd(&work[0], 1.0);
     atomicAdd(&work[1], (double)jb.n * jb.n * jb.n);
+    atomicAdd(&work[3], 16.0 * jb.n * jb.n);  // read X, write X^2 (both triangles), FP64
     double tr = 0.0, fr = 0.0;
     for (int t = 0; t < jb.ntiles; ++t) {
         tr += jb.part[2 * t];

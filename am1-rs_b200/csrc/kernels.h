@@ -69,6 +69,7 @@ struct Sp2Job {
     double* X1;
     double* P;              // output density (w X), n x n (may alias X0)
     double* part;           // partial sums [max(nblk, ntiles)][2]
+    double* bounds;         // [2] spectral interval of F* used for the mapping (k_sp2_bounds)
     double nocc, weight;
     int n, mol, tile0, ntiles;
 };
@@ -107,12 +108,13 @@ __global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles
 __global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
 __global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force, const int* mask);
 __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, const int* mask);
+// one CTA of 256 threads per job, 3 n doubles of dynamic shared memory
+__global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 __global__ void k_sp2_step(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
 // E = F.P - P.F over the upper-triangle tiles: history push of E and its CDIIS Gram row
 __global__ void k_commutator(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
-__global__ void k_dgemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work);

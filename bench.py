@@ -120,6 +120,13 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # CPU baseline / reference arm: the oracle (C++ restatement of am1-rs's SCF) on host cores
 # ---------------------------------------------------------------------------------------
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_sp2_step launch over the whole 512-molecule
+# batch (every molecule active), divided by that launch's algorithmic bytes 16 sum(n^2): 257.3 MB /
+# 297.0 MB (profiles/k_sp2_step__batch512_alkane_water.md).  Traffic grows with the molecules a launch
+# processes, so the per-launch traffic of this run is its algorithmic bytes times this ratio.
+SP2_DRAM_PER_ALG_BYTE = 0.866
+
+
 def oracle_rate(mols, order, budget_s, threads, chunk=None):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
@@ -304,6 +311,7 @@ def run_ours(args):
         pl = {k: sum(s["phase_launches"][k] for s in stats) / args.steps for k in stats[0]["phase_launches"]}
         step_dev_ms = sum(step_ms) / args.steps
         sp2_flops = sum(s["purification_flops"] for s in stats) / args.steps  # n^3 per product
+        sp2_bytes = sum(s["purification_bytes"] for s in stats) / args.steps  # 16 n^2 per product
         sp2_ms = ph["eigen:inner"]
         sp2_launch_ms = sp2_ms / max(pl["eigen:inner"], 1)
         achieved_tf = sp2_flops / (sp2_ms * 1e-3) / 1e12
@@ -345,7 +353,11 @@ def run_ours(args):
                     "h2d_bytes_per_step": e2e_stats["h2d_bytes"], "d2h_bytes_per_step": e2e_stats["d2h_bytes"]},
             "roofline": {"kernel": "k_sp2_step (density purification: symmetric FP64 X.X on mma.sync m16n8k8 f64)",
                          "bound": "tensor", "achieved": achieved_tf, "peak": peak_fp64, "unit": "TFLOP/s",
-                         "frac": achieved_tf / peak_fp64 if peak_fp64 else None, "traffic": None,
+                         "frac": achieved_tf / peak_fp64 if peak_fp64 else None,
+                         "traffic": SP2_DRAM_PER_ALG_BYTE * sp2_bytes / max(pl["eigen:inner"], 1),
+                         "traffic_note": "bytes per launch: this run's algorithmic bytes per launch (16 n^2 per "
+                                         "product) x the DRAM/algorithmic ratio of one ncu capture of a full-batch "
+                                         f"launch ({SP2_DRAM_PER_ALG_BYTE})",
                          "peak_source": "FP64 cuBLAS DGEMM (torch.matmul float64 8192^3) measured in this run; "
                                         "MEASURED_PEAKS.json has no FP64 figure",
                          "algorithmic": "n^3 flops per symmetric product X.X (half of 2n^3), summed over the "

@@ -211,6 +211,7 @@ typedef struct {
     int32_t eigen_fallbacks;     /* molecule-iterations whose purification stalled (eigensolver used) */
     double purification_steps;   /* purification steps summed over molecules, channels, iterations */
     double purification_flops;   /* their algorithmic work: n^3 per symmetric product X.X */
+    double purification_bytes;   /* their algorithmic HBM traffic: 16 n^2 per product (read X, write X^2) */
 } am1gpu_call_stats;
 
 /* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */
