@@ -53,26 +53,21 @@ __device__ __forceinline__ void dg_cp16(double* smem_dst, const double* gsrc, co
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(valid ? gsrc : base), "r"(bytes));
 }
 
-// True when both operands can be copied in 16-byte pairs: 16-byte aligned bases, even leading
-// dimensions (every row starts on a pair), and even K and N (a pair never straddles an edge).
-__device__ __forceinline__ bool dg_pairs_ok(const double* A, int lda, const double* B, int ldb, int N, int K) {
-    return ((reinterpret_cast<unsigned long long>(A) | reinterpret_cast<unsigned long long>(B)) & 15ull) == 0 &&
-           ((lda | ldb | N | K) & 1) == 0;
-}
 __device__ __forceinline__ void dg_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void dg_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Issue the copies of k-tile kt into pipeline stage `st` (16-byte pairs when `pairs`).
+// Issue the copies of k-tile kt into pipeline stage `st` (16-byte pairs when PAIRS).
+template <bool PAIRS>
 __device__ __forceinline__ void dg_load(double* smem, int st, const double* __restrict__ A, int lda, const double* __restrict__ B,
-                                        int ldb, int M, int N, int K, int m0, int n0, int kt, bool pairs) {
+                                        int ldb, int M, int N, int K, int m0, int n0, int kt) {
     double* As = smem + st * DG_STAGE;
     double* Bs = As + DG_TILE * DG_AS;
     const int k0 = kt * DG_BK;
     const int tid = threadIdx.x;
-    if (pairs) {
+    if constexpr (PAIRS) {
 #pragma unroll
         for (int l = 0; l < 4; ++l) {
             const int idx = tid + l * DG_THREADS;
@@ -83,26 +78,38 @@ __device__ __forceinline__ void dg_load(double* smem, int st, const double* __re
             const int gbk = k0 + bk, gj = n0 + bc;
             dg_cp16(&Bs[bk * DG_BS + bc], B + (long long)gbk * ldb + gj, B, gbk < K && gj < N);
         }
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        const int idx = tid + l * DG_THREADS;
-        const int ar = idx >> 4, ak = idx & 15;
-        const int gi = m0 + ar, gk = k0 + ak;
-        dg_cp8(&As[ar * DG_AS + ak], A + (long long)gi * lda + gk, A, gi < M && gk < K);
-        const int bk = idx >> 6, bc = idx & 63;
-        const int gbk = k0 + bk, gj = n0 + bc;
-        dg_cp8(&Bs[bk * DG_BS + bc], B + (long long)gbk * ldb + gj, B, gbk < K && gj < N);
+        for (int l = 0; l < 8; ++l) {
+            const int idx = tid + l * DG_THREADS;
+            const int ar = idx >> 4, ak = idx & 15;
+            const int gi = m0 + ar, gk = k0 + ak;
+            dg_cp8(&As[ar * DG_AS + ak], A + (long long)gi * lda + gk, A, gi < M && gk < K);
+            const int bk = idx >> 6, bc = idx & 63;
+            const int gbk = k0 + bk, gj = n0 + bc;
+            dg_cp8(&Bs[bk * DG_BS + bc], B + (long long)gbk * ldb + gj, B, gbk < K && gj < N);
+        }
     }
 }
 
+// Whether this warp's 32x32 quarter of the 64x64 tile needs computing: not when it is padding
+// or, in a tile on the diagonal of a symmetric result (only its upper triangle is needed), when it
+// lies below the diagonal.  (Skipping finer 16x8 blocks inside a quarter costs more in predicated
+// issue than it saves.)
+__device__ __forceinline__ bool dg_quarter_on(int m0, int n0, int M, int N, bool diag_tile) {
+    const int warp = threadIdx.x >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    return m0 + wr < M && n0 + wc < N && !(diag_tile && wr > wc);
+}
+
 // acc[i][j][e]: element (dg_row(i, e), dg_col(j, e)) of the 64x64 tile.  A warp with
-// compute == false still takes part in the copies and barriers but issues no MMAs (its 32x32
-// quarter of the tile is padding, or redundant by symmetry); the SM gives its issue slots to
-// other CTAs' warps.
+// compute == false still takes part in the copies and barriers but issues no MMAs; the SM gives
+// its issue slots to other CTAs' warps.  PAIRS: both operands can be copied in 16-byte pairs
+// (16-byte aligned bases, even leading dimensions, even K and N; the host sorts tiles by it).
+// The last k-tile skips its second half when K ends inside the first.
+template <bool PAIRS>
 __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restrict__ A, int lda, const double* __restrict__ B, int ldb,
-                                            int M, int N, int K, int m0, int n0, double acc[2][4][4], bool compute = true) {
+                                            int M, int N, int K, int m0, int n0, double acc[2][4][4], bool compute) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
     const int g = lane >> 2, tq = lane & 3;
@@ -113,23 +120,23 @@ __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restri
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     const int KT = (K + DG_BK - 1) / DG_BK;
-    const bool pairs = dg_pairs_ok(A, lda, B, ldb, N, K);
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {
-        if (s < KT) dg_load(smem, s, A, lda, B, ldb, M, N, K, m0, n0, s, pairs);
+        if (s < KT) dg_load<PAIRS>(smem, s, A, lda, B, ldb, M, N, K, m0, n0, s);
         dg_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
         dg_wait<DG_STAGES - 2>();
         __syncthreads();
         const int nk = kt + DG_STAGES - 1;
-        if (nk < KT) dg_load(smem, nk % DG_STAGES, A, lda, B, ldb, M, N, K, m0, n0, nk, pairs);
+        if (nk < KT) dg_load<PAIRS>(smem, nk % DG_STAGES, A, lda, B, ldb, M, N, K, m0, n0, nk);
         dg_commit();
         const double* As = smem + (kt % DG_STAGES) * DG_STAGE;
         const double* Bs = As + DG_TILE * DG_AS;
         if (!compute) continue;
 #pragma unroll
         for (int kk = 0; kk < DG_BK; kk += 8) {
+            if (kk > 0 && kt * DG_BK + kk >= K) break;
             double a[2][4], b[4][2];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
@@ -159,6 +166,7 @@ __device__ __forceinline__ void dg_mainloop(double* smem, const double* __restri
 // the k-tiles of the second product follow those of the first, and the accumulator is negated
 // between the two (so the pipeline never drains in the middle).  All four operands share M = N = K
 // and the leading dimension ld.  Same fragment layout and `compute` rule as dg_mainloop.
+template <bool PAIRS>
 __device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __restrict__ A1, const double* __restrict__ B1,
                                                  const double* __restrict__ A2, const double* __restrict__ B2, int ld,
                                                  int n, int m0, int n0, double acc[2][4][4], bool compute) {
@@ -172,12 +180,11 @@ __device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __r
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     const int KT = (n + DG_BK - 1) / DG_BK;  // k-tiles per product
-    const bool pairs = dg_pairs_ok(A1, ld, B1, ld, n, n) && dg_pairs_ok(A2, ld, B2, ld, n, n);
     auto load = [&](int st, int kt) {
         if (kt < KT)
-            dg_load(smem, st, A1, ld, B1, ld, n, n, n, m0, n0, kt, pairs);
+            dg_load<PAIRS>(smem, st, A1, ld, B1, ld, n, n, n, m0, n0, kt);
         else
-            dg_load(smem, st, A2, ld, B2, ld, n, n, n, m0, n0, kt - KT, pairs);
+            dg_load<PAIRS>(smem, st, A2, ld, B2, ld, n, n, n, m0, n0, kt - KT);
     };
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {
@@ -201,8 +208,10 @@ __device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __r
 #pragma unroll
                     for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
         }
+        const int kbase = (kt < KT ? kt : kt - KT) * DG_BK;
 #pragma unroll
         for (int kk = 0; kk < DG_BK; kk += 8) {
+            if (kk > 0 && kbase + kk >= n) break;
             double a[2][4], b[4][2];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {

@@ -52,6 +52,8 @@ inline const DevElem& helem(int method, int z) { return host_param_table()[metho
 
 // ---------------------------------------------------------------------------------------
 // Device context: parameter table uploaded once per device
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 // ---------------------------------------------------------------------------------------
 struct DeviceCtx {
     std::once_flag once;
@@ -112,12 +114,10 @@ int device_ctx(DeviceCtx** out) {
             return bad("tridiag smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("tridiag cluster attribute", err);
-        if ((err = cudaFuncSetAttribute(k_sp2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
-            cudaSuccess)
-            return bad("sp2 smem attribute", err);
-        if ((err = cudaFuncSetAttribute(k_commutator, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) !=
-            cudaSuccess)
-            return bad("commutator smem attribute", err);
+        for (const void* f : {(const void*)k_sp2_step16, (const void*)k_sp2_step8, (const void*)k_commutator16,
+                              (const void*)k_commutator8})
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
+                return bad("tile kernel smem attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
@@ -379,8 +379,8 @@ struct Batch {
     std::vector<Bucket> buckets;      // eigensolver jobs by cluster size
     std::vector<Bucket> tri_buckets;  // tridiagonalisation jobs by cluster size
     Sp2Job* d_sp2;
-    GemmTile* d_sp2_tiles;
-    int nt_sp2 = 0, sp2_nblk = 1;
+    GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
+    int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
     Sp2State* d_sp2_state;
     TriJob* d_tri;
     int* d_need_eigen;
@@ -548,7 +548,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     Sp2Job* hsp2 = (Sp2Job*)(Hs + o_sp2);
     GemmTile* hsp2t = (GemmTile*)(Hs + o_sp2t);
     TriJob* htri = (TriJob*)(Hs + o_tri);
-    int nsp2t = 0;
+    std::vector<GemmTile> tiles_pairs, tiles_other;  // jobs with even n and 16-byte aligned slots / the rest
     MolState* hst = (MolState*)(Hs + o_st);
     long long a_off = 0, w_off = 0, ar_off = 0, hi_off = 0, mi_off = 0;
     int atom_base = 0, job = 0, ntile = 0, cid_off = 0;
@@ -655,10 +655,14 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.weight = md.occ_weight;
             sj.n = (int)n;
             sj.mol = mi;
-            sj.tile0 = nsp2t;
+            // the purification and commutator kernels copy 16-byte pairs when every row of X0, X1,
+            // F and P starts on 16 bytes: even n (slot bases are then 16-byte aligned too)
+            const bool pairs = n % 2 == 0 && aligned16(sj.X0) && aligned16(sj.X1) && aligned16(cj.F) && aligned16(cj.P);
+            std::vector<GemmTile>& tl = pairs ? tiles_pairs : tiles_other;
+            sj.tile0 = (int)tl.size();  // tile index inside its own launch
             for (int x = 0; x < (int)tn_; ++x)
-                for (int y = x; y < (int)tn_; ++y) hsp2t[nsp2t++] = GemmTile{job, x, y};
-            sj.ntiles = nsp2t - sj.tile0;
+                for (int y = x; y < (int)tn_; ++y) tl.push_back(GemmTile{job, x, y});
+            sj.ntiles = (int)tl.size() - sj.tile0;
             hsp2[job] = sj;
             TriJob tj{};
             tj.A = cj.Fx;
@@ -705,7 +709,10 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     }
     hpp[b.nmol] = a_off;
     b.nt_gt = b.nt_dn = ntile;
-    b.nt_sp2 = nsp2t;
+    for (size_t i = 0; i < tiles_pairs.size(); ++i) hsp2t[i] = tiles_pairs[i];
+    for (size_t i = 0; i < tiles_other.size(); ++i) hsp2t[tiles_pairs.size() + i] = tiles_other[i];
+    b.nt_sp2_pairs = (int)tiles_pairs.size();
+    b.nt_sp2 = (int)(tiles_pairs.size() + tiles_other.size());
     // eigen jobs grouped by cluster size, largest first inside a group
     std::vector<int> idx(eig_all.size());
     for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
@@ -749,6 +756,13 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
 }
 
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+// The upper-triangle tile kernels run as up to two launches: the 16-byte-copy tiles, then the rest.
+template <class F>
+void launch_tiles(const Batch& b, cudaStream_t, F&& launch) {
+    if (b.nt_sp2_pairs > 0) launch(b.d_sp2_tiles, b.nt_sp2_pairs, true);
+    if (b.nt_sp2 > b.nt_sp2_pairs) launch(b.d_sp2_tiles + b.nt_sp2_pairs, b.nt_sp2 - b.nt_sp2_pairs, false);
+}
 
 int launch_core(Batch& b, Mem* ws, const DevElem* dp, Run* run) {
     cudaStream_t s = ws->stream;
@@ -849,7 +863,10 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                                                       b.d_st, 0);
             run.launched(AM1GPU_PHASE_FOCK);
             if ((rc = run.end(AM1GPU_PHASE_FOCK, ph)) || (rc = run.begin(&ph))) return rc;
-            k_commutator<<<b.nt_sp2, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, b.d_sp2_tiles, b.nt_sp2, b.d_st);
+            launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+                if (pairs) k_commutator16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+                else k_commutator8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+            });
             k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
             run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
             if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, ph)) || (rc = run.begin(&ph))) return rc;
@@ -867,7 +884,10 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
-                    k_sp2_step<<<b.nt_sp2, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, b.d_sp2_tiles, b.nt_sp2, b.d_sp2_state);
+                    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+                        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                    });
                     run.launched(AM1GPU_PHASE_DENSITY_CORE);
                     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
                     CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));

@@ -147,8 +147,9 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
 // upper-triangle tiles are computed.  The epilogue takes the strict upper triangle: it stores e in
 // the packed history slot of this iteration and forms this tile's share of |e|_F^2 and of
 // <e, e_slot> for every live slot (the new CDIIS Gram row).
-__global__ void __launch_bounds__(DG_THREADS, 4) k_commutator(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                              int ntiles, const MolState* __restrict__ st) {
+template <bool PAIRS>
+__device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
+                                                const MolState* __restrict__ st) {
     extern __shared__ __align__(16) double dsm[];
     __shared__ double red[CP_N][4];
     const int t = blockIdx.x;
@@ -164,11 +165,10 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_commutator(const ChanJob* __r
     const long long la = packed_anti_len(n);
     const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // this warp's 32x32 quarter: skip it when it is padding or lies below the diagonal
-    const int qr = (warp >> 1) * 32, qc = (warp & 1) * 32;
-    const bool compute = m0 + qr < n && n0 + qc < n && !(tl.tm == tl.tn && qr > qc);
+    // e is antisymmetric: a warp whose quarter is padding or lies below the diagonal issues no MMAs
+    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
     double acc[2][4][4];
-    dg_mainloop_diff(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
+    dg_mainloop_diff<PAIRS>(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
     double v[CP_N];
 #pragma unroll
     for (int k = 0; k < CP_N; ++k) v[k] = 0.0;
@@ -207,6 +207,15 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_commutator(const ChanJob* __r
         const int local = tl.tm * T - tl.tm * (tl.tm - 1) / 2 + (tl.tn - tl.tm);
         jb.cpart[(long long)local * CP_N + tid] = red[tid][0] + red[tid][1] + red[tid][2] + red[tid][3];
     }
+}
+
+__global__ void __launch_bounds__(DG_THREADS, 4) k_commutator16(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                                int ntiles, const MolState* __restrict__ st) {
+    commutator_body<true>(jobs, tiles, ntiles, st);
+}
+__global__ void __launch_bounds__(DG_THREADS, 4) k_commutator8(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                               int ntiles, const MolState* __restrict__ st) {
+    commutator_body<false>(jobs, tiles, ntiles, st);
 }
 
 // Gaussian elimination with partial pivoting; false when a pivot is below 1e-12.

@@ -273,31 +273,31 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
 }
 
 // One SP2 step over all upper-triangle 64x64 tiles of every active channel.
-__global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                            int ntiles, const Sp2State* __restrict__ sst) {
+template <bool PAIRS>
+__device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
+                                              const Sp2State* __restrict__ sst) {
     extern __shared__ __align__(16) double dsm[];
     __shared__ double red[2][4];
     const int t = blockIdx.x;
     if (t >= ntiles) return;
     const GemmTile tl = tiles[t];
-    const Sp2State s = sst[tl.job];
-    if (!s.active) return;
-    const Sp2Job jb = jobs[tl.job];
-    const int n = jb.n;
-    const double* X = s.cur ? jb.X1 : jb.X0;
-    double* Y = s.cur ? jb.X0 : jb.X1;
+    const Sp2State* sp = sst + tl.job;
+    if (!sp->active) return;
+    const Sp2Job* jp = jobs + tl.job;
+    const int n = jp->n;
+    const int cur = sp->cur;
+    const double* X = cur ? jp->X1 : jp->X0;
     const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool diag_tile = tl.tm == tl.tn;
-    // this warp's 32x32 quarter: skip it when it is padding, or the lower-left quarter of a
-    // diagonal tile (the upper-right quarter computes and mirrors it)
-    const int qr = (warp >> 1) * 32, qc = (warp & 1) * 32;
-    const bool lower_quarter = diag_tile && qr > qc;
-    const bool compute = m0 + qr < n && n0 + qc < n && !lower_quarter;
+    // only the upper triangle of X^2 is computed: a warp whose quarter is padding or lies below
+    // the diagonal of a diagonal tile issues no MMAs
+    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
     double acc[2][4][4];
-    dg_mainloop(dsm, X, n, X, n, n, n, n, m0, n0, acc, compute);  // X symmetric: X[rows m0..] . X[:, n0..]
-    // epilogue: Y = X^2 or 2X - X^2, mirrored; partial trace / Frobenius sums
-    const bool mirror = !diag_tile || qr < qc;  // off-diagonal content: write the transpose too
+    dg_mainloop<PAIRS>(dsm, X, n, X, n, n, n, n, m0, n0, acc, compute);  // X symmetric: X[rows m0..] . X[:, n0..]
+    // epilogue: Y = X^2 or 2X - X^2 for r <= c, mirrored; partial trace / Frobenius sums (the job
+    // fields it needs are read only now, so they hold no registers during the k-loop)
+    double* Y = cur ? jp->X0 : jp->X1;
+    const int square = sp->square;
     double tr = 0.0, fr = 0.0;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -307,13 +307,17 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __rest
             for (int e = 0; e < 4; ++e) {
                 const int r = m0 + dg_row(i, e);
                 const int c = n0 + dg_col(j, e);
-                if (compute && r < n && c < n) {
+                if (compute && r <= c && c < n) {
                     const double x2 = acc[i][j][e];
-                    const double y = s.square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
+                    const double y = square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
                     Y[(long long)r * n + c] = y;
-                    if (mirror) Y[(long long)c * n + r] = y;
-                    fr += (mirror ? 2.0 : 1.0) * y * y;
-                    if (r == c) tr += y;
+                    if (r < c) {
+                        Y[(long long)c * n + r] = y;
+                        fr += 2.0 * y * y;
+                    } else {
+                        fr += y * y;
+                        tr += y;
+                    }
                 }
             }
     for (int o = 16; o > 0; o >>= 1) {
@@ -326,7 +330,7 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step(const Sp2Job* __rest
     }
     __syncthreads();
     if (tid == 0) {
-        double* p = jb.part + 2 * (t - jb.tile0);
+        double* p = jp->part + 2 * (t - jp->tile0);
         p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
         p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
     }
@@ -393,5 +397,14 @@ __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __
 }
 
 size_t dgemm_smem_bytes() { return DG_SMEM; }
+
+__global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step16(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                              int ntiles, const Sp2State* __restrict__ sst) {
+    sp2_step_body<true>(jobs, tiles, ntiles, sst);
+}
+__global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step8(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                             int ntiles, const Sp2State* __restrict__ sst) {
+    sp2_step_body<false>(jobs, tiles, ntiles, sst);
+}
 
 }  // namespace am1

@@ -112,9 +112,13 @@ __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, co
 __global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
-__global__ void k_sp2_step(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+// *16: every matrix of the tile list has even n and 16-byte aligned rows (16-byte copies);
+// *8: any matrix (8-byte copies)
+__global__ void k_sp2_step16(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+__global__ void k_sp2_step8(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
 // E = F.P - P.F over the upper-triangle tiles: history push of E and its CDIIS Gram row
-__global__ void k_commutator(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
+__global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
+__global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work);
