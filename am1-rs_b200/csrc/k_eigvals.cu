@@ -17,30 +17,32 @@ namespace cg = cooperative_groups;
 // Householder reduction of one symmetric matrix held on chip.  The n x n matrix is distributed by
 // rows over a thread-block cluster of C CTAs (row r lives in CTA r % C, at local row r / C, full
 // length n), so the whole reduction runs out of shared memory; C is the smallest cluster whose
-// share fits one CTA.  Step k (GVL Alg. 8.3.1: the reflector I - beta v v^T zeroes row/column k
-// below the subdiagonal):
-//   sync #1   the owner of row k has v_k, beta_k ready; every other CTA copies them (distributed
-//             shared memory)
-//   p_r = beta A[r, k+1:] . v for the CTA's rows r > k, sent to every CTA with the warp's share of p.v
-//   sync #2   A[r, k+1:] -= v_r w + w_r v with w = p - (beta/2)(p.v) v, formed on the fly
-// Look-ahead: the warp that updates row k+1 (warp 0 of its owner) derives v_{k+1}, beta_{k+1}, d, e
-// from it at once, into the other half of the double-buffered v, so a step costs two cluster
-// barriers and one CTA barrier.  All control flow is uniform over the cluster (alpha = 0 gives
-// beta = 0 and a no-op update), so every CTA takes the same barriers.
+// share fits one CTA.  Reflector s (GVL Alg. 8.3.1) zeroes row/column s below the subdiagonal:
+// v_s = x + sign(x0)|x| e1 from x = A[s, s+1:], beta_s = 1/(|x|(|x| + |x0|)), and the trailing
+// block takes the rank-2 update A -= v w^T + w v^T with p = beta A v, w = p - (beta/2)(p.v) v.
+// Iteration s of the loop:
+//   (a) one warp of the owner of row s applies update s-1 to row s and derives reflector s
+//   cluster barrier: v_s ready; the other CTAs copy it (distributed shared memory)
+//   (b) one fused pass over the CTA's rows > s, a thread per column > s: apply update s-1 and
+//       accumulate this CTA's share of A v_s (A symmetric: column r of the share is a dot product
+//       down the rows, so consecutive threads read consecutive words)
+//   cluster barrier: every CTA's share ready; each CTA sums the C shares itself -> p, w_s
+// Column s below the diagonal is never updated: row s holds the same numbers and is the one read.
+// All control flow is uniform over the cluster, so every CTA takes the same barriers.
 constexpr int TRI_THREADS = 512;
 constexpr int TRI_WARPS = TRI_THREADS / 32;
 
-// Dynamic shared memory of one CTA: local rows, v (two buffers), p, the per-warp shares of p.v
-// from every CTA, beta (two buffers).
+// Dynamic shared memory of one CTA: local rows, v and w (two buffers each), the share of A v,
+// beta (two buffers) and two reduction scratches.
 size_t tridiag_smem_bytes(int n, int C) {
     const size_t rows = (size_t)(n + C - 1) / C;
-    return sizeof(double) * (rows * n + 3 * (size_t)n + (size_t)C * TRI_WARPS + 2);
+    return sizeof(double) * (rows * n + 5 * (size_t)n + 2 + TRI_WARPS + TRI_THREADS);
 }
 
-// Householder vector of row `row` (the trailing part from column c0 = k + 1), computed by one
-// warp: v = x + sign(x0) |x| e1 into vbuf, beta into *beta, and d[k], e[k].
-__device__ __forceinline__ void tri_reflector(const double* row, int k, int n, double* vbuf, double* beta, double* d, double* e) {
-    const int lane = threadIdx.x & 31, c0 = k + 1;
+// Householder vector of row `row` (the trailing part from column s + 1), computed by one warp:
+// v into vbuf, beta into *beta, and d[s], e[s].
+__device__ __forceinline__ void tri_reflector(const double* row, int s, int n, double* vbuf, double* beta, double* d, double* e) {
+    const int lane = threadIdx.x & 31, c0 = s + 1;
     double nrm = 0.0;
     for (int c = c0 + lane; c < n; c += 32) {
         const double x = row[c];
@@ -53,8 +55,8 @@ __device__ __forceinline__ void tri_reflector(const double* row, int k, int n, d
     const double sg = x0 >= 0.0 ? 1.0 : -1.0;
     __syncwarp();
     if (lane == 0) {
-        d[k] = row[k];
-        e[k] = alpha == 0.0 ? 0.0 : -sg * alpha;
+        d[s] = row[s];
+        e[s] = alpha == 0.0 ? 0.0 : -sg * alpha;
         *beta = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x0)));
         if (alpha != 0.0) vbuf[c0] = x0 + sg * alpha;
     }
@@ -69,11 +71,13 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
     const int n = jb.n;
     const int R = (n + C - 1) / C;
     extern __shared__ double sh[];
-    double* A = sh;                     // R x n: global row lr * C + crank at local row lr
-    double* vb = A + (size_t)R * n;     // v, two buffers of n (global column index)
-    double* p = vb + 2 * (size_t)n;     // p (global index)
-    double* part = p + n;               // [C * TRI_WARPS] shares of p.v
-    double* bb = part + C * TRI_WARPS;  // beta, two buffers
+    double* A = sh;                    // R x n: global row lr * C + crank at local row lr
+    double* vb = A + (size_t)R * n;    // v, two buffers of n (global column index)
+    double* wb = vb + 2 * (size_t)n;   // w, two buffers of n
+    double* pp = wb + 2 * (size_t)n;   // this CTA's share of A v
+    double* bb = pp + n;               // beta, two buffers
+    double* red = bb + 2;              // [TRI_WARPS]
+    double* red2 = red + TRI_WARPS;    // [TRI_THREADS] partial column sums of the row groups
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     auto csync = [&]() {
         if (C > 1) cluster.sync();
@@ -84,60 +88,111 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
         if (r >= n) break;
         for (int c = lane; c < n; c += 32) A[(size_t)lr * n + c] = jb.A[(size_t)r * n + c];
     }
+    for (int c = tid; c < n; c += TRI_THREADS) {  // update "-1" is the identity
+        vb[n + c] = 0.0;
+        wb[n + c] = 0.0;
+    }
     __syncthreads();
-    if (n >= 3 && crank == 0 && warp == 0) tri_reflector(A, 0, n, vb, bb, jb.d, jb.e);
-    for (int k = 0; k + 2 < n; ++k) {
-        const int par = k & 1, owner = k % C, c0 = k + 1;
-        double* v = vb + (size_t)par * n;
-        csync();  // #1: v_k and beta_k are ready in the owner
-        if (crank != owner) {
-            const double* rv = cluster.map_shared_rank(v, owner);
-            for (int c = c0 + tid; c < n; c += TRI_THREADS) v[c] = rv[c];
-            if (tid == 0) bb[par] = *cluster.map_shared_rank(bb + par, owner);
+    for (int s = 0; s + 1 < n; ++s) {
+        const int cur = (s + 1) & 1, nxt = s & 1;
+        const double* v = vb + (size_t)cur * n;  // reflector s - 1
+        const double* w = wb + (size_t)cur * n;
+        double* vn = vb + (size_t)nxt * n;       // reflector s
+        const bool has_next = s + 2 < n;
+        const int owner = s % C;
+        if (crank == owner && warp == 0) {  // (a)
+            double* row = A + (size_t)(s / C) * n;
+            const double vs = v[s], ws = w[s];
+            for (int c = s + lane; c < n; c += 32) row[c] -= vs * w[c] + ws * v[c];
+            __syncwarp();
+            if (has_next) tri_reflector(row, s, n, vn, bb + nxt, jb.d, jb.e);
+        }
+        csync();  // v_s ready in the owner
+        if (has_next && crank != owner) {
+            const double* rv = cluster.map_shared_rank(vn, owner);
+            for (int c = s + 1 + tid; c < n; c += TRI_THREADS) vn[c] = rv[c];
+            if (tid == 0) bb[nxt] = *cluster.map_shared_rank(bb + nxt, owner);
             __syncthreads();
         }
-        const double beta = bb[par];
-        const int lr0 = (c0 - crank + C - 1) / C;  // first local row with global index >= c0
-        double wpart = 0.0;
-        for (int lr = lr0 + warp; lr < R; lr += TRI_WARPS) {
-            const int r = lr * C + crank;
-            if (r >= n) break;
-            const double* row = A + (size_t)lr * n;
-            double acc = 0.0;
-            for (int c = c0 + lane; c < n; c += 32) acc = fma(row[c], v[c], acc);
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            const double pr = beta * acc;
-            if (lane < C) *cluster.map_shared_rank(&p[r], lane) = pr;  // to every CTA, itself included
-            wpart += pr * v[r];
-        }
-        if (lane < C) *cluster.map_shared_rank(&part[crank * TRI_WARPS + warp], lane) = wpart;
-        csync();  // #2: p and every share of p.v are complete everywhere
-        double pv = 0.0;
-        for (int q = lane; q < C * TRI_WARPS; q += 32) pv += part[q];
-        for (int o = 16; o > 0; o >>= 1) pv += __shfl_xor_sync(0xffffffffu, pv, o);
-        const double kk = 0.5 * beta * pv;
-        for (int lr = lr0 + warp; lr < R; lr += TRI_WARPS) {
-            const int r = lr * C + crank;
-            if (r >= n) break;
-            double* row = A + (size_t)lr * n;
-            const double vr = v[r], wr = p[r] - kk * vr;
-            for (int c = c0 + lane; c < n; c += 32) row[c] -= vr * (p[c] - kk * v[c]) + wr * v[c];
-            // look-ahead: row k+1 is final now; its reflector is the next step's
-            if (r == c0 && c0 + 2 < n) {
-                __syncwarp();
-                tri_reflector(row, c0, n, vb + (size_t)(par ^ 1) * n, bb + (par ^ 1), jb.d, jb.e);
+        // (b) columns r > s, rows c > s of this CTA: threads in G groups of cpg; thread (g, j) owns
+        // column s + 1 + j and rows lr0 + g, lr0 + g + G, ... (more groups when there are few columns)
+        const int lr0 = (s + 1 - crank + C - 1) / C;  // first local row with global index > s
+        const int lre = (n - crank + C - 1) / C;      // local rows with global index < n
+        const int ncol = n - (s + 1);
+        const int G = max(1, min(16, TRI_THREADS / (((ncol + 31) / 32) * 32)));
+        const int cpg = TRI_THREADS / G;
+        const int g = tid / cpg, j = tid - g * cpg;
+        double acc = 0.0;
+        if (g < G && j < ncol) {
+            const int r = s + 1 + j;
+            const double vr = v[r], wr = w[r];
+            int lr = lr0 + g;
+            for (; lr + 3 * G < lre; lr += 4 * G) {  // four independent rows per trip
+                double* a0 = A + (size_t)lr * n + r;
+                double* a1 = a0 + (size_t)G * n;
+                double* a2 = a1 + (size_t)G * n;
+                double* a3 = a2 + (size_t)G * n;
+                const int c0 = lr * C + crank, c1 = c0 + G * C, c2 = c1 + G * C, c3 = c2 + G * C;
+                const double x0 = *a0, x1 = *a1, x2 = *a2, x3 = *a3;
+                const double y0 = x0 - v[c0] * wr - w[c0] * vr, y1 = x1 - v[c1] * wr - w[c1] * vr;
+                const double y2 = x2 - v[c2] * wr - w[c2] * vr, y3 = x3 - v[c3] * wr - w[c3] * vr;
+                *a0 = y0;
+                *a1 = y1;
+                *a2 = y2;
+                *a3 = y3;
+                acc = fma(y0, vn[c0], acc);
+                acc = fma(y1, vn[c1], acc);
+                acc = fma(y2, vn[c2], acc);
+                acc = fma(y3, vn[c3], acc);
+            }
+            for (; lr < lre; lr += G) {
+                const int c = lr * C + crank;
+                double* ap = A + (size_t)lr * n + r;
+                const double y = *ap - v[c] * wr - w[c] * vr;
+                *ap = y;
+                acc = fma(y, vn[c], acc);
             }
         }
+        if (G == 1) {
+            if (j < ncol) pp[s + 1 + j] = acc;
+        } else {  // uniform over the CTA
+            red2[tid] = acc;
+            __syncthreads();
+            if (g == 0 && j < ncol) {
+                double t = 0.0;
+                for (int q = 0; q < G; ++q) t += red2[q * cpg + j];
+                pp[s + 1 + j] = t;
+            }
+        }
+        if (!has_next) break;
+        csync();  // every CTA's share of A v_s ready
+        const double beta = bb[nxt];
+        double part = 0.0;
+        for (int r = s + 1 + tid; r < n; r += TRI_THREADS) {
+            double sum = 0.0;
+            for (int q = 0; q < C; ++q) sum += *cluster.map_shared_rank(pp + r, q);
+            const double p = beta * sum;
+            wb[(size_t)nxt * n + r] = p;  // p for now, w below
+            part += p * vn[r];
+        }
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        double pv = 0.0;
+        for (int q = 0; q < TRI_WARPS; ++q) pv += red[q];
+        const double kk = 0.5 * beta * pv;
+        for (int r = s + 1 + tid; r < n; r += TRI_THREADS) wb[(size_t)nxt * n + r] -= kk * vn[r];
+        __syncthreads();
     }
     __syncthreads();
     // the last 2 x 2 block (or the 1 x 1 matrix)
     if (tid == 0) {
         if (n >= 2) {
-            if ((n - 2) % C == crank) jb.d[n - 2] = A[(size_t)((n - 2) / C) * n + n - 2];
-            if ((n - 1) % C == crank) {
-                jb.e[n - 2] = A[(size_t)((n - 1) / C) * n + n - 2];
-                jb.d[n - 1] = A[(size_t)((n - 1) / C) * n + n - 1];
+            if ((n - 2) % C == crank) {
+                jb.d[n - 2] = A[(size_t)((n - 2) / C) * n + n - 2];
+                jb.e[n - 2] = A[(size_t)((n - 2) / C) * n + n - 1];
             }
+            if ((n - 1) % C == crank) jb.d[n - 1] = A[(size_t)((n - 1) / C) * n + n - 1];
         } else if (crank == 0) {
             jb.d[0] = A[0];
         }
