@@ -398,6 +398,9 @@ struct Batch {
     double* h_work;
     double* h_res;
     double* h_charges;
+    double* d_eps;  // every channel's orbital energies, contiguous (job order)
+    double* h_eps;  // their pinned host copy
+    long long eps_total = 0;
     long long arena_doubles = 0;
 };
 
@@ -478,12 +481,15 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         const long long tn = (p.nao + 63) / 64;
         const long long sp2part = 2 * std::max<long long>(sp2_nblk, tn * (tn + 1) / 2);
         const long long cpart = CP_N * tn * (tn + 1) / 2;
-        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 2 + 128);
+        misc += p.nch * (4LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 2 + 128);
     }
     const size_t o_misc = take(dv, sizeof(double) * misc);
     const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
     const size_t o_res = take(dv, sizeof(double) * RES_N * b.nmol);
     const size_t o_chg = take(dv, sizeof(double) * std::max<long long>(natoms, 1));
+    long long eps_total = 0;
+    for (auto& p : b.plans) eps_total += (long long)p.nch * p.nao;
+    const size_t o_eps = take(dv, sizeof(double) * std::max<long long>(eps_total, 1));
     const size_t dtotal = align256(dv);
     // pinned staging also receives the outputs
     size_t hs = staged;
@@ -491,6 +497,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t h_o_work = take(hs, sizeof(double) * 4);
     const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
+    const size_t h_o_eps = take(hs, sizeof(double) * std::max<long long>(eps_total, 1));
     int rc = mem_ensure(mem, dtotal, align256(hs));
     if (rc) return rc;
     Mem* ws = &mem;
@@ -528,10 +535,13 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     int* d_colid = (int*)dptr(o_colid);
     b.d_res = (double*)dptr(o_res);
     b.d_charges = (double*)dptr(o_chg);
+    b.d_eps = (double*)dptr(o_eps);
+    b.eps_total = eps_total;
     b.h_active = (int*)(Hs + h_o_active);
     b.h_work = (double*)(Hs + h_o_work);
     b.h_res = (double*)(Hs + h_o_res);
     b.h_charges = (double*)(Hs + h_o_chg);
+    b.h_eps = (double*)(Hs + h_o_eps);
     // ---- fill the staged region
     MolDesc* hm = (MolDesc*)(Hs + o_mols);
     int* hz = (int*)(Hs + o_z);
@@ -550,7 +560,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     TriJob* htri = (TriJob*)(Hs + o_tri);
     std::vector<GemmTile> tiles_pairs, tiles_other;  // jobs with even n and 16-byte aligned slots / the rest
     MolState* hst = (MolState*)(Hs + o_st);
-    long long a_off = 0, w_off = 0, ar_off = 0, hi_off = 0, mi_off = 0;
+    long long a_off = 0, w_off = 0, ar_off = 0, hi_off = 0, mi_off = 0, eps_off = 0;
     int atom_base = 0, job = 0, ntile = 0, cid_off = 0;
     std::vector<EigJob> eig_all;
     std::vector<int> eig_cluster;
@@ -620,8 +630,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             mi_off += n;
             cj.rowmax = d_misc + mi_off;
             mi_off += n;
-            cj.eps = d_misc + mi_off;
-            mi_off += n;
+            cj.eps = b.d_eps + eps_off;
+            eps_off += n;
             double* tri_d = d_misc + mi_off;
             mi_off += n;
             double* tri_e = d_misc + mi_off;
@@ -967,8 +977,10 @@ int fetch_results(Batch& b, Mem& mem, am1gpu_call_stats* stats) {
     cudaStream_t s = mem.stream;
     CK(cudaMemcpyAsync(b.h_res, b.d_res, sizeof(double) * RES_N * b.nmol, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(b.h_charges, b.d_charges, sizeof(double) * std::max(b.natoms, 1), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(b.h_eps, b.d_eps, sizeof(double) * std::max(b.eps_total, 1LL), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    stats->d2h_bytes += (int64_t)(sizeof(double) * RES_N * b.nmol + sizeof(double) * std::max(b.natoms, 1));
+    stats->d2h_bytes += (int64_t)(sizeof(double) * RES_N * b.nmol + sizeof(double) * std::max(b.natoms, 1) +
+                                  sizeof(double) * std::max(b.eps_total, 1LL));
     return AM1GPU_OK;
 }
 
@@ -1032,11 +1044,7 @@ int write_result(Batch& b, Mem* ws, int mi, am1gpu_result* r, am1gpu_call_stats*
         double* e_out = c == 0 ? r->mo_energies : r->beta_energies;
         double* c_out = c == 0 ? r->mo_coeff : r->beta_coeff;
         const ChanJob& jc = b.jobs[b.job0[mi] + c];
-        if (e_out) {
-            CK(cudaMemcpyAsync(e_out, jc.eps, sizeof(double) * n, cudaMemcpyDeviceToHost, ws->stream));
-            CK(cudaStreamSynchronize(ws->stream));
-            stats->d2h_bytes += (int64_t)sizeof(double) * n;
-        }
+        if (e_out) std::memcpy(e_out, b.h_eps + (jc.eps - b.d_eps), sizeof(double) * n);  // fetched in bulk
         if (c_out) {
             if (density_mode() == 0) {
                 // the purification path has no eigenvectors: diagonalise the last F* now
