@@ -953,7 +953,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
     // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
     if ((rc = launch_tridiag(b, ws))) return rc;
-    k_bisect<<<njobs, 128, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);
+    k_bisect<<<njobs, 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue (n <= 448)
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
     run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size());

@@ -200,15 +200,36 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
     csync();  // no CTA leaves while another may still address its shared memory
 }
 
-// number of eigenvalues of T below x
+// Number of eigenvalues of T below x: the sign changes of the leading principal minors
+// p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2} (p_{-1} = 1), the Sturm sequence of the
+// tridiagonal.  Same count as the LDL^T pivots q_i = p_i / p_{i-1} < 0, without the division on the
+// critical path (one FMA per step).  The pair (p_{i-1}, p_{i-2}) is rescaled by a power of two
+// every 8 steps (exact), which keeps it far from overflow and underflow; a zero p_i is replaced by a
+// tiny multiple of p_{i-1} (a zero pivot counts as non-negative, as in the division form).
 __device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x) {
     int c = 0;
-    double q = d[0] - x;
-    if (q < 0.0) ++c;
+    double p2 = 1.0;
+    double p1 = d[0] - x;
+    if (p1 == 0.0) p1 = 0x1p-200;
+    bool neg = p1 < 0.0;
+    if (neg) ++c;
     for (int i = 1; i < n; ++i) {
-        const double qq = q == 0.0 ? 1e-300 : q;
-        q = d[i] - x - e2[i - 1] / qq;
-        if (q < 0.0) ++c;
+        double p = fma(d[i] - x, p1, -e2[i - 1] * p2);
+        if (p == 0.0) p = 0x1p-200 * p1;
+        const bool ng = p < 0.0;
+        c += ng != neg;
+        neg = ng;
+        p2 = p1;
+        p1 = p;
+        if ((i & 7) == 0) {
+            const double m = fmax(fabs(p1), fabs(p2));
+            const int ex = (int)((__double_as_longlong(m) >> 52) & 0x7ff) - 1023;
+            if (ex > 400 || ex < -400) {
+                const double sc = __longlong_as_double((long long)(1023 - ex) << 52);  // 2^-ex
+                p1 *= sc;
+                p2 *= sc;
+            }
+        }
     }
     return c;
 }
