@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/am1gpu.h"
@@ -287,9 +288,10 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
     if (m.natoms < 0 || (m.natoms > 0 && (!m.z || !m.xyz_bohr))) return fail(AM1GPU_INVALID_INPUT, "null molecule arrays");
     if (m.multiplicity < 1) return fail(AM1GPU_INVALID_INPUT, "multiplicity must be >= 1");
     const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
+    const DevElem* tab = host_param_table() + method * (MAX_Z + 1);  // once, not per atom
     for (int i = 0; i < m.natoms; ++i) {
         const int z = m.z[i];
-        if (z < 0 || z > MAX_Z || !helem(method, z).present) {
+        if (z < 0 || z > MAX_Z || !tab[z].present) {
             std::string sup;
             for (int k = 1; k <= MAX_Z; ++k)
                 if (helem(method, k).present) sup += (sup.empty() ? "" : ", ") + std::string(kSymbols[k]);
@@ -297,7 +299,7 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
             return fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, std::string(name) + " has no parameters for element Z=" +
                                                               std::to_string(z) + "; " + name + " covers " + sup);
         }
-        if (helem(method, z).n > 3)
+        if (tab[z].n > 3)
             return fail(AM1GPU_UNSUPPORTED, std::string("element ") + kSymbols[z] +
                                                 " has a valence shell n >= 4; its Slater overlap needs the numerical quadrature, "
                                                 "which this GPU path does not implement");
@@ -305,7 +307,7 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
             return fail(AM1GPU_INVALID_INPUT, "non-finite coordinate for atom " + std::to_string(i));
     }
     double n_elec = 0.0;
-    for (int i = 0; i < m.natoms; ++i) n_elec += helem(method, m.z[i]).core_charge;
+    for (int i = 0; i < m.natoms; ++i) n_elec += tab[m.z[i]].core_charge;
     n_elec -= m.charge;
     const long long ne = (long long)std::llround(n_elec);
     if (std::fabs(n_elec - (double)ne) > 1.0e-6 || ne < 0)
@@ -334,23 +336,23 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
     p.n_occ[1] = uhf ? n_beta : n_alpha;
     p.order.clear();
     for (int i = 0; i < m.natoms; ++i)
-        if (helem(method, m.z[i]).norb == 4) p.order.push_back(i);
+        if (tab[m.z[i]].norb == 4) p.order.push_back(i);
     p.nheavy = (int)p.order.size();
     for (int i = 0; i < m.natoms; ++i)
-        if (helem(method, m.z[i]).norb != 4) p.order.push_back(i);
+        if (tab[m.z[i]].norb != 4) p.order.push_back(i);
     p.nao = 4 * p.nheavy + (m.natoms - p.nheavy);
     // caller AO offsets
     std::vector<int> uoff(m.natoms);
     int acc = 0;
     for (int i = 0; i < m.natoms; ++i) {
         uoff[i] = acc;
-        acc += helem(method, m.z[i]).norb;
+        acc += tab[m.z[i]].norb;
     }
     p.ao_map.assign(p.nao, 0);
     int k = 0;
     for (int ia = 0; ia < m.natoms; ++ia) {
         const int u = p.order[ia];
-        const int no = helem(method, m.z[u]).norb;
+        const int no = tab[m.z[u]].norb;
         for (int t = 0; t < no; ++t) p.ao_map[k++] = uoff[u] + t;
     }
     if (!choose_cluster(p.nao, &p.npad, &p.cluster))
@@ -1102,22 +1104,42 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
             if (status) status[i] = rc;
         return rc;
     }
+    // plan every molecule (validation, atom order, AO map): independent per molecule, so large
+    // batches plan on several host threads; results and the first error are taken in input order
+    std::vector<MolPlan> all(nmol);
+    std::vector<int> rcs(nmol, AM1GPU_OK);
+    std::vector<std::string> msgs(nmol);
+    auto plan_range = [&](int lo, int hi) {
+        for (int i = lo; i < hi; ++i) {
+            if (mols[i].natoms == 0 && mols[i].multiplicity >= 1 && std::fabs(mols[i].charge) < 1e-6) {
+                fill_empty(&res[i]);
+                rcs[i] = -1;  // solved: nothing to plan
+                continue;
+            }
+            rcs[i] = plan_molecule(mols[i], *opts, i, all[i]);
+            if (rcs[i]) msgs[i] = g_err;
+        }
+    };
+    const int nthr = nmol >= 512 ? (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (nthr > 1) {
+        std::vector<std::thread> pool;
+        const int chunk = (nmol + nthr - 1) / nthr;
+        for (int t = 0; t < nthr; ++t) pool.emplace_back(plan_range, t * chunk, std::min(nmol, (t + 1) * chunk));
+        for (auto& th : pool) th.join();
+    } else {
+        plan_range(0, nmol);
+    }
     std::vector<MolPlan> plans;
+    plans.reserve(nmol);
     int first = AM1GPU_OK;
     std::string first_msg;
     for (int i = 0; i < nmol; ++i) {
-        MolPlan p;
-        int r = AM1GPU_OK;
-        if (mols[i].natoms == 0 && mols[i].multiplicity >= 1 && std::fabs(mols[i].charge) < 1e-6) {
-            fill_empty(&res[i]);
-        } else {
-            r = plan_molecule(mols[i], *opts, i, p);
-            if (r == AM1GPU_OK) plans.push_back(std::move(p));
-        }
+        const int r = rcs[i] < 0 ? AM1GPU_OK : rcs[i];
+        if (rcs[i] == AM1GPU_OK) plans.push_back(std::move(all[i]));
         if (status) status[i] = r;
         if (r && !first) {
             first = r;
-            first_msg = g_err;
+            first_msg = msgs[i];
         }
     }
     if (!plans.empty()) {
