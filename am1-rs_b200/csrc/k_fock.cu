@@ -2,14 +2,14 @@
 //
 // One warp per atom A; every off-diagonal block has exactly one writer and every sum is a
 // gather in a fixed order, so the result is deterministic and needs no atomics.
-//   * heavy partners B of a heavy A (100-integral blocks, src/fock.rs:427-466): one pair at a
-//     time, the block staged through shared memory with coalesced loads; lanes 16..25 gather the
-//     Coulomb term J_A = sum_B (A A | B B) . P_BB, lanes 0..15 the 16 exchange outputs
-//     K_AB = -s sum P^s_ab (mu nu | lambda sigma) when B > A, written to F_AB and F_BA;
-//   * every other partner (a hydrogen B, or any B of a hydrogen A: blocks of 10 or 1 integrals)
-//     is handled lane-parallel, 32 partners at a time: each lane gathers its partner's share of
-//     J_A in registers (reduced over the warp once per atom) and writes the exchange column
-//     F_AB, F_BA of its partner when A is the pair's first atom.
+//   * the Coulomb term J_A = sum_B (A A | B B) . P_BB (src/fock.rs:427-448) is gathered
+//     lane-parallel, a partner per lane, 32 at a time, in registers, and reduced over the warp once
+//     per atom;
+//   * the exchange blocks K_AB = -s sum P^s_ab (mu nu | lambda sigma) (src/fock.rs:449-466) of a
+//     heavy A with heavy B > A: one pair at a time, the 100-integral block staged through shared
+//     memory with coalesced loads, lanes 0..15 on the 16 outputs, written to F_AB and F_BA;
+//   * the exchange of every other pair (a hydrogen on either side: blocks of 10 or 1 integrals)
+//     lane-parallel, the lane of the partner writing F_AB and F_BA when A is the pair's first atom.
 // The one-centre terms (oc_two_electron, src/fock.rs:27-65 and 321-344) finish the diagonal.
 #include <cuda_runtime.h>
 
@@ -41,7 +41,7 @@ constexpr int FOCK_WARPS = 8;
 __host__ __device__ constexpr int pair_hi(int q) { return q < 1 ? 0 : q < 3 ? 1 : q < 6 ? 2 : 3; }
 __host__ __device__ constexpr int pair_lo(int q) { return q - pair_hi(q) * (pair_hi(q) + 1) / 2; }
 
-__global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restrict__ mols, const int* __restrict__ atom_mol,
+__global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __restrict__ mols, const int* __restrict__ atom_mol,
                                                          int natoms_total, const DevElem* __restrict__ params,
                                                          const int* __restrict__ atom_z, const double* __restrict__ wstore,
                                                          double* __restrict__ arena, const MolState* __restrict__ st, int force) {
@@ -72,40 +72,54 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
     double* wb = s_w[warp];
     auto ptot = [&](long long idx) { return P1 ? P0[idx] + P1[idx] : P0[idx]; };
 
-    double jacc = 0.0;  // heavy-heavy part: lane 16 + k owns J_A[k]
+    // Coulomb gather J_A (per lane over its partners, reduced over the warp once at the end)
+    double jl[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) jl[k] = 0.0;
     if (aheavy) {
-        for (int B = 0; B < h; ++B) {
+        // heavy partners, lane-parallel: J_A += (AA|BB) . P_BB over the 10x10 block of the pair
+        for (int B = lane; B < h; B += 32) {
             if (B == A) continue;
             const int oB = 4 * B;
             const int i = min(A, B), j = max(A, B);
             const double* blk = w + 100LL * ((long long)i * h - (long long)i * (i + 1) / 2 + (j - i - 1));
-            for (int l = lane; l < 100; l += 32) wb[l] = blk[l];
-            if (lane < 10) {  // packed P_BB, off-diagonal pairs counted twice
-                const int hi = pair_hi(lane), lo = pair_lo(lane);
+            double pq[10];  // packed P_BB, off-diagonal pairs counted twice
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                const int hi = pair_hi(q), lo = pair_lo(q);
                 const double v = ptot((long long)(oB + hi) * n + oB + lo);
-                s_q[warp][lane] = hi == lo ? v : 2.0 * v;
+                pq[q] = hi == lo ? v : 2.0 * v;
             }
-            const bool do_k = B > A;
-            if (do_k && lane < 16) {
+            if (A == i) {  // A's side of the block is its rows
+#pragma unroll
+                for (int k = 0; k < 10; ++k) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 10; ++q) acc = fma(blk[k * 10 + q], pq[q], acc);
+                    jl[k] += acc;
+                }
+            } else {  // A is the pair's second atom: its side is the columns
+#pragma unroll
+                for (int k = 0; k < 10; ++k) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 10; ++q) acc = fma(blk[q * 10 + k], pq[q], acc);
+                    jl[k] += acc;
+                }
+            }
+        }
+        // exchange blocks with the heavier-indexed heavy partners (A is the pair's first atom)
+        for (int B = A + 1; B < h; ++B) {
+            const int oB = 4 * B;
+            const double* blk = w + 100LL * ((long long)A * h - (long long)A * (A + 1) / 2 + (B - A - 1));
+            for (int l = lane; l < 100; l += 32) wb[l] = blk[l];
+            if (lane < 16) {
                 const long long idx = (long long)(oA + (lane >> 2)) * n + oB + (lane & 3);
                 s_pab[warp][0][lane] = P0[idx];
                 if (P1) s_pab[warp][1][lane] = P1[idx];
             }
             __syncwarp();
-            if (lane >= 16 && lane < 26) {
-                // Coulomb: A's side of the block is its rows when A is the first atom, else its columns
-                const int k = lane - 16;
-                double acc = 0.0;
-                if (A == i) {
-#pragma unroll
-                    for (int q = 0; q < 10; ++q) acc += wb[k * 10 + q] * s_q[warp][q];
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 10; ++q) acc += wb[q * 10 + k] * s_q[warp][q];
-                }
-                jacc += acc;
-            }
-            if (do_k && lane < 16) {  // exchange block (A = first atom, B = second)
+            if (lane < 16) {
                 const int mu = lane >> 2, la = lane & 3;
                 const long long ab = (long long)(oA + mu) * n + oB + la;
                 const long long ba = (long long)(oB + la) * n + oA + mu;
@@ -128,9 +142,6 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
         }
     }
     // every other partner, lane-parallel
-    double jl[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) jl[k] = 0.0;
     if (aheavy) {
         // hydrogen partners B (XH blocks: A's 10 packed pairs x B's ss); A is the first atom
         for (int B = h + lane; B < N; B += 32) {
@@ -191,7 +202,7 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
             }
         }
     }
-    // J_A = heavy-heavy part (lanes 16..25) + the lane-parallel part (reduced over the warp)
+    // J_A: the lane-parallel sums reduced over the warp
 #pragma unroll
     for (int k = 0; k < 10; ++k) {
         double v = jl[k];
@@ -204,7 +215,7 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS) k_fock(const MolDesc* __restr
         for (int k = 0; k < 10; ++k) s_q[warp][k] = jl[k];
     }
     __syncwarp();
-    if (lane >= 16 && lane < 16 + npA) s_j[warp][lane - 16] = jacc + s_q[warp][lane - 16];
+    if (lane < npA) s_j[warp][lane] = s_q[warp][lane];
     __syncwarp();
     // one-centre terms and the diagonal block
     if (lane < 16) {
