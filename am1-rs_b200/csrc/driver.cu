@@ -888,7 +888,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
             if ((rc = run.end(AM1GPU_PHASE_ACCEL, ph)) || (rc = run.begin(&ph))) return rc;
             if (density_mode() == 0) {
                 // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
-                k_sp2_bounds<<<njobs, 256, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
+                k_sp2_bounds<<<njobs, 512, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
                 k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
                 k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
                 CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));

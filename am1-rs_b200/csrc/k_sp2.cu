@@ -32,7 +32,7 @@ namespace am1 {
 // the interval maps just outside [0, 1], where the trace-correcting steps pull it back; a run
 // that still fails to converge falls back to the eigensolver.  One CTA per channel.
 constexpr int SP2_LANCZOS = 12;
-constexpr int SP2_BOUND_THREADS = 256;
+constexpr int SP2_BOUND_THREADS = 512;
 
 __device__ double bounds_block_sum(double v, double* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -143,12 +143,17 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
     int m = 0;
     double bprev = 0.0;
     for (int j = 0; j < K; ++j) {
-        for (int r = warp; r < n; r += NW) {
-            const double* Fr = jb.F + (long long)r * n;
+        // w = F q: eight lanes per row, so every warp has four rows' loads in flight
+        const int sub = lane >> 3, sl = lane & 7;
+        for (int r0 = 4 * warp; r0 < n; r0 += 4 * NW) {
+            const int r = r0 + sub;
             double acc = 0.0;
-            for (int c = lane; c < n; c += 32) acc = fma(Fr[c], q[c], acc);
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) w[r] = acc;
+            if (r < n) {
+                const double* Fr = jb.F + (long long)r * n;
+                for (int c = sl; c < n; c += 8) acc = fma(Fr[c], q[c], acc);
+            }
+            for (int o = 4; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (sl == 0 && r < n) w[r] = acc;
         }
         __syncthreads();
         double part = 0.0;

@@ -108,7 +108,7 @@ __global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles
 __global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
 __global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force, const int* mask);
 __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, const int* mask);
-// one CTA of 256 threads per job, 3 n doubles of dynamic shared memory
+// one CTA of 512 threads per job, 3 n doubles of dynamic shared memory
 __global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
