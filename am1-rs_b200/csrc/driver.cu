@@ -64,12 +64,16 @@ struct DeviceCtx {
     int sms = 0;
     int jacobi_smem = 0;  // dynamic shared memory available to one eigensolver CTA
     int tridiag_smem = 0;  // ... and to one tridiagonalisation CTA
+    int trib_grid = 0;     // CTAs of the grid-wide tridiagonalisation (all co-resident)
+    int sp2b_grid = 0;     // ... and of the grid-wide Lanczos bounds
 };
 
 // Shared-memory budgets the planner sizes eigensolver and tridiagonalisation clusters for (set
 // when a device is opened).
 int g_jacobi_budget = 232448 - 1024;
 int g_tridiag_budget = 232448 - 1024;
+int g_trib_grid = 148;  // CTAs of the grid-wide tridiagonalisation (set when a device is opened)
+int g_sp2b_grid = 148;  // ... and of the grid-wide Lanczos bounds
 
 // Smallest cluster (1, 2, 4, 8, 16 CTAs) whose row share of an n x n matrix fits one CTA's
 // shared memory; 0 when none does.
@@ -109,6 +113,22 @@ int device_ctx(DeviceCtx** out) {
             return bad("jacobi smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("jacobi cluster attribute", err);
+        {
+            int per_sm = 0;
+            if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_big, TRIB_THREADS, 0)) != cudaSuccess)
+                return bad("grid tridiagonalisation occupancy", err);
+            c.trib_grid = std::max(1, std::min(per_sm, 2)) * c.sms;
+            if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sp2_bounds_big, 512, 0)) != cudaSuccess)
+                return bad("grid bounds occupancy", err);
+            c.sp2b_grid = std::max(1, std::min(per_sm, 2)) * c.sms;
+        }
+        for (const void* f : {(const void*)k_bisect, (const void*)k_sp2_bounds}) {  // 2 n and 3 n doubles
+            cudaFuncAttributes fb{};
+            if ((err = cudaFuncGetAttributes(&fb, f)) != cudaSuccess) return bad("bisection / bounds attributes", err);
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fb.sharedSizeBytes)) !=
+                cudaSuccess)
+                return bad("bisection / bounds smem attribute", err);
+        }
         if ((err = cudaFuncGetAttributes(&fa, k_tridiag)) != cudaSuccess) return bad("tridiag attributes", err);
         c.tridiag_smem = optin - (int)fa.sharedSizeBytes;
         if ((err = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, c.tridiag_smem)) != cudaSuccess)
@@ -123,6 +143,8 @@ int device_ctx(DeviceCtx** out) {
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
     g_tridiag_budget = c.tridiag_smem;
+    g_trib_grid = c.trib_grid;
+    g_sp2b_grid = c.sp2b_grid;
     *out = &c;
     return AM1GPU_OK;
 }
@@ -267,6 +289,11 @@ struct MolPlan {
     std::vector<int> ao_map; // internal AO -> caller AO
 };
 
+// Largest molecule (orbitals) the purification path takes: the Lanczos bounds and the bisection hold
+// 3 n and 2 n doubles in one CTA's shared memory.
+constexpr int kMaxAo = 8192;
+int density_mode();
+
 int choose_cluster(int n, int* npad_out, int* c_out) {
     static const int cs[5] = {1, 2, 4, 8, 16};
     for (int k = 0; k < 5; ++k) {
@@ -355,9 +382,18 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
         const int no = tab[m.z[u]].norb;
         for (int t = 0; t < no; ++t) p.ao_map[k++] = uoff[u] + t;
     }
-    if (!choose_cluster(p.nao, &p.npad, &p.cluster))
-        return fail(AM1GPU_UNSUPPORTED, "molecule with " + std::to_string(p.nao) +
-                                            " orbitals exceeds the cluster eigensolver's shared-memory capacity (448)");
+    if (!choose_cluster(p.nao, &p.npad, &p.cluster)) {
+        // larger than the cluster eigensolver holds: the purification SCF and the final spectrum
+        // (grid-wide tridiagonalisation) still run; eigenvectors and the eigensolver path do not
+        if (p.nao > kMaxAo)
+            return fail(AM1GPU_UNSUPPORTED, "molecule with " + std::to_string(p.nao) + " orbitals exceeds the limit of " +
+                                                std::to_string(kMaxAo));
+        if (density_mode() != 0)
+            return fail(AM1GPU_UNSUPPORTED, "the eigensolver density path holds at most 448 orbitals; this molecule has " +
+                                                std::to_string(p.nao));
+        p.cluster = 0;
+        p.npad = p.nao;
+    }
     return AM1GPU_OK;
 }
 
@@ -380,6 +416,8 @@ struct Batch {
     struct Bucket { int off, count, C; size_t smem; };
     std::vector<Bucket> buckets;      // eigensolver jobs by cluster size
     std::vector<Bucket> tri_buckets;  // tridiagonalisation jobs by cluster size
+    std::vector<TriJob> tri_big;      // matrices too large for a cluster (grid-wide kernel)
+    std::vector<int> sp2_big;         // purification jobs of those matrices (grid-wide Lanczos)
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
@@ -567,6 +605,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     std::vector<EigJob> eig_all;
     std::vector<int> eig_cluster;
     std::vector<TriJob> tri_all;
+    b.sp2_big.clear();
     for (int mi = 0; mi < b.nmol; ++mi) {
         MolPlan& p = b.plans[mi];
         const am1gpu_molecule& m = in[p.user];
@@ -671,6 +710,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             // F and P starts on 16 bytes: even n (slot bases are then 16-byte aligned too)
             const bool pairs = n % 2 == 0 && aligned16(sj.X0) && aligned16(sj.X1) && aligned16(cj.F) && aligned16(cj.P);
             std::vector<GemmTile>& tl = pairs ? tiles_pairs : tiles_other;
+            sj.fallback = p.cluster > 0;
+            if (!sj.fallback) b.sp2_big.push_back(job);
             sj.tile0 = (int)tl.size();  // tile index inside its own launch
             for (int x = 0; x < (int)tn_; ++x)
                 for (int y = x; y < (int)tn_; ++y) tl.push_back(GemmTile{job, x, y});
@@ -678,6 +719,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             hsp2[job] = sj;
             TriJob tj{};
             tj.A = cj.Fx;
+            tj.W = base + SLOT_GT * nn;    // large matrices: the working copy (free after the SCF)
+            tj.work = base + SLOT_VS * nn;  // and the scratch vectors
             tj.d = tri_d;
             tj.e = tri_e;
             tj.eps = cj.eps;
@@ -708,8 +751,10 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             ej.n = (int)n;
             ej.npad = p.npad;
             ej.mol = mi;
-            eig_all.push_back(ej);
-            eig_cluster.push_back(p.cluster);
+            if (p.cluster > 0) {  // large molecules have no eigensolver job
+                eig_all.push_back(ej);
+                eig_cluster.push_back(p.cluster);
+            }
             ++job;
         }
         hm[mi] = md;
@@ -747,11 +792,15 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     for (size_t i = 0; i < tix.size(); ++i) tix[i] = (int)i;
     std::stable_sort(tix.begin(), tix.end(), [&](int x, int y) { return tri_all[x].n > tri_all[y].n; });
     b.tri_buckets.clear();
+    b.tri_big.clear();
     for (size_t i = 0; i < tix.size(); ++i) {
         const TriJob& tj = tri_all[tix[i]];
         htri[i] = tj;
         const int C = tridiag_cluster(tj.n);
-        if (!C) return fail(AM1GPU_UNSUPPORTED, "matrix too large for the on-chip tridiagonalisation");
+        if (!C) {  // too large for a cluster: the grid-wide kernel (these sort first)
+            b.tri_big.push_back(tj);
+            continue;
+        }
         if (b.tri_buckets.empty() || b.tri_buckets.back().C != C) b.tri_buckets.push_back({(int)i, 0, C, 0});
         b.tri_buckets.back().count++;
         b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tj.n, C));
@@ -889,6 +938,12 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
             if (density_mode() == 0) {
                 // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
                 k_sp2_bounds<<<njobs, 512, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
+                for (int jbig : b.sp2_big) {  // one cooperative launch per large matrix
+                    const Sp2Job* jobs = b.d_sp2;
+                    const MolState* stp = b.d_st;
+                    void* args[] = {&jobs, &jbig, &stp};
+                    CK(cudaLaunchCooperativeKernel((const void*)k_sp2_bounds_big, dim3(g_sp2b_grid), dim3(512), args, 0, s));
+                }
                 k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
                 k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
                 CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
@@ -912,13 +967,15 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                         if (b.h_active[1] == 0) break;
                     }
                 }
-                k_sp2_finish<<<dim3(8, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_work);
+                const unsigned fin_blocks = std::max(8u, std::min(256u, cdiv((long long)b.maxn * b.maxn, 65536)));
+                k_sp2_finish<<<dim3(fin_blocks, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_status,
+                                                                     b.d_work);
                 run.launched(AM1GPU_PHASE_EIGEN);
                 // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
                 k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
                 if ((rc = launch_jacobi(b, ws, 0, b.d_need_eigen))) return rc;
                 run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
-                k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
+                if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
                 k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
                 run.launched(AM1GPU_PHASE_EIGEN, 3);
                 if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
@@ -930,7 +987,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 if ((rc = launch_jacobi(b, ws, 0))) return rc;
                 run.launched(AM1GPU_PHASE_DENSITY_CORE, (int)b.buckets.size());
                 if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pj))) return rc;
-                k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
+                if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
                 run.launched(AM1GPU_PHASE_EIGEN, 2);
                 if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
                 k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, nullptr);
@@ -955,10 +1012,15 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
     // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
     if ((rc = launch_tridiag(b, ws))) return rc;
-    k_bisect<<<njobs, 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue (n <= 448)
+    for (const TriJob& tj : b.tri_big) {  // one cooperative launch per large matrix
+        TriJob arg = tj;
+        void* args[] = {&arg};
+        CK(cudaLaunchCooperativeKernel((const void*)k_tridiag_big, dim3(g_trib_grid), dim3(TRIB_THREADS), args, 0, s));
+    }
+    k_bisect<<<dim3(njobs, cdiv(b.maxn, 512)), 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
-    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size());
+    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() + (int)b.tri_big.size());
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;
@@ -1048,6 +1110,9 @@ int write_result(Batch& b, Mem* ws, int mi, am1gpu_result* r, am1gpu_call_stats*
         const ChanJob& jc = b.jobs[b.job0[mi] + c];
         if (e_out) std::memcpy(e_out, b.h_eps + (jc.eps - b.d_eps), sizeof(double) * n);  // fetched in bulk
         if (c_out) {
+            if (p.cluster == 0)
+                return fail(AM1GPU_UNSUPPORTED, "eigenvectors (mo_coeff) are available up to 448 orbitals; this molecule has " +
+                                                    std::to_string(n) + " (every other result is filled)");
             if (density_mode() == 0) {
                 // the purification path has no eigenvectors: diagonalise the last F* now
                 int rc = fetch_matrix(ws, jc.Fx, n, t0, stats);

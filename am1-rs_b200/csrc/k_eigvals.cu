@@ -122,46 +122,51 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
         const int G = max(1, min(16, TRI_THREADS / (((ncol + 31) / 32) * 32)));
         const int cpg = TRI_THREADS / G;
         const int g = tid / cpg, j = tid - g * cpg;
-        double acc = 0.0;
-        if (g < G && j < ncol) {
-            const int r = s + 1 + j;
-            const double vr = v[r], wr = w[r];
-            int lr = lr0 + g;
-            for (; lr + 3 * G < lre; lr += 4 * G) {  // four independent rows per trip
-                double* a0 = A + (size_t)lr * n + r;
-                double* a1 = a0 + (size_t)G * n;
-                double* a2 = a1 + (size_t)G * n;
-                double* a3 = a2 + (size_t)G * n;
-                const int c0 = lr * C + crank, c1 = c0 + G * C, c2 = c1 + G * C, c3 = c2 + G * C;
-                const double x0 = *a0, x1 = *a1, x2 = *a2, x3 = *a3;
-                const double y0 = x0 - v[c0] * wr - w[c0] * vr, y1 = x1 - v[c1] * wr - w[c1] * vr;
-                const double y2 = x2 - v[c2] * wr - w[c2] * vr, y3 = x3 - v[c3] * wr - w[c3] * vr;
-                *a0 = y0;
-                *a1 = y1;
-                *a2 = y2;
-                *a3 = y3;
-                acc = fma(y0, vn[c0], acc);
-                acc = fma(y1, vn[c1], acc);
-                acc = fma(y2, vn[c2], acc);
-                acc = fma(y3, vn[c3], acc);
+        // columns s + 1 + j, j = this thread's index in its group, then strided by the group size
+        // (more columns than threads take several trips; more groups only when columns are few)
+        for (int jj = j; jj < ncol || (G > 1 && jj == j); jj += cpg) {
+            double acc = 0.0;
+            if (g < G && jj < ncol) {
+                const int r = s + 1 + jj;
+                const double vr = v[r], wr = w[r];
+                int lr = lr0 + g;
+                for (; lr + 3 * G < lre; lr += 4 * G) {  // four independent rows per trip
+                    double* a0 = A + (size_t)lr * n + r;
+                    double* a1 = a0 + (size_t)G * n;
+                    double* a2 = a1 + (size_t)G * n;
+                    double* a3 = a2 + (size_t)G * n;
+                    const int c0 = lr * C + crank, c1 = c0 + G * C, c2 = c1 + G * C, c3 = c2 + G * C;
+                    const double x0 = *a0, x1 = *a1, x2 = *a2, x3 = *a3;
+                    const double y0 = x0 - v[c0] * wr - w[c0] * vr, y1 = x1 - v[c1] * wr - w[c1] * vr;
+                    const double y2 = x2 - v[c2] * wr - w[c2] * vr, y3 = x3 - v[c3] * wr - w[c3] * vr;
+                    *a0 = y0;
+                    *a1 = y1;
+                    *a2 = y2;
+                    *a3 = y3;
+                    acc = fma(y0, vn[c0], acc);
+                    acc = fma(y1, vn[c1], acc);
+                    acc = fma(y2, vn[c2], acc);
+                    acc = fma(y3, vn[c3], acc);
+                }
+                for (; lr < lre; lr += G) {
+                    const int c = lr * C + crank;
+                    double* ap = A + (size_t)lr * n + r;
+                    const double y = *ap - v[c] * wr - w[c] * vr;
+                    *ap = y;
+                    acc = fma(y, vn[c], acc);
+                }
             }
-            for (; lr < lre; lr += G) {
-                const int c = lr * C + crank;
-                double* ap = A + (size_t)lr * n + r;
-                const double y = *ap - v[c] * wr - w[c] * vr;
-                *ap = y;
-                acc = fma(y, vn[c], acc);
-            }
-        }
-        if (G == 1) {
-            if (j < ncol) pp[s + 1 + j] = acc;
-        } else {  // uniform over the CTA
-            red2[tid] = acc;
-            __syncthreads();
-            if (g == 0 && j < ncol) {
-                double t = 0.0;
-                for (int q = 0; q < G; ++q) t += red2[q * cpg + j];
-                pp[s + 1 + j] = t;
+            if (G == 1) {
+                if (jj < ncol) pp[s + 1 + jj] = acc;
+            } else {  // one trip only (ncol <= cpg), uniform over the CTA
+                red2[tid] = acc;
+                __syncthreads();
+                if (g == 0 && jj < ncol) {
+                    double t = 0.0;
+                    for (int q = 0; q < G; ++q) t += red2[q * cpg + jj];
+                    pp[s + 1 + jj] = t;
+                }
+                break;
             }
         }
         if (!has_next) break;
@@ -198,6 +203,121 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
         }
     }
     csync();  // no CTA leaves while another may still address its shared memory
+}
+
+// Householder reduction of one matrix too large for a cluster's shared memory (n > ~448), by the
+// whole GPU in one cooperative launch: the matrix is copied to W (global memory, row-major), row r
+// belongs to CTA r % G, and every step takes two grid barriers.  Step s, as in k_tridiag:
+//   (a) the CTA owning row s applies update s-1 to it (all its threads, a column each) and derives
+//       reflector s (a block reduction for the norm): v_s into global scratch, beta_s, d[s], e[s]
+//   grid barrier
+//   (b) every CTA, a warp per own row r > s: apply update s-1 to row r (columns > s) and form
+//       p_r = beta_s W[r, s+1:] . v_s in the same pass; the CTA's share of p.v
+//   grid barrier
+//   every CTA sums the G shares in the same order, so all hold the same kk_s = beta_s (p.v) / 2;
+//   w_s = p_s - kk_s v_s is never stored, only formed where it is used.
+// Scratch (job.work): v[2][n] | p[2][n] | share[G] | beta[2].
+__global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
+    cg::grid_group grid = cg::this_grid();
+    const int G = (int)gridDim.x, gi = (int)blockIdx.x;
+    const int n = jb.n;
+    double* W = jb.W;
+    double* vb = jb.work;              // v_s, two buffers
+    double* pb = vb + 2 * (size_t)n;   // p_s, two buffers
+    double* share = pb + 2 * (size_t)n;
+    double* bb = share + G;            // beta_s, two buffers
+    constexpr int NW = TRIB_THREADS / 32;
+    __shared__ double red[NW + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    auto bsum = [&](double v) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        __syncthreads();
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        double t = 0.0;
+        for (int q = 0; q < NW; ++q) t += red[q];
+        return t;
+    };
+    // own rows into W; update "-1" is the identity: v = p = 0, kk = 0
+    for (int r = gi + warp * G; r < n; r += NW * G)
+        for (int c = lane; c < n; c += 32) W[(size_t)r * n + c] = jb.A[(size_t)r * n + c];
+    for (int c = gi * TRIB_THREADS + tid; c < n; c += G * TRIB_THREADS) {
+        vb[n + c] = 0.0;
+        pb[n + c] = 0.0;
+    }
+    double kk = 0.0;
+    grid.sync();
+    for (int s = 0; s + 1 < n; ++s) {
+        const int cur = (s + 1) & 1, nxt = s & 1;
+        const double* v = vb + (size_t)cur * n;  // reflector s - 1
+        const double* p = pb + (size_t)cur * n;
+        double* vn = vb + (size_t)nxt * n;       // reflector s
+        double* pn = pb + (size_t)nxt * n;
+        const bool has_next = s + 2 < n;
+        if (gi == s % G) {  // (a)
+            double* row = W + (size_t)s * n;
+            const double vs = __ldcg(v + s), ws = __ldcg(p + s) - kk * vs;
+            double nrm = 0.0;
+            for (int c = s + tid; c < n; c += TRIB_THREADS) {
+                const double vc = __ldcg(v + c);
+                const double y = row[c] - vs * (__ldcg(p + c) - kk * vc) - ws * vc;
+                row[c] = y;
+                if (c > s) {
+                    vn[c] = y;
+                    nrm += y * y;
+                }
+            }
+            nrm = bsum(nrm);  // its barriers also make row[s], row[s + 1] visible to thread 0
+            if (tid == 0) {
+                const double alpha = sqrt(nrm), x0 = row[s + 1];
+                const double sg = x0 >= 0.0 ? 1.0 : -1.0;
+                jb.d[s] = row[s];
+                if (has_next) {
+                    jb.e[s] = alpha == 0.0 ? 0.0 : -sg * alpha;
+                    bb[nxt] = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x0)));
+                    if (alpha != 0.0) vn[s + 1] = x0 + sg * alpha;
+                } else {
+                    jb.e[s] = row[s + 1];  // the last 2 x 2 block: e[n-2]
+                }
+            }
+        }
+        grid.sync();  // v_s and beta_s ready
+        // (b) own rows r > s, a warp per row
+        const double beta = has_next ? __ldcg(bb + nxt) : 0.0;
+        double part = 0.0;
+        const int r0 = s + 1 + ((gi - (s + 1) % G) % G + G) % G;  // first own row > s
+        for (int r = r0 + warp * G; r < n; r += NW * G) {
+            double* row = W + (size_t)r * n;
+            const double vr = __ldcg(v + r), wr = __ldcg(p + r) - kk * vr;
+            double acc = 0.0;
+#pragma unroll 4
+            for (int c = s + 1 + lane; c < n; c += 32) {
+                const double vc = __ldcg(v + c);
+                const double y = row[c] - vr * (__ldcg(p + c) - kk * vc) - wr * vc;
+                row[c] = y;
+                acc = fma(y, __ldcg(vn + c), acc);
+            }
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            const double pr = beta * acc;
+            if (lane == 0 && has_next) pn[r] = pr;
+            part += pr * __ldcg(vn + r);
+        }
+        if (!has_next) break;
+        part = bsum(lane == 0 ? part : 0.0);
+        if (tid == 0) share[gi] = part;
+        grid.sync();  // p_s and every share ready
+        if (tid == 0) {
+            double pv = 0.0;
+            for (int q = 0; q < G; ++q) pv += __ldcg(share + q);
+            red[NW] = 0.5 * beta * pv;
+        }
+        __syncthreads();
+        kk = red[NW];
+        __syncthreads();
+    }
+    __syncthreads();
+    if (n == 1 && gi == 0 && tid == 0) jb.d[0] = W[0];
+    if (n >= 2 && gi == (n - 1) % G && tid == 0) jb.d[n - 1] = W[(size_t)(n - 1) * n + n - 1];
 }
 
 // Number of eigenvalues of T below x: the sign changes of the leading principal minors
@@ -259,7 +379,9 @@ __global__ void k_bisect(const TriJob* __restrict__ jobs, const int* __restrict_
         bounds[1] = hi + pad;
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int k0 = blockIdx.y * blockDim.x;  // this block's share of the eigenvalue indices
+    if (k0 >= n) return;
+    for (int k = k0 + threadIdx.x; k < min(n, k0 + (int)blockDim.x); k += blockDim.x) {
         double lo = bounds[0], hi = bounds[1];
         for (int it = 0; it < 200; ++it) {
             const double mid = 0.5 * (lo + hi);

@@ -11,6 +11,7 @@
 // folds in the choice of branch and the tile's share of tr X and ||X||_F^2 (= tr X^2 for the
 // next step's decision).  No eigenvectors, no fine-grained synchronisation: every step is one
 // launch over all (molecule, channel) tiles of the batch.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "am1gpu_internal.h"
@@ -18,6 +19,8 @@
 #include "kernels.h"
 
 namespace am1 {
+
+namespace cg = cooperative_groups;
 
 
 // Spectral bounds [e_min, e_max] of F* for the SP2 mapping.  The number of purification steps
@@ -96,7 +99,7 @@ __device__ double lz_last_component(const double* a, const double* b, int m, dou
 
 __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* __restrict__ jobs, const MolState* __restrict__ st) {
     const Sp2Job jb = jobs[blockIdx.x];
-    if (!st[jb.mol].active) return;
+    if (!st[jb.mol].active || !jb.fallback) return;  // large matrices: k_sp2_bounds_big
     const int n = jb.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = SP2_BOUND_THREADS / 32;
@@ -208,6 +211,149 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
         jb.bounds[0] = fmax(lo, glo);
         jb.bounds[1] = fmin(hi, ghi);
     }
+}
+
+// The interval from the Lanczos tridiagonal (alpha, beta of m steps) and the Gershgorin bounds.
+__device__ void lz_interval(const double* alpha, const double* beta, int m, double glo, double ghi, double* out) {
+    double tlo = 1e300, thi = -1e300;
+    for (int i = 0; i < m; ++i) {
+        const double rad = (i > 0 ? fabs(beta[i - 1]) : 0.0) + (i + 1 < m ? fabs(beta[i]) : 0.0);
+        tlo = fmin(tlo, alpha[i] - rad);
+        thi = fmax(thi, alpha[i] + rad);
+    }
+    const double pad = 1e-12 * (fabs(tlo) + fabs(thi)) + 1e-300;
+    tlo -= pad;
+    thi += pad;
+    const double th_min = lz_eig(alpha, beta, m, 0, tlo, thi);
+    const double th_max = lz_eig(alpha, beta, m, m - 1, tlo, thi);
+    const double width = fmax(th_max - th_min, 1e-6);
+    const double eps = 1e-8 * (fabs(th_min) + fabs(th_max) + 1.0);
+    const double bm = beta[m - 1];
+    const double r_min = fabs(bm) * lz_last_component(alpha, beta, m, th_min - eps);
+    const double r_max = fabs(bm) * lz_last_component(alpha, beta, m, th_max + eps);
+    double lo = th_min - r_min - 0.005 * width;
+    double hi = th_max + r_max + 0.005 * width;
+    if (!isfinite(lo) || !isfinite(hi) || !(hi > lo)) {
+        lo = glo;
+        hi = ghi;
+    }
+    out[0] = fmax(lo, glo);
+    out[1] = fmin(hi, ghi);
+}
+
+// k_sp2_bounds for one matrix too large for one CTA (no eigensolver fallback, n > ~448): the same
+// Lanczos run by the whole GPU in one cooperative launch.  Row r of F* belongs to CTA r % G; the
+// vectors live in global scratch (job.X1, free until purification starts) and every CTA keeps the
+// same alpha, beta (sums of the per-CTA shares in one fixed order).  Three grid barriers per step.
+// Cross-CTA data is read through L2 (__ldcg).  Scratch: q[3][n] | share[2][G].
+__global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2Job* __restrict__ jobs, int job,
+                                                                       const MolState* __restrict__ st) {
+    cg::grid_group grid = cg::this_grid();
+    const Sp2Job jb = jobs[job];
+    if (!st[jb.mol].active) return;  // uniform over the grid
+    const int G = (int)gridDim.x, gi = (int)blockIdx.x;
+    const int n = jb.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = SP2_BOUND_THREADS / 32;
+    double* qb = jb.X1;                 // three Lanczos vectors
+    double* share = qb + 3 * (size_t)n; // [2][G]
+    __shared__ double red[NW + 2];
+    __shared__ double alpha[SP2_LANCZOS], beta[SP2_LANCZOS];
+    auto bsum = [&](double v) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        __syncthreads();
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        double t = 0.0;
+        for (int q = 0; q < NW; ++q) t += red[q];
+        __syncthreads();
+        return t;
+    };
+    // Gershgorin interval and the start vector (every CTA computes the norm itself)
+    double glo = 1e300, ghi = -1e300, nq = 0.0;
+    for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
+        glo = fmin(glo, jb.rowmin[i]);
+        ghi = fmax(ghi, jb.rowmax[i]);
+        const double x = cos(0.7 * i + 0.3) + 0.5;
+        nq += x * x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+        ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+    }
+    __shared__ double gred[2][NW];
+    if (lane == 0) {
+        gred[0][warp] = glo;
+        gred[1][warp] = ghi;
+    }
+    nq = bsum(nq);
+    glo = gred[0][0];
+    ghi = gred[1][0];
+    for (int v = 1; v < NW; ++v) {
+        glo = fmin(glo, gred[0][v]);
+        ghi = fmax(ghi, gred[1][v]);
+    }
+    const double inq = 1.0 / sqrt(nq);
+    for (int i = gi * SP2_BOUND_THREADS + tid; i < n; i += G * SP2_BOUND_THREADS) {
+        qb[i] = (cos(0.7 * i + 0.3) + 0.5) * inq;  // q_0
+        qb[2 * (size_t)n + i] = 0.0;            // q_{-1}
+    }
+    grid.sync();
+    const int K = min(SP2_LANCZOS, n);
+    int m = 0, cur = 0, prv = 2;
+    double bprev = 0.0;
+    for (int j = 0; j < K; ++j) {
+        const int nxt = 3 - cur - prv;  // the third buffer: w, then q_{j+1}
+        const double* q = qb + (size_t)cur * n;
+        const double* qp = qb + (size_t)prv * n;
+        double* wq = qb + (size_t)nxt * n;
+        // w_r = F[r, :] . q for own rows (a warp per row) and the CTA's share of q . w
+        double part = 0.0;
+        for (int r = gi + warp * G; r < n; r += NW * G) {
+            const double* Fr = jb.F + (long long)r * n;
+            double acc = 0.0;
+#pragma unroll 4
+            for (int c = lane; c < n; c += 32) acc = fma(Fr[c], __ldcg(q + c), acc);
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) wq[r] = acc;
+            part += acc * __ldcg(q + r);
+        }
+        part = bsum(lane == 0 ? part : 0.0);
+        if (tid == 0) share[gi] = part;
+        grid.sync();
+        double a = 0.0;
+        for (int g = 0; g < G; ++g) a += __ldcg(share + g);
+        // w <- w - a q - b_prev q_prev on own rows, the CTA's share of |w|^2
+        part = 0.0;
+        for (int r = gi + warp * G; r < n; r += NW * G) {
+            if (lane == 0) {
+                const double x = __ldcg(wq + r) - a * __ldcg(q + r) - bprev * __ldcg(qp + r);
+                wq[r] = x;
+                part += x * x;
+            }
+        }
+        part = bsum(part);
+        if (tid == 0) share[G + gi] = part;
+        grid.sync();
+        double b2 = 0.0;
+        for (int g = 0; g < G; ++g) b2 += __ldcg(share + G + g);
+        const double bnorm = sqrt(b2);
+        if (tid == 0) {
+            alpha[j] = a;
+            beta[j] = bnorm;
+        }
+        m = j + 1;
+        if (!(bnorm > 1e-12 * fmax(fabs(a), 1.0))) break;  // invariant subspace: T is exact (uniform)
+        const double ib = 1.0 / bnorm;
+        for (int r = gi + warp * G; r < n; r += NW * G)
+            if (lane == 0) wq[r] = __ldcg(wq + r) * ib;
+        bprev = bnorm;
+        prv = cur;
+        cur = nxt;
+        grid.sync();
+    }
+    __syncthreads();
+    if (gi == 0 && tid == 0) lz_interval(alpha, beta, m, glo, ghi, jb.bounds);
 }
 
 // X0 = (e_max I - F*) / (e_max - e_min); per-block partial sums of tr X0 and ||X0||_F^2.
@@ -384,14 +530,18 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
 // P_new = w X (the converged X); molecules whose purification stalled are flagged for the
 // eigensolver path.
 __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __restrict__ sst, const MolState* __restrict__ st,
-                             int* __restrict__ need_eigen, double* __restrict__ work) {
+                             int* __restrict__ need_eigen, int* __restrict__ mol_status, double* __restrict__ work) {
     const Sp2Job jb = jobs[blockIdx.y];
     if (!st[jb.mol].active) return;
     const Sp2State& s = sst[blockIdx.y];
     if (!s.converged) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            need_eigen[jb.mol] = 1;
-            atomicAdd(&work[2], 1.0);
+            if (jb.fallback) {
+                need_eigen[jb.mol] = 1;
+                atomicAdd(&work[2], 1.0);
+            } else {
+                mol_status[jb.mol] = 5;  // AM1GPU_LINALG: no eigensolver for this size
+            }
         }
         return;
     }

@@ -72,6 +72,7 @@ struct Sp2Job {
     double* bounds;         // [2] spectral interval of F* used for the mapping (k_sp2_bounds)
     double nocc, weight;
     int n, mol, tile0, ntiles;
+    int fallback;           // 1: a stalled purification falls back to the eigensolver; 0: LINALG
 };
 
 struct Sp2State {
@@ -83,6 +84,8 @@ struct Sp2State {
 // One tridiagonalisation + bisection problem.
 struct TriJob {
     const double* A;   // symmetric input, n x n
+    double* W;         // large matrices only: working copy, n x n (global memory)
+    double* work;      // large matrices only: scratch vectors, 4 n + grid + 4 doubles
     double* d;         // diagonal, n
     double* e;         // off-diagonal, n
     double* eps;       // ascending eigenvalues, n
@@ -108,8 +111,10 @@ __global__ void k_gemm_nn(const GemmJob* jobs, const GemmTile* tiles, int ntiles
 __global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, int force, const int* mask);
 __global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force, const int* mask);
 __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, const int* mask);
-// one CTA of 512 threads per job, 3 n doubles of dynamic shared memory
+// one CTA of 512 threads per job, 3 n doubles of dynamic shared memory; jobs without an eigensolver
+// fallback (large matrices) are left to k_sp2_bounds_big, one cooperative launch each
 __global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
+__global__ void k_sp2_bounds_big(const Sp2Job* jobs, int job, const MolState* st);
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 // *16: every matrix of the tile list has even n and 16-byte aligned rows (16-byte copies);
@@ -121,11 +126,17 @@ __global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int n
 __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
-__global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work);
+__global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, int* mol_status,
+                             double* work);
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each
 __global__ void k_tridiag(const TriJob* jobs, const int* mask);
 size_t tridiag_smem_bytes(int n, int C);
+// a thread per eigenvalue; blockIdx.y selects the block of 512 eigenvalue indices (large n)
 __global__ void k_bisect(const TriJob* jobs, const int* mask);
+// matrices too large for a cluster's shared memory: one cooperative launch over the whole GPU
+// (grid <= co-resident CTAs of TRIB_THREADS threads), the matrix in global memory
+constexpr int TRIB_THREADS = 512;
+__global__ void k_tridiag_big(TriJob job);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
 __global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
