@@ -1,0 +1,28 @@
+"""The serving loop on a B200: requests arriving while batches run on several worker streams
+give the same results as the molecule solved alone."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_stream_results_equal_solo_runs(gpu):
+    from am1gpu import serve, workloads as W, _abi
+
+    reqs = [r for r in W.config3(400, rate=4000.0, seed=5) if r.mol.numbers.size <= 150][:120]
+    assert len(reqs) >= 60 and any(r.mol.multiplicity > 1 for r in reqs)
+    with serve.ScfServer(workers=3, budget_bytes=8 << 30) as srv:
+        out, wall = serve.run_stream(reqs, srv)
+        stats = srv.stats
+    assert stats.solved == len(reqs) and stats.batches >= 2
+    for rq, (status, r, lat) in zip(reqs, out):
+        m = rq.mol
+        assert status == 0 and r["converged"]
+        solo = gpu.scf(m.numbers, _abi.angstrom_to_bohr(m.xyz), m.charge, m.multiplicity, want_matrices=False)
+        assert abs(solo["heat_of_formation_kcal"] - r["heat_of_formation_kcal"]) < 1e-9
+        assert np.max(np.abs(solo["charges"] - r["charges"])) < 1e-12
+        assert solo["iterations"] == r["iterations"]
+        assert lat > 0
