@@ -64,16 +64,15 @@ struct DeviceCtx {
     int sms = 0;
     int jacobi_smem = 0;  // dynamic shared memory available to one eigensolver CTA
     int tridiag_smem = 0;  // ... and to one tridiagonalisation CTA
-    int trib_grid = 0;     // CTAs of the grid-wide tridiagonalisation (all co-resident)
-    int sp2b_grid = 0;     // ... and of the grid-wide Lanczos bounds
+    int sp2b_grid = 0;     // CTAs of the grid-wide Lanczos bounds (all co-resident)
 };
 
 // Shared-memory budgets the planner sizes eigensolver and tridiagonalisation clusters for (set
 // when a device is opened).
 int g_jacobi_budget = 232448 - 1024;
 int g_tridiag_budget = 232448 - 1024;
-int g_trib_grid = 148;  // CTAs of the grid-wide tridiagonalisation (set when a device is opened)
-int g_sp2b_grid = 148;  // ... and of the grid-wide Lanczos bounds
+int g_sp2b_grid = 148;  // CTAs of the grid-wide Lanczos bounds (set when a device is opened)
+int g_sms = 148;        // SMs of the current device
 
 // Smallest cluster (1, 2, 4, 8, 16 CTAs) whose row share of an n x n matrix fits one CTA's
 // shared memory; 0 when none does.
@@ -115,9 +114,6 @@ int device_ctx(DeviceCtx** out) {
             return bad("jacobi cluster attribute", err);
         {
             int per_sm = 0;
-            if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_big, TRIB_THREADS, 0)) != cudaSuccess)
-                return bad("grid tridiagonalisation occupancy", err);
-            c.trib_grid = std::max(1, std::min(per_sm, 2)) * c.sms;
             if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sp2_bounds_big, 512, 0)) != cudaSuccess)
                 return bad("grid bounds occupancy", err);
             c.sp2b_grid = std::max(1, std::min(per_sm, 2)) * c.sms;
@@ -135,6 +131,16 @@ int device_ctx(DeviceCtx** out) {
             return bad("tridiag smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
             return bad("tridiag cluster attribute", err);
+        for (const void* f : {(const void*)k_tridiag_cl, (const void*)k_sp2_bounds_cl})
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+                return bad("large-matrix cluster attribute", err);
+        for (const void* f : {(const void*)k_tridiag_cl, (const void*)k_tridiag_big}) {  // 3 n doubles
+            cudaFuncAttributes fb{};
+            if ((err = cudaFuncGetAttributes(&fb, f)) != cudaSuccess) return bad("large tridiagonalisation attributes", err);
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fb.sharedSizeBytes)) !=
+                cudaSuccess)
+                return bad("large tridiagonalisation smem attribute", err);
+        }
         for (const void* f : {(const void*)k_sp2_step16, (const void*)k_sp2_step8, (const void*)k_commutator16,
                               (const void*)k_commutator8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
@@ -143,7 +149,7 @@ int device_ctx(DeviceCtx** out) {
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
     g_tridiag_budget = c.tridiag_smem;
-    g_trib_grid = c.trib_grid;
+    g_sms = c.sms;
     g_sp2b_grid = c.sp2b_grid;
     *out = &c;
     return AM1GPU_OK;
@@ -233,6 +239,30 @@ int density_mode() {
         return (e && std::strcmp(e, "jacobi") == 0) ? 1 : 0;
     }();
     return mode;
+}
+
+// Matrices too large for a cluster's shared memory (tridiagonalisation, Lanczos bounds): one of
+// at least kBigGridN orbitals takes the whole GPU (a cooperative launch each); all the others of
+// the batch get a cluster of big_cluster(count) CTAs each, in one launch.
+// AM1GPU_BIG=grid / cluster forces one form (for measurements).
+constexpr int kBigGridN = 2048;
+
+bool big_on_grid(int n) {
+    static const int force = [] {
+        const char* e = std::getenv("AM1GPU_BIG");
+        if (e && std::strcmp(e, "grid") == 0) return 1;
+        if (e && std::strcmp(e, "cluster") == 0) return 2;
+        return 0;
+    }();
+    if (force) return force == 1;
+    return n >= kBigGridN;
+}
+
+// Cluster size for `count` matrices: about two CTAs of 512 threads per SM in all.
+int big_cluster(int count, int sms) {
+    int C = 16;
+    while (C > 4 && (long long)C * count > 2LL * sms) C /= 2;
+    return C;
 }
 
 struct Run {
@@ -416,8 +446,9 @@ struct Batch {
     struct Bucket { int off, count, C; size_t smem; };
     std::vector<Bucket> buckets;      // eigensolver jobs by cluster size
     std::vector<Bucket> tri_buckets;  // tridiagonalisation jobs by cluster size
-    std::vector<TriJob> tri_big;      // matrices too large for a cluster (grid-wide kernel)
-    std::vector<int> sp2_big;         // purification jobs of those matrices (grid-wide Lanczos)
+    std::vector<TriJob> tri_big;      // matrices too large for a cluster's shared memory (d_tri[0 .. count))
+    std::vector<int> sp2_big;         // purification jobs of those matrices (d_sp2_big), largest first
+    int* d_sp2_big;
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
@@ -502,6 +533,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
     const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
+    const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
     const size_t staged = align256(st);
     // ---- device-only region
@@ -559,6 +591,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_sp2 = (Sp2Job*)dptr(o_sp2);
     b.d_sp2_tiles = (GemmTile*)dptr(o_sp2t);
     b.d_tri = (TriJob*)dptr(o_tri);
+    b.d_sp2_big = (int*)dptr(o_sp2big);
     b.d_need_eigen = (int*)dptr(o_need);
     b.d_sp2_active = (int*)dptr(o_sp2a);
     b.d_work = (double*)dptr(o_work);
@@ -805,6 +838,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         b.tri_buckets.back().count++;
         b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tj.n, C));
     }
+    std::stable_sort(b.sp2_big.begin(), b.sp2_big.end(), [&](int x, int y) { return hsp2[x].n > hsp2[y].n; });
+    std::copy(b.sp2_big.begin(), b.sp2_big.end(), (int*)(Hs + o_sp2big));
     b.mols.assign(hm, hm + b.nmol);
     b.jobs.assign(hj, hj + job);
     b.job0.assign(hj0, hj0 + b.nmol);
@@ -860,6 +895,78 @@ int launch_tridiag(Batch& b, Mem* ws) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         CK(cudaLaunchKernelEx(&cfg, k_tridiag, (const TriJob*)(b.d_tri + bk.off), (const int*)nullptr));
+    }
+    return AM1GPU_OK;
+}
+
+// Matrices on the grid-wide path: the leading ones (sizes n_of(i) descending) of at least kBigGridN
+template <class NOf>
+int big_split(int count, NOf n_of) {
+    int k = 0;
+    while (k < count && big_on_grid(n_of(k))) ++k;
+    return k;
+}
+
+// one launch per grid matrix and one for all the rest
+int big_launches(int grid_count, int count) { return grid_count + (count > grid_count ? 1 : 0); }
+
+cudaError_t launch_clusters(const void* f, int C, int count, int threads, size_t smem, cudaStream_t s, void** args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(C, count, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, f, args);
+}
+
+// Lanczos bounds of the matrices without an eigensolver fallback (b.sp2_big, largest first)
+int launch_big_bounds(Batch& b, cudaStream_t s) {
+    const int count = (int)b.sp2_big.size();
+    if (count == 0) return AM1GPU_OK;
+    const Sp2Job* jobs = b.d_sp2;
+    const MolState* stp = b.d_st;
+    const int k = big_split(count, [&](int i) { return b.jobs[b.sp2_big[i]].n; });
+    for (int i = 0; i < k; ++i) {  // one cooperative launch per matrix
+        int jbig = b.sp2_big[i];
+        void* args[] = {&jobs, &jbig, &stp};
+        CK(cudaLaunchCooperativeKernel((const void*)k_sp2_bounds_big, dim3(g_sp2b_grid), dim3(512), args, 0, s));
+    }
+    if (k < count) {
+        const int* big = b.d_sp2_big + k;
+        void* args[] = {&jobs, &big, &stp};
+        CK(launch_clusters((const void*)k_sp2_bounds_cl, big_cluster(count - k, g_sms), count - k, 512, 0, s, args));
+    }
+    return AM1GPU_OK;
+}
+
+// Householder reduction of the matrices too large for a cluster's shared memory (the first
+// entries of d_tri, largest first)
+int launch_big_tridiag(Batch& b, cudaStream_t s) {
+    const int count = (int)b.tri_big.size();
+    if (count == 0) return AM1GPU_OK;
+    const int k = big_split(count, [&](int i) { return b.tri_big[i].n; });
+    for (int i = 0; i < k; ++i) {  // one cooperative launch per matrix, as many CTAs as fit at once
+        TriJob arg = b.tri_big[i];
+        const size_t smem = tridiag_big_smem_bytes(arg.n);
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_big, TRIB_THREADS, smem));
+        if (per_sm < 1) return fail(AM1GPU_DEVICE_ERROR, "grid tridiagonalisation does not fit an SM");
+        const int grid = std::min(per_sm, 2) * g_sms;
+        void* args[] = {&arg};
+        CK(cudaLaunchCooperativeKernel((const void*)k_tridiag_big, dim3(grid), dim3(TRIB_THREADS), args, smem, s));
+    }
+    if (k < count) {
+        const TriJob* jobs = b.d_tri + k;
+        void* args[] = {&jobs};
+        CK(launch_clusters((const void*)k_tridiag_cl, big_cluster(count - k, g_sms), count - k, TRIB_THREADS,
+                           tridiag_big_smem_bytes(b.tri_big[k].n), s, args));
     }
     return AM1GPU_OK;
 }
@@ -938,16 +1045,13 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
             if (density_mode() == 0) {
                 // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
                 k_sp2_bounds<<<njobs, 512, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
-                for (int jbig : b.sp2_big) {  // one cooperative launch per large matrix
-                    const Sp2Job* jobs = b.d_sp2;
-                    const MolState* stp = b.d_st;
-                    void* args[] = {&jobs, &jbig, &stp};
-                    CK(cudaLaunchCooperativeKernel((const void*)k_sp2_bounds_big, dim3(g_sp2b_grid), dim3(512), args, 0, s));
-                }
+                if ((rc = launch_big_bounds(b, s))) return rc;
                 k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
                 k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
                 CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
-                run.launched(AM1GPU_PHASE_EIGEN, 3);
+                run.launched(AM1GPU_PHASE_EIGEN,
+                             3 + big_launches(big_split((int)b.sp2_big.size(), [&](int i) { return b.jobs[b.sp2_big[i]].n; }),
+                                              (int)b.sp2_big.size()));
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
@@ -1012,15 +1116,13 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
     // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
     if ((rc = launch_tridiag(b, ws))) return rc;
-    for (const TriJob& tj : b.tri_big) {  // one cooperative launch per large matrix
-        TriJob arg = tj;
-        void* args[] = {&arg};
-        CK(cudaLaunchCooperativeKernel((const void*)k_tridiag_big, dim3(g_trib_grid), dim3(TRIB_THREADS), args, 0, s));
-    }
+    if ((rc = launch_big_tridiag(b, s))) return rc;
     k_bisect<<<dim3(njobs, cdiv(b.maxn, 512)), 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
-    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() + (int)b.tri_big.size());
+    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() +
+                                         big_launches(big_split((int)b.tri_big.size(), [&](int i) { return b.tri_big[i].n; }),
+                                                      (int)b.tri_big.size()));
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;

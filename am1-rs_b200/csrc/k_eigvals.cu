@@ -205,29 +205,41 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
     csync();  // no CTA leaves while another may still address its shared memory
 }
 
-// Householder reduction of one matrix too large for a cluster's shared memory (n > ~448), by the
-// whole GPU in one cooperative launch: the matrix is copied to W (global memory, row-major), row r
-// belongs to CTA r % G, and every step takes two grid barriers.  Step s, as in k_tridiag:
+// Householder reduction of one matrix too large for a cluster's shared memory (n > ~448), by a
+// group of G CTAs: the whole GPU (one cooperative launch per matrix) or a thread-block cluster
+// (one cluster per matrix, all such matrices of a batch in one launch).  The matrix is copied to
+// W (global memory, row-major), row r belongs to CTA r % G, and every step takes two group
+// barriers.  Step s, as in k_tridiag:
+//   every CTA stages v_{s-1} and w_{s-1} = p_{s-1} - kk_{s-1} v_{s-1} (columns >= s) in shared
+//   memory
 //   (a) the CTA owning row s applies update s-1 to it (all its threads, a column each) and derives
 //       reflector s (a block reduction for the norm): v_s into global scratch, beta_s, d[s], e[s]
-//   grid barrier
+//   group barrier; every CTA stages v_s
 //   (b) every CTA, a warp per own row r > s: apply update s-1 to row r (columns > s) and form
-//       p_r = beta_s W[r, s+1:] . v_s in the same pass; the CTA's share of p.v
-//   grid barrier
-//   every CTA sums the G shares in the same order, so all hold the same kk_s = beta_s (p.v) / 2;
-//   w_s = p_s - kk_s v_s is never stored, only formed where it is used.
-// Scratch (job.work): v[2][n] | p[2][n] | share[G] | beta[2].
-__global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
-    cg::grid_group grid = cg::this_grid();
-    const int G = (int)gridDim.x, gi = (int)blockIdx.x;
+//       p_r = beta_s W[r, s+1:] . v_s in the same pass; the CTA's share of p.v.  Each lane loads
+//       TRIB_BATCH elements of the row before it stores any, so that many loads are in flight.
+//   group barrier
+//   every warp sums the G shares in the same order, so all hold the same kk_s = beta_s (p.v) / 2.
+// Global scratch (job.work): v[2][n] | p[2][n] | share[G] | beta[2]; dynamic shared memory: 3 n
+// doubles (tridiag_big_smem_bytes).
+constexpr int TRIB_BATCH = 8;
+
+size_t tridiag_big_smem_bytes(int n) { return sizeof(double) * 3 * (size_t)n; }
+
+template <class Sync>
+__device__ void tridiag_group(const TriJob& jb, int G, int gi, Sync sync) {
     const int n = jb.n;
     double* W = jb.W;
     double* vb = jb.work;              // v_s, two buffers
     double* pb = vb + 2 * (size_t)n;   // p_s, two buffers
     double* share = pb + 2 * (size_t)n;
     double* bb = share + G;            // beta_s, two buffers
+    extern __shared__ double tsh[];
+    double* sv = tsh;           // v_{s-1}
+    double* sw = tsh + n;       // w_{s-1}
+    double* svn = tsh + 2 * n;  // v_s
     constexpr int NW = TRIB_THREADS / 32;
-    __shared__ double red[NW + 1];
+    __shared__ double red[NW];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     auto bsum = [&](double v) {
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
         pb[n + c] = 0.0;
     }
     double kk = 0.0;
-    grid.sync();
+    sync();
     for (int s = 0; s + 1 < n; ++s) {
         const int cur = (s + 1) & 1, nxt = s & 1;
         const double* v = vb + (size_t)cur * n;  // reflector s - 1
@@ -254,13 +266,19 @@ __global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
         double* vn = vb + (size_t)nxt * n;       // reflector s
         double* pn = pb + (size_t)nxt * n;
         const bool has_next = s + 2 < n;
+        for (int c = s + tid; c < n; c += TRIB_THREADS) {
+            const double vc = __ldcg(v + c);
+            sv[c] = vc;
+            sw[c] = __ldcg(p + c) - kk * vc;
+        }
+        __syncthreads();
         if (gi == s % G) {  // (a)
             double* row = W + (size_t)s * n;
-            const double vs = __ldcg(v + s), ws = __ldcg(p + s) - kk * vs;
+            const double vs = sv[s], ws = sw[s];
             double nrm = 0.0;
             for (int c = s + tid; c < n; c += TRIB_THREADS) {
-                const double vc = __ldcg(v + c);
-                const double y = row[c] - vs * (__ldcg(p + c) - kk * vc) - ws * vc;
+                const double vc = sv[c];
+                const double y = row[c] - vs * sw[c] - ws * vc;
                 row[c] = y;
                 if (c > s) {
                     vn[c] = y;
@@ -281,43 +299,59 @@ __global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
                 }
             }
         }
-        grid.sync();  // v_s and beta_s ready
+        sync();  // v_s and beta_s ready
+        for (int c = s + 1 + tid; c < n; c += TRIB_THREADS) svn[c] = __ldcg(vn + c);
+        __syncthreads();
         // (b) own rows r > s, a warp per row
         const double beta = has_next ? __ldcg(bb + nxt) : 0.0;
         double part = 0.0;
         const int r0 = s + 1 + ((gi - (s + 1) % G) % G + G) % G;  // first own row > s
         for (int r = r0 + warp * G; r < n; r += NW * G) {
             double* row = W + (size_t)r * n;
-            const double vr = __ldcg(v + r), wr = __ldcg(p + r) - kk * vr;
+            const double vr = sv[r], wr = sw[r];
             double acc = 0.0;
-#pragma unroll 4
-            for (int c = s + 1 + lane; c < n; c += 32) {
-                const double vc = __ldcg(v + c);
-                const double y = row[c] - vr * (__ldcg(p + c) - kk * vc) - wr * vc;
-                row[c] = y;
-                acc = fma(y, __ldcg(vn + c), acc);
+            for (int c0 = s + 1 + lane; c0 < n; c0 += 32 * TRIB_BATCH) {
+                double x[TRIB_BATCH];
+#pragma unroll
+                for (int u = 0; u < TRIB_BATCH; ++u) {
+                    const int c = c0 + 32 * u;
+                    x[u] = c < n ? row[c] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < TRIB_BATCH; ++u) {
+                    const int c = c0 + 32 * u;
+                    if (c < n) {
+                        const double y = x[u] - vr * sw[c] - wr * sv[c];
+                        row[c] = y;
+                        acc = fma(y, svn[c], acc);
+                    }
+                }
             }
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             const double pr = beta * acc;
             if (lane == 0 && has_next) pn[r] = pr;
-            part += pr * __ldcg(vn + r);
+            part += pr * svn[r];
         }
         if (!has_next) break;
         part = bsum(lane == 0 ? part : 0.0);
         if (tid == 0) share[gi] = part;
-        grid.sync();  // p_s and every share ready
-        if (tid == 0) {
-            double pv = 0.0;
-            for (int q = 0; q < G; ++q) pv += __ldcg(share + q);
-            red[NW] = 0.5 * beta * pv;
-        }
-        __syncthreads();
-        kk = red[NW];
-        __syncthreads();
+        sync();  // p_s and every share ready
+        kk = 0.5 * beta * group_share_sum(share, G);
     }
     __syncthreads();
     if (n == 1 && gi == 0 && tid == 0) jb.d[0] = W[0];
     if (n >= 2 && gi == (n - 1) % G && tid == 0) jb.d[n - 1] = W[(size_t)(n - 1) * n + n - 1];
+}
+
+__global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_big(TriJob jb) {
+    cg::grid_group grid = cg::this_grid();
+    tridiag_group(jb, (int)gridDim.x, (int)blockIdx.x, [&] { grid.sync(); });
+}
+
+// One cluster (gridDim.x CTAs) per matrix of jobs[blockIdx.y].
+__global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_cl(const TriJob* __restrict__ jobs) {
+    cg::cluster_group cl = cg::this_cluster();
+    tridiag_group(jobs[blockIdx.y], (int)cl.num_blocks(), (int)cl.block_rank(), [&] { cl.sync(); });
 }
 
 // Number of eigenvalues of T below x: the sign changes of the leading principal minors

@@ -242,16 +242,14 @@ __device__ void lz_interval(const double* alpha, const double* beta, int m, doub
 }
 
 // k_sp2_bounds for one matrix too large for one CTA (no eigensolver fallback, n > ~448): the same
-// Lanczos run by the whole GPU in one cooperative launch.  Row r of F* belongs to CTA r % G; the
-// vectors live in global scratch (job.X1, free until purification starts) and every CTA keeps the
-// same alpha, beta (sums of the per-CTA shares in one fixed order).  Three grid barriers per step.
-// Cross-CTA data is read through L2 (__ldcg).  Scratch: q[3][n] | share[2][G].
-__global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2Job* __restrict__ jobs, int job,
-                                                                       const MolState* __restrict__ st) {
-    cg::grid_group grid = cg::this_grid();
-    const Sp2Job jb = jobs[job];
-    if (!st[jb.mol].active) return;  // uniform over the grid
-    const int G = (int)gridDim.x, gi = (int)blockIdx.x;
+// Lanczos run by a group of G CTAs, either the whole GPU (one cooperative launch per matrix) or a
+// thread-block cluster (one cluster per matrix, all such matrices of a batch in one launch).
+// Row r of F* belongs to CTA r % G; the vectors live in global scratch (job.X1, free until
+// purification starts) and every CTA keeps the same alpha, beta (sums of the per-CTA shares in one
+// fixed order).  Three group barriers per step; cross-CTA data is read through L2 (__ldcg).
+// Scratch: q[3][n] | share[2][G].
+template <class Sync>
+__device__ void sp2_bounds_group(const Sp2Job& jb, int G, int gi, Sync sync) {
     const int n = jb.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = SP2_BOUND_THREADS / 32;
@@ -298,7 +296,7 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2J
         qb[i] = (cos(0.7 * i + 0.3) + 0.5) * inq;  // q_0
         qb[2 * (size_t)n + i] = 0.0;            // q_{-1}
     }
-    grid.sync();
+    sync();
     const int K = min(SP2_LANCZOS, n);
     int m = 0, cur = 0, prv = 2;
     double bprev = 0.0;
@@ -320,9 +318,8 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2J
         }
         part = bsum(lane == 0 ? part : 0.0);
         if (tid == 0) share[gi] = part;
-        grid.sync();
-        double a = 0.0;
-        for (int g = 0; g < G; ++g) a += __ldcg(share + g);
+        sync();
+        const double a = group_share_sum(share, G);
         // w <- w - a q - b_prev q_prev on own rows, the CTA's share of |w|^2
         part = 0.0;
         for (int r = gi + warp * G; r < n; r += NW * G) {
@@ -334,10 +331,8 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2J
         }
         part = bsum(part);
         if (tid == 0) share[G + gi] = part;
-        grid.sync();
-        double b2 = 0.0;
-        for (int g = 0; g < G; ++g) b2 += __ldcg(share + G + g);
-        const double bnorm = sqrt(b2);
+        sync();
+        const double bnorm = sqrt(group_share_sum(share + G, G));
         if (tid == 0) {
             alpha[j] = a;
             beta[j] = bnorm;
@@ -350,10 +345,28 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2J
         bprev = bnorm;
         prv = cur;
         cur = nxt;
-        grid.sync();
+        sync();
     }
     __syncthreads();
     if (gi == 0 && tid == 0) lz_interval(alpha, beta, m, glo, ghi, jb.bounds);
+}
+
+__global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_big(const Sp2Job* __restrict__ jobs, int job,
+                                                                       const MolState* __restrict__ st) {
+    cg::grid_group grid = cg::this_grid();
+    const Sp2Job jb = jobs[job];
+    if (!st[jb.mol].active) return;  // uniform over the grid
+    sp2_bounds_group(jb, (int)gridDim.x, (int)blockIdx.x, [&] { grid.sync(); });
+}
+
+// One cluster (gridDim.x CTAs) per large matrix; blockIdx.y indexes big[], the purification jobs
+// without the eigensolver fallback.
+__global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds_cl(const Sp2Job* __restrict__ jobs, const int* __restrict__ big,
+                                                                      const MolState* __restrict__ st) {
+    cg::cluster_group cl = cg::this_cluster();
+    const Sp2Job jb = jobs[big[blockIdx.y]];
+    if (!st[jb.mol].active) return;  // uniform over the cluster
+    sp2_bounds_group(jb, (int)cl.num_blocks(), (int)cl.block_rank(), [&] { cl.sync(); });
 }
 
 // X0 = (e_max I - F*) / (e_max - e_min); per-block partial sums of tr X0 and ||X0||_F^2.

@@ -112,9 +112,11 @@ __global__ void k_gemm_tn(const GemmJob* jobs, const GemmTile* tiles, int ntiles
 __global__ void k_jacobi(const EigJob* jobs, const MolState* st, int* mol_status, int force, const int* mask);
 __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, const int* mask);
 // one CTA of 512 threads per job, 3 n doubles of dynamic shared memory; jobs without an eigensolver
-// fallback (large matrices) are left to k_sp2_bounds_big, one cooperative launch each
+// fallback (large matrices) are left to k_sp2_bounds_big (one cooperative launch per matrix) or
+// k_sp2_bounds_cl (a cluster per matrix, grid (C, count of big), blockIdx.y indexes big[])
 __global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
 __global__ void k_sp2_bounds_big(const Sp2Job* jobs, int job, const MolState* st);
+__global__ void k_sp2_bounds_cl(const Sp2Job* jobs, const int* big, const MolState* st);
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 // *16: every matrix of the tile list has even n and 16-byte aligned rows (16-byte copies);
@@ -133,11 +135,29 @@ __global__ void k_tridiag(const TriJob* jobs, const int* mask);
 size_t tridiag_smem_bytes(int n, int C);
 // a thread per eigenvalue; blockIdx.y selects the block of 512 eigenvalue indices (large n)
 __global__ void k_bisect(const TriJob* jobs, const int* mask);
-// matrices too large for a cluster's shared memory: one cooperative launch over the whole GPU
-// (grid <= co-resident CTAs of TRIB_THREADS threads), the matrix in global memory
+// matrices too large for a cluster's shared memory, the matrix in global memory: one cooperative
+// launch over the whole GPU (grid <= co-resident CTAs of TRIB_THREADS threads), or a cluster of
+// C CTAs per matrix (grid (C, count), blockIdx.y indexes jobs); tridiag_big_smem_bytes(largest n)
+// of dynamic shared memory
 constexpr int TRIB_THREADS = 512;
 __global__ void k_tridiag_big(TriJob job);
+__global__ void k_tridiag_cl(const TriJob* jobs);
+size_t tridiag_big_smem_bytes(int n);
 size_t jacobi_smem_bytes(int n, int npad, int C);
+
+#ifdef __CUDACC__
+// Sum of the G per-CTA shares of a multi-CTA reduction, the same in every warp of every CTA: lane
+// l adds shares l, l+32, ... in that order, then a butterfly over the lanes (every lane ends with
+// the same sum: each level adds the same two partial sums, and addition commutes exactly).  All
+// loads are in flight at once, so the cost is one L2 round trip whatever G is.
+__device__ __forceinline__ double group_share_sum(const double* share, int G) {
+    const int lane = threadIdx.x & 31;
+    double t = 0.0;
+    for (int g = lane; g < G; g += 32) t += __ldcg(share + g);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return t;
+}
+#endif
 
 __global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                            const int* atom_z, double* arena);

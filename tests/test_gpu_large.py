@@ -66,3 +66,34 @@ def test_config4_full_size(gpu):
     b = gpu.scf(m.numbers, xyz, want_matrices=False)  # deterministic: no atomics in any sum
     assert b["heat_of_formation_kcal"] == a["heat_of_formation_kcal"]
     assert np.array_equal(b["mo_energies"], a["mo_energies"])
+
+
+def test_batch_of_large_molecules_matches_oracle(gpu, oracle):
+    # several matrices past the cluster eigensolver in one batch: one launch of a cluster per
+    # matrix for the Lanczos bounds and the tridiagonalisation, beside small molecules
+    from am1gpu import workloads as W, _abi
+
+    big = [_water(k, 100 + k) for k in (76, 84)]
+    rng = np.random.default_rng(5)
+    small = [W.alkane(3, rng), W.water_cluster(4, rng)]
+    mols = [(z, x, 0.0, 1) for z, x in big] + [(m.numbers, _abi.angstrom_to_bohr(m.xyz), 0.0, 1) for m in small]
+    status, res = gpu.scf_batch(mols, want_matrices=False)
+    assert all(s == 0 for s in status), status
+    for (z, x, _, _), g in zip(mols, res):
+        o = oracle.scf(z, x, want_matrices=False)
+        assert abs(g["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < 1e-6
+        assert np.max(np.abs(g["charges"] - o["charges"])) < 1e-7
+        assert np.max(np.abs(g["mo_energies"] - o["mo_energies"])) < 1e-7
+
+
+def test_many_large_molecules_match_solo(gpu):
+    # 40 matrices of 450-480 orbitals: small clusters per matrix in the batch, a 16-CTA cluster
+    # alone; the two summation orders agree to rounding
+    mols = [(*_water(75 + i % 6, 300 + i), 0.0, 1) for i in range(40)]
+    status, res = gpu.scf_batch(mols, want_matrices=False)
+    assert all(s == 0 for s in status), status
+    for m, g in zip(mols, res):
+        solo = gpu.scf(*m, want_matrices=False)
+        assert solo["iterations"] == g["iterations"]
+        assert abs(solo["heat_of_formation_kcal"] - g["heat_of_formation_kcal"]) < 1e-8
+        assert np.max(np.abs(solo["mo_energies"] - g["mo_energies"])) < 1e-9
