@@ -120,6 +120,8 @@ class CallStats(ctypes.Structure):
         ("purification_steps", ctypes.c_double),
         ("purification_flops", ctypes.c_double),
         ("purification_bytes", ctypes.c_double),
+        ("lowp_purification_steps", ctypes.c_double),
+        ("lowp_purification_flops", ctypes.c_double),
     ]
 
 
@@ -169,6 +171,8 @@ def stats_dict(st: CallStats) -> dict:
         "purification_steps": float(st.purification_steps),
         "purification_flops": float(st.purification_flops),
         "purification_bytes": float(st.purification_bytes),
+        "lowp_purification_steps": float(st.lowp_purification_steps),
+        "lowp_purification_flops": float(st.lowp_purification_flops),
     }
 
 _lib = None

@@ -74,6 +74,9 @@ struct MolState {
     int hist_head;     // physical slot of the oldest entry
     int mode;          // extrapolation of this iteration: 0 plain F, 1 combine history
     int accel_used;    // 0 none, 1 CDIIS, 2 ADIIS (diagnostic)
+    int lowp;          // mixed precision: 1 while this molecule's purification runs in TF32
+    int lowp_end;      // iteration at which the TF32 phase ended (convergence is tested only after it)
+    int lowp_flush;    // 1 in the first FP64 iteration: its history entry still holds the TF32 density
     double e_old, e_elec, err_norm, dp, residual;
     double coeff[MAX_DIIS];            // combination coefficients in logical order
     double bmat[MAX_DIIS * MAX_DIIS];  // CDIIS Gram <e_i, e_j>, logical order

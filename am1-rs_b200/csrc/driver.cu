@@ -145,6 +145,9 @@ int device_ctx(DeviceCtx** out) {
                               (const void*)k_commutator8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
                 return bad("tile kernel smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_sp2_step_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf32_smem_bytes())) !=
+            cudaSuccess)
+            return bad("tf32 tile kernel smem attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
@@ -230,6 +233,30 @@ bool timing_on() {
 thread_local am1gpu_call_stats tl_stats;
 
 constexpr int kSp2MaxSteps = 100;
+constexpr int kWorkN = 8;  // device counters of a run (Batch::d_work)
+
+// Mixed precision: a molecule's TF32 phase ends when its RMS density change falls below
+// kLowpSwitch (about where TF32 purification stops improving the density), or after
+// kLowpMaxIter iterations.
+// AM1GPU_LOWP_SWITCH / AM1GPU_LOWP_MAXIT override them (for tuning).
+constexpr double kLowpSwitch = 1e-3;
+constexpr int kLowpMaxIter = 12;
+
+double lowp_switch() {
+    static const double v = [] {
+        const char* e = std::getenv("AM1GPU_LOWP_SWITCH");
+        return e && *e ? std::atof(e) : kLowpSwitch;
+    }();
+    return v;
+}
+
+int lowp_max_iter() {
+    static const int v = [] {
+        const char* e = std::getenv("AM1GPU_LOWP_MAXIT");
+        return e && *e ? std::atoi(e) : kLowpMaxIter;
+    }();
+    return v;
+}
 
 // How the SCF step forms P from F*: 0 purification (default), 1 eigenvectors every iteration.
 // AM1GPU_DENSITY=jacobi selects the eigensolver path (kept for comparison and testing).
@@ -318,6 +345,10 @@ struct MolPlan {
     std::vector<int> order;  // internal atom -> caller atom
     std::vector<int> ao_map; // internal AO -> caller AO
 };
+
+// Rows of a channel's VS slot (n doubles each): the eigensolver's npad vectors, and room for the
+// mixed path's two FP32 iterates of n rows of (n rounded up to 4) floats plus 16-byte alignment.
+long long vs_rows(const MolPlan& p) { return std::max<long long>(p.npad, ((p.nao + 3) & ~3) + 2); }
 
 // Largest molecule (orbitals) the purification path takes: the Lanczos bounds and the bisection hold
 // 3 n and 2 n doubles in one CTA's shared memory.
@@ -456,7 +487,8 @@ struct Batch {
     TriJob* d_tri;
     int* d_need_eigen;
     int* d_sp2_active;
-    double* d_work;  // [0] purification steps, [1] their flops, [2] eigensolver fallbacks, [3] their bytes
+    double* d_work;  // [0] purification steps, [1] their flops, [2] eigensolver fallbacks, [3] their bytes,
+                     // [4] TF32 purification steps, [5] their flops
     MolState* d_st;
     int* d_status;
     double *d_wstore, *d_ecc, *d_arena, *d_res, *d_charges;
@@ -491,7 +523,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         const long long h = p.nheavy, H = p.natoms - p.nheavy;
         wsize += 100 * h * (h - 1) / 2 + 10 * h * H + H * (H - 1) / 2;
         const long long nn = (long long)p.nao * p.nao;
-        arena += nn + p.nch * (5 * nn + (long long)p.npad * p.nao) + 64;
+        arena += nn + p.nch * (5 * nn + (long long)vs_rows(p) * p.nao) + 64;
         const long long ls = packed_sym_len(p.nao), la = packed_anti_len(p.nao);
         hist += p.nch * MAX_DIIS * (ls + la + ((adiis && p.nch == 1) ? ls : 0)) + 64;
         nch_total += p.nch;
@@ -541,7 +573,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_status = take(dv, sizeof(int) * b.nmol);
     const size_t o_need = take(dv, sizeof(int) * b.nmol);
     const size_t o_sp2a = take(dv, sizeof(int) * 4);
-    const size_t o_work = take(dv, sizeof(double) * 4);
+    const size_t o_work = take(dv, sizeof(double) * kWorkN);
     const size_t o_sp2s = take(dv, sizeof(Sp2State) * nch_total);
     const size_t o_active = take(dv, sizeof(int) * 4);
     const size_t o_w = take(dv, sizeof(double) * std::max<long long>(wsize, 1));
@@ -566,7 +598,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     // pinned staging also receives the outputs
     size_t hs = staged;
     const size_t h_o_active = take(hs, sizeof(int) * 4);
-    const size_t h_o_work = take(hs, sizeof(double) * 4);
+    const size_t h_o_work = take(hs, sizeof(double) * kWorkN);
     const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
     const size_t h_o_eps = take(hs, sizeof(double) * std::max<long long>(eps_total, 1));
@@ -661,7 +693,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         long long cur = ar_off + nn;
         for (int c = 0; c < p.nch; ++c) {
             md.ch_base[c] = cur;
-            cur += 5 * nn + (long long)p.npad * n;
+            cur += 5 * nn + (long long)vs_rows(p) * n;
         }
         ar_off = (cur + 31) & ~31LL;
         for (int ia = 0; ia < p.natoms; ++ia) {
@@ -744,6 +776,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             const bool pairs = n % 2 == 0 && aligned16(sj.X0) && aligned16(sj.X1) && aligned16(cj.F) && aligned16(cj.P);
             std::vector<GemmTile>& tl = pairs ? tiles_pairs : tiles_other;
             sj.fallback = p.cluster > 0;
+            sj.ldf = (int)((n + 3) & ~3LL);  // FP32 iterates of the mixed path: in the VS slot, 16-byte aligned
+            sj.Xf0 = (float*)(((uintptr_t)(base + SLOT_VS * nn) + 15) & ~(uintptr_t)15);
+            sj.Xf1 = sj.Xf0 + n * sj.ldf;
             if (!sj.fallback) b.sp2_big.push_back(job);
             sj.tile0 = (int)tl.size();  // tile index inside its own launch
             for (int x = 0; x < (int)tn_; ++x)
@@ -1003,9 +1038,12 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.event(&t0))) return rc;
     if ((rc = run.begin(&ph))) return rc;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, s));
-    CK(cudaMemsetAsync(b.d_work, 0, sizeof(double) * 4, s));
+    CK(cudaMemsetAsync(b.d_work, 0, sizeof(double) * kWorkN, s));
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * b.arena_doubles, s));
-    k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.nmol);
+    // mixed precision: every molecule starts with TF32 purification (k_converge ends that phase)
+    const bool mixed = o.precision == AM1GPU_PRECISION_MIXED && density_mode() == 0;
+    bool lowp_left = mixed;  // some molecule may still be in its TF32 phase
+    k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.nmol, mixed ? 1 : 0);
     run.launched(AM1GPU_PHASE_CORE);
     rc = launch_core(b, ws, dp, &run);
     if (rc) return rc;
@@ -1018,14 +1056,14 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     run.launched(AM1GPU_PHASE_CORE);
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_CORE, ph))) return rc;
-    ScfParams prm{o.max_scf, o.use_diis, o.accelerator, o.e_tol, o.p_tol, o.adiis_switch};
+    ScfParams prm{o.max_scf, o.use_diis, o.accelerator, o.e_tol, o.p_tol, o.adiis_switch, lowp_switch(), lowp_max_iter()};
     const int nblk = b.nblk;
     const int rowblk = std::max(1, std::min(64, (b.maxn + 7) / 8));
     int done = 0;
     const int check = b.nmol > 64 ? 4 : 1;
     while (done < o.max_scf) {
         for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
-            CK(cudaMemsetAsync(b.d_active, 0, sizeof(int), s));
+            CK(cudaMemsetAsync(b.d_active, 0, 2 * sizeof(int), s));
             if ((rc = run.begin(&ph))) return rc;
             k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena,
                                                       b.d_st, 0);
@@ -1055,11 +1093,23 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
-                    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-                        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                    });
-                    run.launched(AM1GPU_PHASE_DENSITY_CORE);
+                    // FP64 steps (none in the first iteration of the mixed path: every molecule is
+                    // in its TF32 phase), then the TF32 steps while any molecule may be in it
+                    int nl = 0;
+                    if (!(mixed && done == 0)) {
+                        launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+                            if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                            else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                            ++nl;
+                        });
+                    }
+                    if (lowp_left) {
+                        launch_tiles(b, s, [&](const GemmTile* t, int nt, bool) {
+                            k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                            ++nl;
+                        });
+                    }
+                    run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
                     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
                     CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
                     k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, kSp2MaxSteps, b.d_sp2_active,
@@ -1105,8 +1155,10 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
             CK(cudaGetLastError());
         }
         CK(cudaMemcpyAsync(b.h_active, b.d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (lowp_left) CK(cudaMemcpyAsync(b.h_active + 2, b.d_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         if (*b.h_active == 0) break;
+        if (lowp_left && b.h_active[2] == 0) lowp_left = false;  // no molecule returns to TF32
     }
     stats->scf_cycles = done;
     // final energy at the final density (src/scf.rs:698-701, 835-839) and the result records
@@ -1127,12 +1179,14 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;
     if ((rc = run.event(&t1))) return rc;
-    CK(cudaMemcpyAsync(b.h_work, b.d_work, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(b.h_work, b.d_work, sizeof(double) * kWorkN, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     stats->purification_steps += b.h_work[0];
     stats->purification_flops += b.h_work[1];
     stats->purification_bytes += b.h_work[3];
     stats->eigen_fallbacks += (int32_t)b.h_work[2];
+    stats->lowp_purification_steps += b.h_work[4];
+    stats->lowp_purification_flops += b.h_work[5];
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, mem.events[t0], mem.events[t1]));
     stats->device_ms += ms;
@@ -1571,7 +1625,9 @@ int am1gpu_basis_size(int32_t natoms, const int32_t* z, int32_t method, int32_t*
 int am1gpu_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res) {
     if (!mol || !opts || !res) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
     int32_t st = 0;
-    return am1::scf_batch(1, mol, opts, res, &st);
+    am1gpu_options o = *opts;
+    o.precision = AM1GPU_PRECISION_FP64;  // the plain path is FP64 throughout
+    return am1::scf_batch(1, mol, &o, res, &st);
 }
 
 int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* results,

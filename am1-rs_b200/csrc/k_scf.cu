@@ -54,11 +54,12 @@ __global__ void k_sad_init(const MolDesc* __restrict__ mols, const int* __restri
 }
 
 // Fresh SCF state for every molecule of a batch (each run starts from the SAD guess).
-__global__ void k_state_init(MolState* __restrict__ st, int nmol) {
+__global__ void k_state_init(MolState* __restrict__ st, int nmol, int lowp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nmol) return;
     MolState s{};
     s.active = 1;
+    s.lowp = lowp;
     s.residual = __longlong_as_double(0x7ff0000000000000LL);  // +inf
     st[i] = s;
 }
@@ -496,13 +497,33 @@ __global__ void k_converge(const MolDesc* __restrict__ mols, const ChanJob* __re
     s.residual = s.err_norm;
     const int it = s.iter;
     s.iter = it + 1;
-    if (it > 0 && de < prm.e_tol && (dp < prm.p_tol || s.err_norm < 1.0e-7)) {
+    if (s.lowp) {
+        // mixed precision: this iteration's density came from TF32 purification, so no
+        // convergence is declared on it; the TF32 phase ends once the density has settled near its
+        // rounding level, and the FP64 iterations that follow take the SCF to convergence
+        if ((it > 0 && dp < prm.lowp_switch) || s.iter >= prm.lowp_max_iter) {
+            s.lowp = 0;
+            s.lowp_end = it;
+            s.lowp_flush = 1;
+        }
+        if (s.iter >= prm.max_scf) s.active = 0;
+    } else if (s.lowp_flush) {
+        // first FP64 iteration: its Fock matrix was built from the last TF32 density.  The
+        // history restarts after it, so the extrapolation (A-DIIS in particular, whose energy
+        // model would favour that slightly non-idempotent density) sees FP64 iterations only.
+        s.lowp_flush = 0;
+        s.hist_count = 0;
+        if (s.iter >= prm.max_scf) s.active = 0;
+    } else if (it > s.lowp_end && it > 0 && de < prm.e_tol && (dp < prm.p_tol || s.err_norm < 1.0e-7)) {
         s.converged = 1;
         s.active = 0;
     } else if (s.iter >= prm.max_scf) {
         s.active = 0;
     }
-    if (s.active) atomicAdd(active_count, 1);
+    if (s.active) {
+        atomicAdd(active_count, 1);
+        if (s.lowp) atomicAdd(active_count + 1, 1);
+    }
 }
 
 __global__ void k_final_energy(const MolDesc* __restrict__ mols, const ChanJob* __restrict__ jobs, const int* __restrict__ mol_job0,

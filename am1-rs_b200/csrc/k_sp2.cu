@@ -378,9 +378,21 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
     __shared__ double red[2][32];
     const double emin = jb.bounds[0], emax = jb.bounds[1];  // from k_sp2_bounds
     const double inv = 1.0 / fmax(emax - emin, 1e-300);
+    const bool lowp = st[jb.mol].lowp;
     double tr = 0.0, fr = 0.0;
     for (int r = blockIdx.x * nw + warp; r < n; r += nblk * nw) {
         const double* Fr = jb.F + (long long)r * n;
+        if (lowp) {  // FP32 iterate (rows of ldf floats, pad columns zero in both buffers)
+            float* Xr = jb.Xf0 + (long long)r * jb.ldf;
+            for (int c = lane; c < jb.ldf; c += 32) {
+                const float x = c < n ? tf32_round((float)(((c == r ? emax : 0.0) - Fr[c]) * inv)) : 0.0f;
+                Xr[c] = x;
+                if (c >= n) jb.Xf1[(long long)r * jb.ldf + c] = 0.0f;
+                fr += (double)x * x;
+                if (c == r) tr += x;
+            }
+            continue;
+        }
         double* Xr = jb.X0 + (long long)r * n;
         for (int c = lane; c < n; c += 32) {
             const double x = ((c == r ? emax : 0.0) - Fr[c]) * inv;
@@ -422,6 +434,7 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
     const Sp2Job jb = jobs[j];
     Sp2State& s = sst[j];
     s.active = st[jb.mol].active;
+    s.lowp = st[jb.mol].lowp;
     s.steps = 0;
     s.cur = 0;
     s.converged = 0;
@@ -446,7 +459,7 @@ __device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, c
     if (t >= ntiles) return;
     const GemmTile tl = tiles[t];
     const Sp2State* sp = sst + tl.job;
-    if (!sp->active) return;
+    if (!sp->active || sp->lowp) return;  // TF32 runs: k_sp2_step_tf32
     const Sp2Job* jp = jobs + tl.job;
     const int n = jp->n;
     const int cur = sp->cur;
@@ -509,9 +522,14 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
     if (!s.active) return;
     const Sp2Job jb = jobs[j];
     // algorithmic work of the product just taken: a symmetric X.X, n^3 flops
-    atomicAdd(&work[0], 1.0);
-    atomicAdd(&work[1], (double)jb.n * jb.n * jb.n);
-    atomicAdd(&work[3], 16.0 * jb.n * jb.n);  // read X, write X^2 (both triangles), FP64
+    if (s.lowp) {
+        atomicAdd(&work[4], 1.0);
+        atomicAdd(&work[5], (double)jb.n * jb.n * jb.n);
+    } else {
+        atomicAdd(&work[0], 1.0);
+        atomicAdd(&work[1], (double)jb.n * jb.n * jb.n);
+        atomicAdd(&work[3], 16.0 * jb.n * jb.n);  // read X, write X^2 (both triangles), FP64
+    }
     double tr = 0.0, fr = 0.0;
     for (int t = 0; t < jb.ntiles; ++t) {
         tr += jb.part[2 * t];
@@ -524,16 +542,19 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
     // idempotency error tr X - tr X^2 (sum of x(1-x) over the spectrum, >= 0)
     const double idem = fabs(tr - fr);
     const bool floor_reached = idem < 1.0e-6 && idem >= s.idem[0];  // stagnation at the rounding floor
+    // TF32 runs stop at their own rounding level (about 1e-6 relative per eigenvalue), and their
+    // result is always taken: it only starts the FP64 iterations
+    const bool low_done = s.lowp && ((idem < 1.0e-2 * jb.n && idem >= s.idem[0]) || idem < 1.0e-5 * jb.n);
     s.idem[0] = s.idem[1];
     s.idem[1] = idem;
-    if (floor_reached || idem < 1.0e-15 * fmax(1.0, (double)jb.n)) {
+    if (low_done || floor_reached || idem < 1.0e-15 * fmax(1.0, (double)jb.n)) {
         s.active = 0;
         s.converged = 1;
         return;
     }
     if (s.steps >= max_steps) {
         s.active = 0;
-        s.converged = 0;
+        s.converged = s.lowp;
         return;
     }
     s.square = fabs(fr - jb.nocc) < fabs(2.0 * tr - fr - jb.nocc) ? 1 : 0;
@@ -558,8 +579,18 @@ __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __
         }
         return;
     }
-    const double* X = s.cur ? jb.X1 : jb.X0;
     const long long nn = (long long)jb.n * jb.n;
+    if (s.lowp) {
+        // the TF32 iterate, rescaled to the exact electron count (its trace is off by the rounding)
+        const float* Xf = s.cur ? jb.Xf1 : jb.Xf0;
+        const double w = jb.weight * (s.trX > 0.0 ? jb.nocc / s.trX : 1.0);
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x) {
+            const long long r = i / jb.n, c = i - r * jb.n;
+            jb.P[i] = w * (double)Xf[r * jb.ldf + c];
+        }
+        return;
+    }
+    const double* X = s.cur ? jb.X1 : jb.X0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x)
         jb.P[i] = jb.weight * X[i];
 }

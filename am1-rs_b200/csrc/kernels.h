@@ -73,10 +73,16 @@ struct Sp2Job {
     double nocc, weight;
     int n, mol, tile0, ntiles;
     int fallback;           // 1: a stalled purification falls back to the eigensolver; 0: LINALG
+    // mixed precision: the FP32 ping-pong iterates of the TF32 iterations, rows of ldf floats
+    // (n rounded up to a multiple of 4; the pad columns hold zeros), 16-byte aligned
+    float* Xf0;
+    float* Xf1;
+    int ldf;
 };
 
 struct Sp2State {
     int active, steps, cur, square, converged;
+    int lowp;  // this run's products are TF32 (the molecule's MolState::lowp when it started)
     double trX, trX2, emin, emax;
     double idem[2];
 };
@@ -95,6 +101,10 @@ struct TriJob {
 struct ScfParams {
     int max_scf, use_diis, accelerator;
     double e_tol, p_tol, adiis_switch;
+    // mixed precision: a molecule leaves its TF32 phase once the RMS density change falls below
+    // lowp_switch, or after lowp_max_iter iterations
+    double lowp_switch;
+    int lowp_max_iter;
 };
 
 __global__ void k_pair_integrals(const MolDesc* mols, int nmol, const long long* pair_prefix, long long npairs,
@@ -123,6 +133,10 @@ __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* s
 // *8: any matrix (8-byte copies)
 __global__ void k_sp2_step16(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
 __global__ void k_sp2_step8(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+// the TF32 step of the mixed path's reduced-precision iterations (jobs with Sp2State::lowp);
+// tf32_smem_bytes() of dynamic shared memory, same tile lists
+__global__ void k_sp2_step_tf32(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+size_t tf32_smem_bytes();
 // E = F.P - P.F over the upper-triangle tiles: history push of E and its CDIIS Gram row
 __global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
@@ -146,6 +160,13 @@ size_t tridiag_big_smem_bytes(int n);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
 #ifdef __CUDACC__
+// FP32 -> nearest TF32 value (ties away from zero), kept in an FP32 register
+__device__ __forceinline__ float tf32_round(float x) {
+    unsigned u;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(u) : "f"(x));
+    return __uint_as_float(u);
+}
+
 // Sum of the G per-CTA shares of a multi-CTA reduction, the same in every warp of every CTA: lane
 // l adds shares l, l+32, ... in that order, then a butterfly over the lanes (every lane ends with
 // the same sum: each level adds the same two partial sums, and addition commutes exactly).  All
@@ -162,7 +183,7 @@ __device__ __forceinline__ double group_share_sum(const double* share, int G) {
 __global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                            const int* atom_z, double* arena);
 __global__ void k_identity(const ChanJob* jobs);
-__global__ void k_state_init(MolState* st, int nmol);
+__global__ void k_state_init(MolState* st, int nmol, int lowp);
 __global__ void k_post_fock(const ChanJob* jobs, const MolDesc* mols, const MolState* st, int nblk, int energy_only,
                             int force);
 __global__ void k_diis_solve(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,

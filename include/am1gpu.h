@@ -214,6 +214,8 @@ typedef struct {
     double purification_steps;   /* purification steps summed over molecules, channels, iterations */
     double purification_flops;   /* their algorithmic work: n^3 per symmetric product X.X */
     double purification_bytes;   /* their algorithmic HBM traffic: 16 n^2 per product (read X, write X^2) */
+    double lowp_purification_steps;  /* products X.X of the mixed path's reduced-precision (TF32) iterations */
+    double lowp_purification_flops;  /* their algorithmic work, n^3 each (not in purification_flops) */
 } am1gpu_call_stats;
 
 /* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */
