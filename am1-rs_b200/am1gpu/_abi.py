@@ -138,6 +138,15 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(Result), _ip],
     ),
+    "am1gpu_gradient": (
+        ctypes.c_int,
+        [ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double)],
+    ),
+    "am1gpu_gradient_batch": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(Result),
+         ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), _ip],
+    ),
     "am1gpu_build_core": (ctypes.c_int, [ctypes.POINTER(Molecule), ctypes.c_int32, _dp, _dp]),
     "am1gpu_build_fock": (
         ctypes.c_int,

@@ -128,6 +128,38 @@ class Batch:
         return out
 
 
+def gradient(numbers, xyz_bohr, charge=0.0, multiplicity=1, **opts) -> dict:
+    """SCF plus the closed-form nuclear gradient through ``am1gpu_gradient`` (positions in Bohr).
+    Returns the SCF result dict with ``gradient`` (natoms x 3, eV/Bohr) and ``forces``."""
+    mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
+    o = _abi.default_options(**opts)
+    nao = _nao(mb.z, opts.get("method", "am1")) if mb.z.size else 0
+    rb = _abi.ResultBuffers(mb.z.shape[0], nao, False)
+    g = np.zeros((mb.z.shape[0], 3))
+    rc = _abi.lib().am1gpu_gradient(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res),
+                                    g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    d = _result_dict(rb, rc, False)
+    if rc:
+        d["error"] = _abi.lib().am1gpu_last_error().decode()
+    d["gradient"] = g
+    d["forces"] = -g
+    return d
+
+
+def gradient_batch(mols, **opts):
+    """Batched ``am1gpu_gradient_batch``: (status list, result dicts with ``gradient``)."""
+    b = Batch(mols, opts.get("method", "am1"), False)
+    gs = [np.zeros((m.z.shape[0], 3)) for m in b.mbs]
+    ptrs = (ctypes.POINTER(ctypes.c_double) * len(gs))(*[g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for g in gs])
+    o = _abi.default_options(**opts)
+    _abi.lib().am1gpu_gradient_batch(len(b.mbs), b.arr, ctypes.byref(o), b.res, ptrs, b.status)
+    res = b.results()
+    for r, g in zip(res, gs):
+        r["gradient"] = g
+        r["forces"] = -g
+    return list(b.status), res
+
+
 def last_call_stats() -> dict:
     st = _abi.CallStats()
     _check(_abi.lib().am1gpu_last_call_stats(ctypes.byref(st)))

@@ -503,6 +503,8 @@ struct Batch {
     double* h_charges;
     double* d_eps;  // every channel's orbital energies, contiguous (job order)
     double* h_eps;  // their pinned host copy
+    double* d_grad;  // nuclear gradient, 3 per atom (internal atom order), when asked for
+    double* h_grad;
     long long eps_total = 0;
     long long arena_doubles = 0;
 };
@@ -594,6 +596,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     long long eps_total = 0;
     for (auto& p : b.plans) eps_total += (long long)p.nch * p.nao;
     const size_t o_eps = take(dv, sizeof(double) * std::max<long long>(eps_total, 1));
+    const size_t o_grad = take(dv, sizeof(double) * 3 * std::max<long long>(natoms, 1));
     const size_t dtotal = align256(dv);
     // pinned staging also receives the outputs
     size_t hs = staged;
@@ -602,6 +605,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t h_o_res = take(hs, sizeof(double) * RES_N * b.nmol);
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
     const size_t h_o_eps = take(hs, sizeof(double) * std::max<long long>(eps_total, 1));
+    const size_t h_o_grad = take(hs, sizeof(double) * 3 * std::max<long long>(natoms, 1));
     int rc = mem_ensure(mem, dtotal, align256(hs));
     if (rc) return rc;
     Mem* ws = &mem;
@@ -641,12 +645,14 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_res = (double*)dptr(o_res);
     b.d_charges = (double*)dptr(o_chg);
     b.d_eps = (double*)dptr(o_eps);
+    b.d_grad = (double*)dptr(o_grad);
     b.eps_total = eps_total;
     b.h_active = (int*)(Hs + h_o_active);
     b.h_work = (double*)(Hs + h_o_work);
     b.h_res = (double*)(Hs + h_o_res);
     b.h_charges = (double*)(Hs + h_o_chg);
     b.h_eps = (double*)(Hs + h_o_eps);
+    b.h_grad = (double*)(Hs + h_o_grad);
     // ---- fill the staged region
     MolDesc* hm = (MolDesc*)(Hs + o_mols);
     int* hz = (int*)(Hs + o_z);
@@ -1193,6 +1199,22 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     return run.collect();
 }
 
+// Nuclear gradient at the converged densities (closed_form_gradient, src/gradient.rs:173-253),
+// fetched into b.h_grad.
+int run_gradient(Batch& b, Mem& mem, const DevElem* dp, am1gpu_call_stats* stats) {
+    cudaStream_t s = mem.stream;
+    if (b.natoms > 0) {
+        k_gradient<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_atom_xyz, b.d_jobs, b.d_job0,
+                                                     b.d_grad, b.d_status);
+        CK(cudaGetLastError());
+        stats->kernel_launches += 1;
+    }
+    CK(cudaMemcpyAsync(b.h_grad, b.d_grad, sizeof(double) * 3 * std::max(b.natoms, 1), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    stats->d2h_bytes += (int64_t)(sizeof(double) * 3 * std::max(b.natoms, 1));
+    return AM1GPU_OK;
+}
+
 int fetch_results(Batch& b, Mem& mem, am1gpu_call_stats* stats) {
     cudaStream_t s = mem.stream;
     CK(cudaMemcpyAsync(b.h_res, b.d_res, sizeof(double) * RES_N * b.nmol, cudaMemcpyDeviceToHost, s));
@@ -1314,7 +1336,9 @@ void fill_empty(am1gpu_result* r) {
 
 }  // namespace
 
-int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* res, int* status) {
+// grads (optional): one caller buffer of 3 * natoms doubles per molecule for the nuclear gradient
+int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* res, int* status,
+              double* const* grads = nullptr) {
     g_err.clear();
     tl_stats = am1gpu_call_stats{};
     if (nmol < 0 || (nmol > 0 && (!mols || !res)) || !opts) return fail(AM1GPU_INVALID_INPUT, "null argument");
@@ -1369,6 +1393,7 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
         rc = workspace(&ws, 0, 0);
         if (!rc) rc = build_batch(mols, *opts, std::move(plans), b, *ws, &tl_stats);
         if (!rc) rc = run_device(b, *ws, ctx->d_params, *opts, &tl_stats);
+        if (!rc && grads) rc = run_gradient(b, *ws, ctx->d_params, &tl_stats);
         if (!rc) rc = fetch_results(b, *ws, &tl_stats);
         if (rc) {
             for (auto& p : b.plans)
@@ -1377,6 +1402,12 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
         }
         for (int mi = 0; mi < b.nmol; ++mi) {
             const int u = b.plans[mi].user;
+            if (grads && grads[u]) {  // caller atom order
+                const MolPlan& p = b.plans[mi];
+                const double* g = b.h_grad + 3LL * b.mols[mi].atom_base;
+                for (int ia = 0; ia < p.natoms; ++ia)
+                    for (int k = 0; k < 3; ++k) grads[u][3 * p.order[ia] + k] = g[3 * ia + k];
+            }
             int r = write_result(b, ws, mi, &res[u], &tl_stats);
             if (status) status[u] = r;
             if (r && !first) {
@@ -1628,6 +1659,21 @@ int am1gpu_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_re
     am1gpu_options o = *opts;
     o.precision = AM1GPU_PRECISION_FP64;  // the plain path is FP64 throughout
     return am1::scf_batch(1, mol, &o, res, &st);
+}
+
+int am1gpu_gradient(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res, double* gradient) {
+    if (!mol || !opts || !res || !gradient) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    int32_t st = 0;
+    am1gpu_options o = *opts;
+    o.precision = AM1GPU_PRECISION_FP64;
+    double* const g[1] = {gradient};
+    return am1::scf_batch(1, mol, &o, res, &st, g);
+}
+
+int am1gpu_gradient_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* results,
+                          double* const* gradients, int32_t* status) {
+    if (nmol > 0 && !gradients) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    return am1::scf_batch(nmol, mols, opts, results, status, gradients);
 }
 
 int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* results,

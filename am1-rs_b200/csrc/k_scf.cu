@@ -91,6 +91,8 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
     const MolState& s = st[jb.mol];
     if (!force && !s.active) return;
     const int n = jb.n;
+    const int nb = red_blocks(n);
+    if ((int)blockIdx.x >= nb) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int newslot = 0;
     unsigned live = 0;
@@ -100,7 +102,7 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
 #pragma unroll
     for (int k = 0; k < RED_N; ++k) acc[k] = 0.0;
     const bool adiis = jb.hD != nullptr;
-    for (int r = blockIdx.x * POST_WARPS + warp; r < n; r += nblk * POST_WARPS) {
+    for (int r = blockIdx.x * POST_WARPS + warp; r < n; r += nb * POST_WARPS) {
         const double* Fr = jb.F + (long long)r * n;
         const double* Pr = jb.P + (long long)r * n;
         const double* Hr = jb.H + (long long)r * n;
@@ -317,7 +319,7 @@ __global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __
     for (int k = 0; k < RED_N; ++k) tot[k] = 0.0;
     for (int c = 0; c < md.nch; ++c) {
         const ChanJob& jb = jobs[mol_job0[mi] + c];
-        for (int b = 0; b < nblk; ++b)
+        for (int b = 0; b < red_blocks(jb.n); ++b)
             for (int k = 0; k < RED_N; ++k) tot[k] += jb.red[(long long)b * RED_N + k];
         for (int t = 0; t < jb.ntiles; ++t) {  // the commutator pass, in tile order
             tot[RED_ERR2] += jb.cpart[(long long)t * CP_N + CP_ERR2];
@@ -450,9 +452,11 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
 __global__ void k_density_post(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int nblk) {
     const ChanJob jb = jobs[blockIdx.y];
     if (!st[jb.mol].active) return;
+    const int nb = red_blocks(jb.n);
+    if ((int)blockIdx.x >= nb) return;
     const long long nn = (long long)jb.n * jb.n;
     double acc = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)nblk * blockDim.x) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)nb * blockDim.x) {
         const double pn = jb.Pnew[i];
         const double d = pn - jb.P[i];
         acc += d * d;
@@ -488,7 +492,7 @@ __global__ void k_converge(const MolDesc* __restrict__ mols, const ChanJob* __re
     for (int c = 0; c < md.nch; ++c) {
         const ChanJob& jb = jobs[mol_job0[mi] + c];
         double ss = 0.0;
-        for (int b = 0; b < nblk; ++b) ss += jb.red2[b];
+        for (int b = 0; b < red_blocks(jb.n); ++b) ss += jb.red2[b];
         dp += sqrt(ss / fmax((double)jb.n * jb.n, 1.0));
     }
     const double de = fabs(s.e_elec - s.e_old);
@@ -534,7 +538,7 @@ __global__ void k_final_energy(const MolDesc* __restrict__ mols, const ChanJob* 
     double eh = 0.0, ef = 0.0;
     for (int c = 0; c < md.nch; ++c) {
         const ChanJob& jb = jobs[mol_job0[mi] + c];
-        for (int b = 0; b < nblk; ++b) {
+        for (int b = 0; b < red_blocks(jb.n); ++b) {
             eh += jb.red[(long long)b * RED_N + RED_E_H];
             ef += jb.red[(long long)b * RED_N + RED_E_F];
         }

@@ -374,13 +374,15 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
     const Sp2Job jb = jobs[blockIdx.y];
     if (!st[jb.mol].active) return;
     const int n = jb.n;
+    const int nb = sp2_init_blocks(n);
+    if ((int)blockIdx.x >= nb) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     __shared__ double red[2][32];
     const double emin = jb.bounds[0], emax = jb.bounds[1];  // from k_sp2_bounds
     const double inv = 1.0 / fmax(emax - emin, 1e-300);
     const bool lowp = st[jb.mol].lowp;
     double tr = 0.0, fr = 0.0;
-    for (int r = blockIdx.x * nw + warp; r < n; r += nblk * nw) {
+    for (int r = blockIdx.x * nw + warp; r < n; r += nb * nw) {
         const double* Fr = jb.F + (long long)r * n;
         if (lowp) {  // FP32 iterate (rows of ldf floats, pad columns zero in both buffers)
             float* Xr = jb.Xf0 + (long long)r * jb.ldf;
@@ -439,7 +441,7 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
     s.cur = 0;
     s.converged = 0;
     double tr = 0.0, fr = 0.0;
-    for (int b = 0; b < nblk; ++b) {
+    for (int b = 0; b < sp2_init_blocks(jb.n); ++b) {
         tr += jb.part[2 * b];
         fr += jb.part[2 * b + 1];
     }

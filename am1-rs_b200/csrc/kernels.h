@@ -113,6 +113,10 @@ __global__ void k_pair_integrals(const MolDesc* mols, int nmol, const long long*
 __global__ void k_core_diag(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                             const int* atom_z, const double* wstore, double* hmat);
 __global__ void k_core_energy(const MolDesc* mols, const double* ecc, MolState* st);
+// nuclear gradient at the current densities (jobs[].P), a warp per atom (8 per block); gradient:
+// 3 doubles per atom, internal atom order
+__global__ void k_gradient(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params, const int* atom_z,
+                           const double* atom_xyz, const ChanJob* jobs, const int* mol_job0, double* gradient, int* mol_status);
 __global__ void k_fock(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                        const int* atom_z, const double* wstore, double* arena, const MolState* st, int force);
 // C = alpha A B (A row-major M x K) and C = alpha A^T B (A stored K x M)
@@ -127,6 +131,12 @@ __global__ void k_eig_sort(const EigJob* jobs, const MolState* st, int force, co
 __global__ void k_sp2_bounds(const Sp2Job* jobs, const MolState* st);
 __global__ void k_sp2_bounds_big(const Sp2Job* jobs, int job, const MolState* st);
 __global__ void k_sp2_bounds_cl(const Sp2Job* jobs, const int* big, const MolState* st);
+// Blocks of a channel's row reductions (post-Fock pass and density difference: red_blocks; the
+// purification start: sp2_init_blocks).  They depend on the channel's own n only, so a molecule's
+// sums are the same whatever else is in its batch; a launch's x extent is the batch's largest
+// count, and the blocks past a channel's own count leave at once.
+__host__ __device__ __forceinline__ int red_blocks(int n) { return n >= 497 ? 32 : (n + 15) / 16 < 1 ? 1 : (n + 15) / 16; }
+__host__ __device__ __forceinline__ int sp2_init_blocks(int n) { return n >= 249 ? 32 : (n + 7) / 8 < 1 ? 1 : (n + 7) / 8; }
 __global__ void k_sp2_init(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int nblk);
 __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* st, int njobs, int nblk);
 // *16: every matrix of the tile list has even n and 16-byte aligned rows (16-byte copies);

@@ -129,6 +129,21 @@ int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_opt
                      am1gpu_result* results, int32_t* status);
 
 /*
+ * SCF single point plus the closed-form nuclear gradient at its converged density: replaces
+ * closed_form_gradient (src/gradient.rs:173-253) for a molecule (RHF and, through the same
+ * spin-resolved pair formula, UHF: fixed_density_gradient_uhf, src/gradient.rs:495-544).
+ * gradient receives dE/dx (eV/Bohr) as natoms * 3 doubles in the caller's atom order; the
+ * forces are its negation.  The result and return code are those of am1gpu_scf (FP64); a
+ * molecule that did not converge still gets the gradient at its last density, with
+ * AM1GPU_SCF_NOT_CONVERGED returned, as the reference's run_am1 error would stop it there.
+ */
+int am1gpu_gradient(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res, double* gradient);
+
+/* The batched form: gradients[i] (natoms_i * 3 doubles, or NULL to skip) per molecule. */
+int am1gpu_gradient_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
+                          am1gpu_result* results, double* const* gradients, int32_t* status);
+
+/*
  * Core Hamiltonian and core-core energy of one molecule: replaces build_core_with_neighbors
  * (src/hamiltonian.rs:211-366) and core_core_energy_with_neighbors (src/repulsion.rs:38-56)
  * for a molecule.  h_core is nao*nao row-major (eV); *core_ev in eV.
