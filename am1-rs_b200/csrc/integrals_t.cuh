@@ -279,14 +279,16 @@ __device__ void local_xx(const DevElem& ei, const DevElem& ej, const T& r, T ri[
 #undef SQ2
 }
 
-// Integrals of one pair (i = heavy or lower index, j), written to the store; returns its size.
-template <class T>
-__device__ void pair_integrals(const DevElem& ei, const DevElem& ej, const T dv[3], const T& r, T* __restrict__ w) {
+// Integrals of one pair (i = heavy or lower index, j), each handed to sink(kk, ll, mm, nn, value)
+// as it is formed: (kk ll | mm nn) with kk >= ll the orbitals on i and mm >= nn those on j
+// (0 = s, 1-3 = p), in the store's order (row pack(kk, ll), column pack(mm, nn)).
+template <class T, class Sink>
+__device__ void pair_integrals_each(const DevElem& ei, const DevElem& ej, const T dv[3], const T& r, Sink&& sink) {
     const T inv = 1.0 / r;
     const T n[3] = {-(dv[0] * inv), -(dv[1] * inv), -(dv[2] * inv)};  // frame axis, = -x_ij
     const bool hi = ei.norb == 4, hj = ej.norb == 4;
     if (!hi && !hj) {
-        w[0] = rinv(r * r + (ei.rho0 + ej.rho0) * (ei.rho0 + ej.rho0)) * AM1_EV;
+        sink(0, 0, 0, 0, rinv(r * r + (ei.rho0 + ej.rho0) * (ei.rho0 + ej.rho0)) * AM1_EV);
         return;
     }
     // p = I - n n^T
@@ -306,18 +308,17 @@ __device__ void pair_integrals(const DevElem& ei, const DevElem& ej, const T dv[
         const T r1 = rinv((r + da) * (r + da) + ade) * ev1 - rinv((r - da) * (r - da) + ade) * ev1;
         const T r2 = ee + rinv((r + qa) * (r + qa) + aqe) * ev2 + rinv((r - qa) * (r - qa) + aqe) * ev2 - q6;
         const T r3 = ee + rinv(r * r + qa * qa + aqe) * ev1 - q6;
-        w[0] = ee;
+        sink(0, 0, 0, 0, ee);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            w[(k + 1) * (k + 2) / 2] = r1 * n[k];
+            sink(k + 1, 0, 0, 0, r1 * n[k]);
 #pragma unroll
-            for (int l = 0; l <= k; ++l) w[(k + 1) * (k + 2) / 2 + l + 1] = r2 * (n[k] * n[l]) + r3 * p[k][l];
+            for (int l = 0; l <= k; ++l) sink(k + 1, l + 1, 0, 0, r2 * (n[k] * n[l]) + r3 * p[k][l]);
         }
         return;
     }
     T ri[22];
     local_xx(ei, ej, r, ri);
-    int idx = 0;
 #pragma unroll 1
     for (int kk = 0; kk < 4; ++kk)
         for (int ll = 0; ll <= kk; ++ll)
@@ -344,8 +345,17 @@ __device__ void pair_integrals(const DevElem& ei, const DevElem& ej, const T dv[
                             ri[19] * (n[k] * (p[l][q] * n[m] + p[l][m] * n[q]) + n[l] * (p[k][q] * n[m] + p[k][m] * n[q])) +
                             ri[20] * (p[k][l] * p[m][q]) + ri[21] * (p[k][m] * p[l][q] + p[k][q] * p[l][m]);
                     }
-                    w[idx++] = v;
+                    sink(kk, ll, mm, nn, v);
                 }
+}
+
+// pair_integrals_each written to the store: XX 10 x 10 row-major, XH 10, HH 1.
+template <class T>
+__device__ void pair_integrals(const DevElem& ei, const DevElem& ej, const T dv[3], const T& r, T* __restrict__ w) {
+    const int nwb = ej.norb == 4 ? 10 : 1;
+    pair_integrals_each(ei, ej, dv, r, [&](int kk, int ll, int mm, int nn, const T& v) {
+        w[(kk * (kk + 1) / 2 + ll) * nwb + mm * (mm + 1) / 2 + nn] = v;
+    });
 }
 
 template <class T>

@@ -16,7 +16,8 @@
 //
 // A warp per atom walks its partners, a pair per lane; each pair is evaluated for both of its
 // atoms (twice in all) so that every atom's sum is a fixed-order warp reduction: deterministic,
-// no atomics and no per-pair scratch.
+// no atomics and no per-pair scratch.  The two-centre integrals are contracted as they are formed
+// (pair_integrals_each), so no block of 100 dual numbers is held per thread.
 #include <cuda_runtime.h>
 
 #include "am1gpu_internal.h"
@@ -24,8 +25,6 @@
 #include "kernels.h"
 
 namespace am1 {
-
-__device__ __forceinline__ int pack_pair(int k, int l) { return k >= l ? k * (k + 1) / 2 + l : l * (l + 1) / 2 + k; }
 
 // dE_pair/d(delta) of the pair (a, b) at fixed densities; false for an element without the
 // closed-form overlap (valence shell n >= 4).  Pa: channel-0 density (RHF: total), Pb: channel 1
@@ -58,24 +57,26 @@ __device__ bool pair_force(const DevElem& ea, const DevElem& eb, int za, int zb,
         const double bi = i == 0 ? ea.beta_s : ea.beta_p;
         for (int j = 0; j < nb; ++j) acc(pt(oa + i, ob + j) * (bi + (j == 0 ? eb.beta_s : eb.beta_p)), S[i][j]);
     }
-    // two-centre integrals w[pack(mu nu)][pack(la si)] (XX 10 x 10, XH 10 x 1, HH 1 x 1)
-    D3 w[100];
-    pair_integrals(ea, eb, dv, r, w);
-    const int nwb = nb == 4 ? 10 : 1;
-    // electron-core: e1b = -Z_b w[.][0] on a's block, e2a = -Z_a w[0][.] on b's block (src/gradient.rs:434-449)
-    for (int i = 0; i < na; ++i)
-        for (int j = 0; j < na; ++j) acc(-eb.core_charge * pt(oa + i, oa + j), w[pack_pair(i, j) * nwb]);
-    for (int k = 0; k < nb; ++k)
-        for (int l = 0; l < nb; ++l) acc(-ea.core_charge * pt(ob + k, ob + l), w[pack_pair(k, l)]);
-    // two-electron Coulomb and exchange (src/gradient.rs:450-466)
-    for (int mu = 0; mu < na; ++mu)
-        for (int nu = 0; nu < na; ++nu) {
-            const double pmn = pt(oa + mu, oa + nu);
-            const D3* wr = w + pack_pair(mu, nu) * nwb;
-            for (int la = 0; la < nb; ++la)
-                for (int si = 0; si < nb; ++si)
-                    acc(pmn * pt(ob + la, ob + si) - px(oa + mu, ob + la, oa + nu, ob + si), wr[pack_pair(la, si)]);
+    // two-centre integrals, contracted as they are formed (no integral block is stored): the
+    // element (kk ll | mm nn), kk >= ll on a and mm >= nn on b, stands for every ordering of its
+    // index pairs (src/gradient.rs:434-466 sums over all of them):
+    //   electron-core  e1b = -Z_b (mu nu | s s) on a's block, e2a = -Z_a (s s | la si) on b's
+    //   Coulomb        P_{mu nu} P_{la si}
+    //   exchange       -(Pa_{mu la} Pa_{nu si} + Pb_{mu la} Pb_{nu si})
+    pair_integrals_each(ea, eb, dv, r, [&](int kk, int ll, int mm, int nn, const D3& v) {
+        const int ma = kk == ll ? 1 : 2, mb = mm == nn ? 1 : 2;
+        const double pa = pt(oa + kk, oa + ll), pb = pt(ob + mm, ob + nn);
+        double c = ma * mb * pa * pb;
+        c -= px(oa + kk, ob + mm, oa + ll, ob + nn);
+        if (ll != kk) c -= px(oa + ll, ob + mm, oa + kk, ob + nn);
+        if (nn != mm) {
+            c -= px(oa + kk, ob + nn, oa + ll, ob + mm);
+            if (ll != kk) c -= px(oa + ll, ob + nn, oa + kk, ob + mm);
         }
+        if (mm == 0) c -= eb.core_charge * ma * pa;  // (kk ll | s s)
+        if (kk == 0) c -= ea.core_charge * mb * pb;  // (s s | mm nn)
+        acc(c, v);
+    });
     return true;
 }
 
