@@ -231,6 +231,16 @@ def build_fock(numbers, xyz_bohr, p_tot, p_spin, spin_scale, method="am1"):
     return f
 
 
+def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
+    """G(P) = J(P) - K(P/2) for a stack of densities (nrhs x nao x nao), ``am1gpu_g_matrix_batch``."""
+    mb = _abi.MolBuffers(numbers, xyz_bohr)
+    d = np.ascontiguousarray(densities, dtype=np.float64)
+    g = np.zeros_like(d)
+    _check(_abi.lib().am1gpu_g_matrix_batch(ctypes.byref(mb.mol), _abi.METHOD[method], int(d.shape[0]), d.ctypes.data_as(_dp),
+                                            g.ctypes.data_as(_dp)))
+    return g
+
+
 def eigh(a):
     a = np.ascontiguousarray(a, dtype=np.float64)
     n = a.shape[0]

@@ -1515,6 +1515,73 @@ int build_fock_one(const am1gpu_molecule* mol, int method, const double* p_tot, 
     return AM1GPU_OK;
 }
 
+// G(P_r) = J(P_r) - K(P_r / 2) for nrhs densities of one molecule (build_g_matrix,
+// src/fock.rs:556-575, FockBase::Zero).  The right-hand sides become copies of the molecule in one
+// batch, in chunks of at most kGChunk, each with its own closed-shell channel: the pair integrals
+// are formed once per copy (cheap next to the Fock build), H_core is zeroed, and one k_fock launch
+// builds every copy's matrix, so F = 0 + J(P_r) - 1/2 K(P_r) exactly.
+constexpr int kGChunk = 64;
+
+int g_matrix_batch(const am1gpu_molecule* mol, int method, int nrhs, const double* dens, double* g) {
+    g_err.clear();
+    if (!mol || nrhs < 0 || (nrhs > 0 && (!dens || !g))) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (nrhs == 0) return AM1GPU_OK;
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    am1gpu_options o;
+    am1gpu_default_options(&o);
+    o.method = method;
+    o.reference = AM1GPU_REF_RHF;  // one channel per copy: spin scale 1/2
+    am1gpu_molecule m = *mol;
+    double ne = 0.0;
+    for (int i = 0; i < m.natoms; ++i)
+        if (m.z[i] >= 0 && m.z[i] <= MAX_Z) ne += helem(method == 1, m.z[i]).core_charge;
+    m.charge = ((long long)std::llround(ne)) % 2 ? 1.0 : 0.0;  // any closed shell: the electron count plays no part
+    m.multiplicity = 1;
+    MolPlan p;
+    rc = plan_molecule(m, o, 0, p);
+    if (rc) return rc;
+    const int n = p.nao;
+    const size_t nn = (size_t)n * n;
+    Workspace* ws;
+    tl_stats = am1gpu_call_stats{};
+    rc = workspace(&ws, 0, 0);
+    if (rc) return rc;
+    std::vector<double> t(nn);
+    for (int r0 = 0; r0 < nrhs; r0 += kGChunk) {
+        const int cnt = std::min(kGChunk, nrhs - r0);
+        std::vector<am1gpu_molecule> copies(cnt, m);
+        std::vector<MolPlan> plans(cnt, p);
+        for (int c = 0; c < cnt; ++c) plans[c].user = c;
+        Batch b;
+        rc = build_batch(copies.data(), o, std::move(plans), b, *ws, &tl_stats);
+        if (!rc) rc = launch_core(b, ws, ctx->d_params, nullptr);
+        if (rc) return rc;
+        const auto& map = b.plans[0].ao_map;
+        for (int c = 0; c < cnt; ++c) {
+            const double* pr = dens + (size_t)(r0 + c) * nn;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) t[(size_t)i * n + j] = pr[(size_t)map[i] * n + map[j]];
+            CK(cudaMemcpyAsync(b.jobs[c].P, t.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, ws->stream));
+            CK(cudaMemsetAsync(const_cast<double*>(b.jobs[c].H), 0, sizeof(double) * nn, ws->stream));  // the copy's own H_core
+            CK(cudaStreamSynchronize(ws->stream));  // t is reused for the next copy
+        }
+        k_fock<<<cdiv(b.natoms, 8), 256, 0, ws->stream>>>(b.d_mols, b.d_atom_mol, b.natoms, ctx->d_params, b.d_atom_z, b.d_wstore,
+                                                          b.d_arena, b.d_st, 1);
+        CK(cudaGetLastError());
+        tl_stats.kernel_launches += 1;
+        for (int c = 0; c < cnt; ++c) {
+            rc = fetch_matrix(ws, b.jobs[c].F, n, t, &tl_stats);
+            if (rc) return rc;
+            double* gr = g + (size_t)(r0 + c) * nn;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) gr[(size_t)map[i] * n + map[j]] = t[(size_t)i * n + j];
+        }
+    }
+    return AM1GPU_OK;
+}
+
 int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_override = nullptr) {
     g_err.clear();
     if (n < 0 || (n > 0 && (!a || !w || !v))) return fail(AM1GPU_INVALID_INPUT, "null argument");
@@ -1688,6 +1755,10 @@ int am1gpu_build_core(const am1gpu_molecule* mol, int32_t method, double* h_core
 int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* p_tot, const double* p_spin,
                       double spin_scale, double* fock) {
     return am1::build_fock_one(mol, method, p_tot, p_spin, spin_scale, fock);
+}
+
+int am1gpu_g_matrix_batch(const am1gpu_molecule* mol, int32_t method, int32_t nrhs, const double* densities, double* g) {
+    return am1::g_matrix_batch(mol, method, nrhs, densities, g);
 }
 
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {

@@ -151,6 +151,15 @@ int am1gpu_gradient_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gp
 int am1gpu_build_core(const am1gpu_molecule* mol, int32_t method, double* h_core, double* core_ev);
 
 /*
+ * Two-electron matrices G(P_r) = J(P_r) - K(P_r / 2), no H_core, for nrhs densities of one
+ * molecule: replaces build_g_matrix (src/fock.rs:556-575, FockBase::Zero), which the CPHF
+ * response calls 3N times per iteration (src/hessian.rs:1401, 1567).  densities and g are
+ * nrhs consecutive nao x nao row-major matrices in the caller's AO order.
+ */
+int am1gpu_g_matrix_batch(const am1gpu_molecule* mol, int32_t method, int32_t nrhs, const double* densities,
+                          double* g);
+
+/*
  * Spin Fock matrix F = H_core + J(p_tot) - K(spin_scale * p_spin): replaces
  * build_fock_spin_with (src/fock.rs:249-511) with FockBase::CoreHamiltonian.  RHF is
  * p_spin = p_tot with spin_scale 0.5 (build_fock, src/fock.rs:526-546).
