@@ -387,10 +387,6 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
             return fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, std::string(name) + " has no parameters for element Z=" +
                                                               std::to_string(z) + "; " + name + " covers " + sup);
         }
-        if (tab[z].n > 3)
-            return fail(AM1GPU_UNSUPPORTED, std::string("element ") + kSymbols[z] +
-                                                " has a valence shell n >= 4; its Slater overlap needs the numerical quadrature, "
-                                                "which this GPU path does not implement");
         if (!std::isfinite(m.xyz_bohr[3 * i]) || !std::isfinite(m.xyz_bohr[3 * i + 1]) || !std::isfinite(m.xyz_bohr[3 * i + 2]))
             return fail(AM1GPU_INVALID_INPUT, "non-finite coordinate for atom " + std::to_string(i));
     }

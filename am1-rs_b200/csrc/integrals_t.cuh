@@ -8,6 +8,7 @@
 //   frame-free rotation    src/integrals.rs:487-569 (axis n = -x_ab and projector I - n n^T)
 //   electron-core terms    src/integrals.rs:232-276 (e1b / e2a = -Z * row/column 0 of w)
 //   Slater overlap         src/overlap.rs:16-40, 120-322, 357-500 (n <= 3 shells)
+//   numerical overlap      src/overlap_numeric.rs:22-123 (shells with n >= 4)
 //   core-core pair energy  src/repulsion.rs:144-188
 #pragma once
 
@@ -15,6 +16,7 @@
 
 #include "am1gpu_internal.h"
 #include "dual3.cuh"
+#include "params/gauss_legendre.h"
 
 namespace am1 {
 
@@ -84,14 +86,70 @@ __device__ void bint7(const T& x, T b[7]) {
     }
 }
 
-// Local overlaps (s111, s211, s121, s221, s222) for ea.n >= eb.n; returns false for n >= 4.
+// Overlap of two Slater orbitals in the local diatomic frame (b at +z, distance r),
+// <n_a l_a m; z_a | n_b l_b m; z_b> with m = 0 (sigma) or 1 (pi), by Gauss-Legendre quadrature in
+// prolate-spheroidal coordinates: xi in [1, xi_max] (48 nodes), eta in [-1, 1] (40 nodes).  The
+// domain and the angular factors depend on r's value only; the radial factor carries r, so a D3
+// r gives the exact derivative of this quadrature (the boundary term at xi_max is negligible:
+// the integrand has decayed by e^-60 there).
+template <class T>
+__device__ T overlap_sto(int na, double za, int la, int m, int nb, double zb, int lb, const T& r) {
+    double c;
+    if (la == 0 && lb == 0) c = 0.5;
+    else if (la + lb == 1 && m == 0) c = 1.7320508075688772 / 2.0;
+    else if (la == 1 && lb == 1) c = m == 0 ? 1.5 : 0.75;
+    else return zero<T>();
+    auto norm = [](int n, double zeta) {
+        double f = 1.0;
+        for (int k = 2; k <= 2 * n; ++k) f *= (double)k;
+        return ::pow(2.0 * zeta, (double)n + 0.5) / ::sqrt(f);
+    };
+    const double nab = norm(na, za) * norm(nb, zb) * c;
+    const double hr = 0.5 * val(r);
+    const T half_r = r * 0.5;
+    const double p = (za + zb) * hr;
+    const double xi_max = 1.0 + 60.0 / fmax(p, 0.05);
+    const double xi_mid = 0.5 * (1.0 + xi_max), xi_half = 0.5 * (xi_max - 1.0);
+    T sum = zero<T>();
+    for (int i = 0; i < kGlXiN; ++i) {
+        const double xi = xi_mid + xi_half * kGlXiX[i];
+        for (int j = 0; j < kGlEtaN; ++j) {
+            const double eta = kGlEtaX[j];
+            if (hr * (xi + eta) <= 0.0 || hr * (xi - eta) <= 0.0) continue;
+            const double cos_a = (1.0 + xi * eta) / (xi + eta), cos_b = (xi * eta - 1.0) / (xi - eta);
+            const double ang_a = la == 0 ? 1.0 : m == 0 ? cos_a : ::sqrt(fmax(1.0 - cos_a * cos_a, 0.0));
+            const double ang_b = lb == 0 ? 1.0 : m == 0 ? cos_b : ::sqrt(fmax(1.0 - cos_b * cos_b, 0.0));
+            const T ra = half_r * (xi + eta), rb = half_r * (xi - eta);
+            const T radial = dpow_i(ra, na - 1) * dpow_i(rb, nb - 1) * exp(ra * (-za) - rb * zb);
+            sum += radial * (xi_half * kGlXiW[i] * kGlEtaW[j] * ang_a * ang_b * (xi * xi - eta * eta));
+        }
+    }
+    return dpow_i(half_r, 3) * sum * nab;
+}
+
+// The five local overlaps of overlap_local by quadrature (any n; used for n >= 4), with the
+// analytic kernel's sign convention (src/overlap_numeric.rs:22-42).
+template <class T>
+__device__ void overlap_local_numeric(const DevElem& ea, const DevElem& eb, const T& r, T s[5]) {
+    s[0] = overlap_sto(ea.n, ea.zeta_s, 0, 0, eb.n, eb.zeta_s, 0, r);
+    s[1] = overlap_sto(ea.n, ea.zeta_p, 1, 0, eb.n, eb.zeta_s, 0, r);
+    s[2] = -overlap_sto(ea.n, ea.zeta_s, 0, 0, eb.n, eb.zeta_p, 1, r);
+    s[3] = -overlap_sto(ea.n, ea.zeta_p, 1, 0, eb.n, eb.zeta_p, 1, r);
+    s[4] = overlap_sto(ea.n, ea.zeta_p, 1, 1, eb.n, eb.zeta_p, 1, r);
+}
+
+// Local overlaps (s111, s211, s121, s221, s222) for ea.n >= eb.n: the closed forms for n <= 3,
+// the quadrature above.
 template <class T>
 __device__ bool overlap_local(const DevElem& ea, const DevElem& eb, const T& r, T s[5]) {
     const double za0 = ea.zeta_s, za1 = ea.zeta_p, zb0 = eb.zeta_s, zb1 = eb.zeta_p;
     T a[7], b[7];
     s[0] = s[1] = s[2] = s[3] = s[4] = zero<T>();
     const int na = ea.n, nb = eb.n;
-    if (na > 3) return false;
+    if (na > 3) {
+        overlap_local_numeric(ea, eb, r, s);
+        return true;
+    }
     const double sq3 = 1.7320508075688772, sq10 = 3.1622776601683795, sq30 = 5.477225575051661;
     // (s_a | s_b)
     aint7(r * (0.5 * (za0 + zb0)), a);

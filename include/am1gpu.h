@@ -31,11 +31,8 @@ enum am1gpu_status {
     AM1GPU_SCF_NOT_CONVERGED = 3,          /* Am1Error::ScfNotConverged          (error.rs:35-38) */
     AM1GPU_SCF_DIVERGED = 4,               /* Am1Error::ScfDiverged              (error.rs:45-47) */
     AM1GPU_LINALG = 5,                     /* Am1Error::LinearAlgebra            (error.rs:33) */
-    AM1GPU_UNSUPPORTED = 6,                /* element with a valence shell n >= 4 (its Slater
-                                              overlap needs the numerical quadrature of
-                                              src/overlap_numeric.rs, not on this path); more
-                                              than 8192 orbitals; eigenvectors (mo_coeff) of a
-                                              molecule with more than 448 orbitals */
+    AM1GPU_UNSUPPORTED = 6,                /* more than 8192 orbitals; eigenvectors (mo_coeff)
+                                              of a molecule with more than 448 orbitals */
     AM1GPU_DEVICE_ERROR = 7                /* CUDA failure or no device */
 };
 

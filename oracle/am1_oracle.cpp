@@ -229,6 +229,93 @@ void bintgs(double x, double b[13]) {
     }
 }
 
+// src/overlap_numeric.rs:172-213: Legendre P_n and P_n' by the three-term recurrence, and the
+// Gauss-Legendre rule on [-1, 1] by Newton iteration from the Chebyshev guess.
+void legendre_p_dp(int n, double x, double& p, double& dp) {
+    double p0 = 1.0, p1 = x;
+    if (n == 0) {
+        p = 1.0;
+        dp = 0.0;
+        return;
+    }
+    for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+    }
+    p = p1;
+    dp = n * (x * p1 - p0) / (x * x - 1.0);
+}
+
+struct GaussRule {
+    std::vector<double> x, w;
+};
+
+GaussRule gauss_legendre(int n) {
+    GaussRule g{std::vector<double>(n), std::vector<double>(n)};
+    const int m = (n + 1) / 2;
+    for (int i = 0; i < m; ++i) {
+        double x = std::cos(M_PI * (i + 0.75) / (n + 0.5)), p, dp;
+        for (int it = 0; it < 100; ++it) {
+            legendre_p_dp(n, x, p, dp);
+            const double dx = -p / dp;
+            x += dx;
+            if (std::fabs(dx) < 1.0e-15) break;
+        }
+        legendre_p_dp(n, x, p, dp);
+        const double w = 2.0 / ((1.0 - x * x) * dp * dp);
+        g.x[i] = -x;
+        g.x[n - 1 - i] = x;
+        g.w[i] = w;
+        g.w[n - 1 - i] = w;
+    }
+    return g;
+}
+
+// src/overlap_numeric.rs:50-123: <n_a l_a m; z_a | n_b l_b m; z_b> in the local frame (b at +z),
+// prolate-spheroidal quadrature with 48 (xi) x 40 (eta) Gauss-Legendre nodes.
+double overlap_sto(int na, double za, int la, int m, int nb, double zb, int lb, double r) {
+    double c;
+    if (la == 0 && lb == 0) c = 0.5;
+    else if ((la == 1 && lb == 0 && m == 0) || (la == 0 && lb == 1 && m == 0)) c = std::sqrt(3.0) / 2.0;
+    else if (la == 1 && lb == 1 && m == 0) c = 1.5;
+    else if (la == 1 && lb == 1 && m == 1) c = 0.75;
+    else return 0.0;
+    auto norm = [](int n, double zeta) {
+        double f = 1.0;
+        for (int k = 2; k <= 2 * n; ++k) f *= k;
+        return std::pow(2.0 * zeta, n + 0.5) / std::sqrt(std::max(f, 1.0));
+    };
+    static const GaussRule xr = gauss_legendre(48), er = gauss_legendre(40);
+    const double hr = 0.5 * r, p = (za + zb) * hr;
+    const double xi_max = 1.0 + 60.0 / std::max(p, 0.05);
+    const double xi_mid = 0.5 * (1.0 + xi_max), xi_half = 0.5 * (xi_max - 1.0);
+    double sum = 0.0;
+    for (int i = 0; i < 48; ++i) {
+        const double xi = xi_mid + xi_half * xr.x[i];
+        for (int j = 0; j < 40; ++j) {
+            const double eta = er.x[j];
+            const double ra = hr * (xi + eta), rb = hr * (xi - eta);
+            if (ra <= 0.0 || rb <= 0.0) continue;
+            const double cos_a = (1.0 + xi * eta) / (xi + eta), cos_b = (xi * eta - 1.0) / (xi - eta);
+            const double ang_a = la == 0 ? 1.0 : (m == 0 ? cos_a : std::sqrt(std::max(1.0 - cos_a * cos_a, 0.0)));
+            const double ang_b = lb == 0 ? 1.0 : (m == 0 ? cos_b : std::sqrt(std::max(1.0 - cos_b * cos_b, 0.0)));
+            const double radial = std::pow(ra, na - 1) * std::pow(rb, nb - 1) * std::exp(ra * (-za) - rb * zb);
+            sum += radial * (xi_half * xr.w[i] * er.w[j] * ang_a * ang_b * (xi * xi - eta * eta));
+        }
+    }
+    return hr * hr * hr * sum * (norm(na, za) * norm(nb, zb) * c);
+}
+
+// src/overlap_numeric.rs:22-42: the five local overlaps, in the analytic kernel's signs.
+void overlap_locals_numeric(const Elem& ea, const Elem& eb, double r, double s[5]) {
+    s[0] = overlap_sto(ea.n, ea.zeta_s, 0, 0, eb.n, eb.zeta_s, 0, r);
+    s[1] = overlap_sto(ea.n, ea.zeta_p, 1, 0, eb.n, eb.zeta_s, 0, r);
+    s[2] = -overlap_sto(ea.n, ea.zeta_s, 0, 0, eb.n, eb.zeta_p, 1, r);
+    s[3] = -overlap_sto(ea.n, ea.zeta_p, 1, 0, eb.n, eb.zeta_p, 1, r);
+    s[4] = overlap_sto(ea.n, ea.zeta_p, 1, 1, eb.n, eb.zeta_p, 1, r);
+}
+
 // src/overlap.rs:120-296, local-frame overlaps (s111, s211, s121, s221, s222); ea.n >= eb.n.
 bool overlap_locals(const Elem& ea, const Elem& eb, double r, double s[5]) {
     int jcall;
@@ -238,7 +325,10 @@ bool overlap_locals(const Elem& ea, const Elem& eb, double r, double s[5]) {
     else if (ea.n == 3 && eb.n == 1) jcall = 431;
     else if (ea.n == 3 && eb.n == 2) jcall = 5;
     else if (ea.n == 3 && eb.n == 3) jcall = 6;
-    else return false;  // n >= 4: numerical quadrature (src/overlap_numeric.rs), not restated
+    else {  // n >= 4: the numerical quadrature (src/overlap.rs:128-165)
+        overlap_locals_numeric(ea, eb, r, s);
+        return true;
+    }
     const double za[2] = {ea.zeta_s, ea.zeta_p}, zb[2] = {eb.zeta_s, eb.zeta_p};
     double a111[13], b111[13], a211[13], b211[13], a121[13], b121[13], a22[13], b22[13];
     aintgs(r * (0.5 * (za[0] + zb[0])), a111);
@@ -599,9 +689,6 @@ int check_elements(const Molecule& mol, const ParamSet& ps) {
                              std::string(ps.name) + " has no parameters for element Z=" + std::to_string(z) +
                                  "; " + ps.name + " covers Z in {" + sup + "}");
         }
-        if (ps.by_z[z].n > 3)
-            return set_error(AM1GPU_UNSUPPORTED, "element Z=" + std::to_string(z) +
-                                                     " has a valence shell n>=4 (numerical Slater overlap)");
     }
     return AM1GPU_OK;
 }
@@ -1513,6 +1600,19 @@ int run_am1(const am1gpu_molecule* m, const am1gpu_options* o, am1gpu_result* re
 // C ABI of the oracle (same structs as the library's public header, prefixed oracle_)
 // ----------------------------------------------------------------------------------------
 extern "C" {
+
+// The five local overlaps of the pair (za, zb) at distance r (ea.n >= eb.n is arranged here):
+// numeric = 1 forces the quadrature, which for n <= 3 must reproduce the closed forms
+// (src/overlap.rs:718-747 checks the same).
+int oracle_local_overlaps(int method, int za, int zb, double r, int numeric, double out[5]) {
+    const ParamSet& ps = params_for(method);
+    if (za < 0 || za > NDDO_MAX_Z || zb < 0 || zb > NDDO_MAX_Z || !ps.present[za] || !ps.present[zb]) return AM1GPU_INVALID_INPUT;
+    const Elem& a = ps.by_z[za].n >= ps.by_z[zb].n ? ps.by_z[za] : ps.by_z[zb];
+    const Elem& b = ps.by_z[za].n >= ps.by_z[zb].n ? ps.by_z[zb] : ps.by_z[za];
+    if (numeric) overlap_locals_numeric(a, b, r, out);
+    else if (!overlap_locals(a, b, r, out)) return AM1GPU_UNSUPPORTED;
+    return AM1GPU_OK;
+}
 
 int oracle_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res) {
     return run_am1(mol, opts, res);

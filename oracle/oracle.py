@@ -40,6 +40,7 @@ _SIGS = {
     "oracle_element": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dp]),
     "oracle_pair_block": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
     "oracle_bintgs": (None, [ctypes.c_double, _dp]),
+    "oracle_local_overlaps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]),
     "oracle_last_error": (ctypes.c_char_p, []),
 }
 
@@ -206,6 +207,16 @@ def pair_block(za, zb, dvec, method="am1"):
         "e2a": e2a.reshape(4, 4),
         "s": s.reshape(4, 4),
     }
+
+
+def local_overlaps(za, zb, r, numeric=False, method="am1"):
+    """The five local-frame overlaps (s111, s211, s121, s221, s222) of the pair at distance r
+    (Bohr); numeric=True forces the prolate-spheroidal quadrature."""
+    out = np.zeros(5)
+    rc = lib().oracle_local_overlaps(_abi.METHOD[method], int(za), int(zb), float(r), 1 if numeric else 0, _p(out))
+    if rc:
+        raise RuntimeError(f"oracle_local_overlaps: {rc}")
+    return out
 
 
 def bintgs(x):

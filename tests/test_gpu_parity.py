@@ -168,7 +168,10 @@ def test_error_codes(gpu):
 
     r = gpu.scf([2, 1], [[0, 0, 0], [1.4, 0, 0]])
     assert r["status"] == _abi.ELEMENT_NOT_PARAMETERIZED
-    r = gpu.scf([35, 1], [[0, 0, 0], [2.7, 0, 0]])
+    # more than 8192 orbitals: refused before any device work
+    big = np.zeros((2049, 3))
+    big[:, 0] = 2.9 * np.arange(2049)
+    r = gpu.scf(np.full(2049, 6), big, want_matrices=False)
     assert r["status"] == _abi.UNSUPPORTED
     r = gpu.scf([8, 1, 1], [[0, 0, 0], [1.8, 0, 0], [-0.45, 1.75, 0]], multiplicity=2)
     assert r["status"] == _abi.INVALID_INPUT

@@ -184,3 +184,31 @@ def test_density_identities(oracle, ref_values):
     assert np.max(np.abs(f @ p - p @ f)) < 1e-6
     e = 0.5 * (np.sum(p * h) + np.sum(p * f))
     assert abs(e - r["electronic_ev"]) < 1e-11 * abs(e)
+
+
+def test_numerical_overlap_reproduces_closed_forms():
+    # the quadrature used for valence shells n >= 4 must give the closed-form overlaps where both
+    # exist (the reference checks the same: src/overlap.rs:718-747)
+    import oracle as O
+
+    worst = 0.0
+    for za, zb in [(1, 1), (6, 1), (6, 6), (8, 6), (7, 8), (16, 1), (16, 8), (17, 17), (14, 6)]:
+        for r in (1.2, 2.0, 2.8, 4.0, 6.5):
+            a = O.local_overlaps(za, zb, r)
+            q = O.local_overlaps(za, zb, r, numeric=True)
+            worst = max(worst, float(np.max(np.abs(a - q))))
+    assert worst < 1e-10, worst
+
+
+def test_hbr_runs_through_the_numerical_overlap():
+    # tests/molecules.rs:45-60: Br (valence n = 4) converges, Br negative, H positive
+    import oracle as O
+    from am1gpu import _abi
+
+    z = np.array([35, 1], dtype=np.int32)
+    x = _abi.angstrom_to_bohr(np.array([[0.0, 0.0, 0.0], [1.414, 0.0, 0.0]]))
+    r = O.scf(z, x, want_matrices=False)
+    assert r["status"] == 0 and r["converged"]
+    assert r["charges"][0] < 0.0 < r["charges"][1]
+    assert abs(float(np.sum(r["charges"]))) < 1e-6
+    assert abs(r["heat_of_formation_kcal"]) < 60.0
