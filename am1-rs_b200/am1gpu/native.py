@@ -241,6 +241,19 @@ def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
     return g
 
 
+def eigh_batch(mats):
+    """Eigendecompositions of a list of symmetric matrices in one ``am1gpu_symmetric_eigen_batch``
+    call: (status list, [(eigenvalues, eigenvector columns)])."""
+    ms = [np.ascontiguousarray(m, dtype=np.float64) for m in mats]
+    ns = (ctypes.c_int32 * len(ms))(*[m.shape[0] for m in ms])
+    ws = [np.zeros(m.shape[0]) for m in ms]
+    vs = [np.zeros_like(m) for m in ms]
+    arr = lambda xs: (_dp * len(xs))(*[x.ctypes.data_as(_dp) for x in xs])
+    st = (ctypes.c_int32 * len(ms))()
+    _abi.lib().am1gpu_symmetric_eigen_batch(len(ms), ns, arr(ms), arr(ws), arr(vs), st)
+    return list(st), list(zip(ws, vs))
+
+
 def eigh(a):
     a = np.ascontiguousarray(a, dtype=np.float64)
     n = a.shape[0]

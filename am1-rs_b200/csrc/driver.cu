@@ -1669,6 +1669,149 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_o
     return AM1GPU_OK;
 }
 
+// Many independent symmetric eigenproblems in one set of launches: the subsystem blocks of the
+// divide-and-conquer SCF (solve_subsystems, src/divide_conquer.rs:587-617), each of which the
+// reference diagonalises with its own symmetric_eigen call.  Every matrix gets the cluster Jacobi
+// job symmetric_eigen_one would give it (same cluster size, same arithmetic), the jobs are
+// grouped by cluster size and launched together, then sorted.  status[i] receives matrix i's
+// code; the return value is the first nonzero one.
+int symmetric_eigen_batch(int count, const int32_t* ns, const double* const* a, double* const* w, double* const* v, int32_t* status) {
+    g_err.clear();
+    if (count < 0 || (count > 0 && (!ns || !a || !w || !v))) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    int first = AM1GPU_OK;
+    std::string first_msg;
+    auto set = [&](int i, int code, const std::string& msg) {
+        if (status) status[i] = code;
+        if (code && !first) {
+            first = code;
+            first_msg = msg;
+        }
+    };
+    struct Item {
+        int i, n, npad, C;
+        size_t o_g, o_c, o_v, o_l, o_id, o_e, o_r;
+    };
+    std::vector<Item> items;
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        off = align256(off);
+        const size_t o2 = off;
+        off += bytes;
+        return o2;
+    };
+    for (int i = 0; i < count; ++i) {
+        const int n = ns[i];
+        set(i, AM1GPU_OK, "");
+        if (n < 0 || (n > 0 && (!a[i] || !w[i] || !v[i]))) {
+            set(i, AM1GPU_INVALID_INPUT, "matrix " + std::to_string(i) + ": null argument or negative size");
+            continue;
+        }
+        if (n == 0) continue;
+        bool finite = true;
+        for (long long k = 0; k < (long long)n * n && finite; ++k) finite = std::isfinite(a[i][k]);
+        if (!finite) {
+            set(i, AM1GPU_LINALG, "matrix " + std::to_string(i) + " handed to the eigensolver is not finite");
+            continue;
+        }
+        Item it{i, n, 0, 0};
+        if (!choose_cluster(n, &it.npad, &it.C)) {
+            set(i, AM1GPU_UNSUPPORTED, "matrix " + std::to_string(i) + " is larger than the cluster eigensolver's capacity");
+            continue;
+        }
+        const size_t nn = (size_t)n * n;
+        it.o_g = take(nn * 8);
+        it.o_c = take(nn * 8);
+        it.o_v = take((size_t)it.npad * n * 8);
+        it.o_l = take((size_t)it.npad * 8);
+        it.o_id = take((size_t)it.npad * 4);
+        it.o_e = take((size_t)n * 8);
+        it.o_r = take((size_t)n * 8);
+        items.push_back(it);
+    }
+    if (items.empty()) {
+        if (first) g_err = first_msg;
+        return first;
+    }
+    // cluster-size groups, largest clusters (and matrices) first, as the batched SCF orders them
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.C != y.C ? x.C > y.C : x.n > y.n; });
+    const int m = (int)items.size();
+    const size_t o_st = take(sizeof(MolState) * m), o_status = take(sizeof(int) * m), o_job = take(sizeof(EigJob) * m);
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    Workspace* ws;
+    rc = workspace(&ws, align256(off), align256(off));
+    if (rc) return rc;
+    char* D = ws->dpool;
+    char* Hh = ws->hpin;
+    Batch b;
+    b.buckets.clear();
+    for (int k = 0; k < m; ++k) {
+        const Item& it = items[k];
+        const int n = it.n;
+        const double* ak = a[it.i];
+        double* g = (double*)(Hh + it.o_g);
+        double* c = (double*)(Hh + it.o_c);
+        double* rmin = (double*)(Hh + it.o_r);
+        for (int r = 0; r < n; ++r) {
+            double bound = 0.0;
+            for (int q = 0; q < n; ++q) {
+                const double x = r >= q ? ak[(size_t)r * n + q] : ak[(size_t)q * n + r];  // lower triangle
+                g[(size_t)r * n + q] = x;
+                c[(size_t)r * n + q] = r == q ? 1.0 : 0.0;
+                if (r != q) bound += std::fabs(x);
+            }
+            rmin[r] = g[(size_t)r * n + r] - bound;
+        }
+        MolState* hs = (MolState*)(Hh + o_st) + k;
+        *hs = MolState{};
+        hs->active = 1;
+        EigJob* ej = (EigJob*)(Hh + o_job) + k;
+        *ej = EigJob{};
+        ej->Gt = (double*)(D + it.o_g);
+        ej->Ct = (double*)(D + it.o_c);
+        ej->Vs = (double*)(D + it.o_v);
+        ej->lam = (double*)(D + it.o_l);
+        ej->colid_out = (int*)(D + it.o_id);
+        ej->eps = (double*)(D + it.o_e);
+        ej->Ct_out = (double*)(D + it.o_c);
+        ej->rowmin = (double*)(D + it.o_r);
+        ej->n = n;
+        ej->npad = it.npad;
+        ej->mol = k;
+        const size_t sm = jacobi_smem_bytes(n, it.npad, it.C);
+        if (b.buckets.empty() || b.buckets.back().C != it.C) b.buckets.push_back({k, 0, it.C, 0});
+        b.buckets.back().count++;
+        b.buckets.back().smem = std::max(b.buckets.back().smem, sm);
+    }
+    std::memset(Hh + o_status, 0, sizeof(int) * m);
+    CK(cudaMemcpyAsync(D, Hh, align256(off), cudaMemcpyHostToDevice, ws->stream));
+    b.d_eig = (EigJob*)(D + o_job);
+    b.d_st = (MolState*)(D + o_st);
+    b.d_status = (int*)(D + o_status);
+    b.neig = m;
+    rc = launch_jacobi(b, ws, 1);
+    if (rc) return rc;
+    k_eig_sort<<<m, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(Hh, D, align256(off), cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaStreamSynchronize(ws->stream));
+    for (int k = 0; k < m; ++k) {
+        const Item& it = items[k];
+        const int n = it.n;
+        if (((int*)(Hh + o_status))[k]) {
+            set(it.i, AM1GPU_LINALG, "matrix " + std::to_string(it.i) + ": Jacobi eigensolver did not converge");
+            continue;
+        }
+        std::memcpy(w[it.i], Hh + it.o_e, sizeof(double) * n);
+        const double* ct = (const double*)(Hh + it.o_c);
+        for (int q = 0; q < n; ++q)
+            for (int r = 0; r < n; ++r) v[it.i][(size_t)r * n + q] = ct[(size_t)q * n + r];
+    }
+    if (first) g_err = first_msg;
+    return first;
+}
+
 }  // namespace am1
 
 // A resident batch: inputs uploaded once, device memory and stream owned by the handle.
@@ -1755,6 +1898,11 @@ int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* 
 
 int am1gpu_g_matrix_batch(const am1gpu_molecule* mol, int32_t method, int32_t nrhs, const double* densities, double* g) {
     return am1::g_matrix_batch(mol, method, nrhs, densities, g);
+}
+
+int am1gpu_symmetric_eigen_batch(int32_t count, const int32_t* n, const double* const* a, double* const* w, double* const* v,
+                                 int32_t* status) {
+    return am1::symmetric_eigen_batch(count, n, a, w, v, status);
 }
 
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {

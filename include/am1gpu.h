@@ -171,6 +171,15 @@ int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* 
  */
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 
+/*
+ * count independent symmetric eigendecompositions in one call (each as am1gpu_symmetric_eigen,
+ * n[i] <= 448): replaces the per-subsystem symmetric_eigen calls of the divide-and-conquer SCF
+ * (solve_subsystems, src/divide_conquer.rs:587-617).  a[i], w[i], v[i] as above for matrix i;
+ * status[i] (may be NULL) receives its code, and the first nonzero one is returned.
+ */
+int am1gpu_symmetric_eigen_batch(int32_t count, const int32_t* n, const double* const* a, double* const* w,
+                                 double* const* v, int32_t* status);
+
 /* Message of the last failing call on this host thread ("" if none). */
 const char* am1gpu_last_error(void);
 

@@ -272,3 +272,24 @@ def test_eigensolver_density_path(tmp_path):
     env = dict(__import__("os").environ, AM1GPU_DENSITY="jacobi")
     r = subprocess.run([sys.executable, str(f)], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+def test_symmetric_eigen_batch(gpu):
+    # many small blocks in one call, as the divide-and-conquer subsystems are
+    # (src/divide_conquer.rs:587-617); each equals its solo am1gpu_symmetric_eigen, bit for bit
+    rng = np.random.default_rng(44)
+    sizes = [1, 2, 3, 7, 16, 33, 64, 100, 150, 200, 257, 320, 448, 5, 90]
+    mats = []
+    for n in sizes:
+        a = rng.standard_normal((n, n))
+        mats.append(a + a.T)
+    mats.append(np.array([[1.0, np.nan], [np.nan, 1.0]]))  # refused alone, the rest still solved
+    status, out = gpu.eigh_batch(mats)
+    from am1gpu import _abi
+
+    assert status[-1] == _abi.LINALG and all(s == 0 for s in status[:-1]), status
+    for a, (w, v), n in zip(mats, out, sizes):
+        assert np.max(np.abs(w - np.linalg.eigvalsh(a))) < 1e-10 * max(1.0, np.max(np.abs(w)))
+        assert np.max(np.abs(v @ np.diag(w) @ v.T - a)) < 1e-9
+        w1, v1 = gpu.eigh(a)
+        assert np.array_equal(w1, w) and np.array_equal(v1, v)
