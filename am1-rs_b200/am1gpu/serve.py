@@ -212,12 +212,14 @@ def _main():
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="arithmetic of the batched solves (mixed: TF32 purification in the early iterations)")
     args = ap.parse_args()
     reqs = W.config3(args.requests, args.rate, seed=2)
     from . import _abi
 
     native.ensure_loaded()
-    with ScfServer(workers=args.workers) as srv:
+    with ScfServer(workers=args.workers, precision=args.precision) as srv:
         # warm every worker's workspace once
         warm = [srv.submit(r.mol.numbers, _abi.angstrom_to_bohr(r.mol.xyz), r.mol.charge, r.mol.multiplicity) for r in reqs[:64]]
         for f in warm:
@@ -238,7 +240,7 @@ def _main():
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
         "plain_solves_per_s": plain, "batches": stats.batches, "mean_batch": float(np.mean(stats.batch_sizes)),
         "largest_batch": stats.largest_batch, "max_concurrent_batches": stats.max_concurrent_batches,
-        "max_in_flight_gb": stats.max_in_flight_bytes / 1e9, "workers": args.workers,
+        "max_in_flight_gb": stats.max_in_flight_bytes / 1e9, "workers": args.workers, "precision": args.precision,
     }
     print(json.dumps(line))
 
