@@ -241,6 +241,14 @@ def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
     return g
 
 
+def eigvalsh(a):
+    """Ascending eigenvalues of a symmetric matrix (up to 8192 rows), ``am1gpu_symmetric_eigenvalues``."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    w = np.zeros(a.shape[0])
+    _check(_abi.lib().am1gpu_symmetric_eigenvalues(a.shape[0], a.ctypes.data_as(_dp), w.ctypes.data_as(_dp)))
+    return w
+
+
 def eigh_batch(mats):
     """Eigendecompositions of a list of symmetric matrices in one ``am1gpu_symmetric_eigen_batch``
     call: (status list, [(eigenvalues, eigenvector columns)])."""

@@ -134,7 +134,7 @@ int device_ctx(DeviceCtx** out) {
         for (const void* f : {(const void*)k_tridiag_cl, (const void*)k_sp2_bounds_cl})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
                 return bad("large-matrix cluster attribute", err);
-        for (const void* f : {(const void*)k_tridiag_cl, (const void*)k_tridiag_big}) {  // 3 n doubles
+        for (const void* f : {(const void*)k_tridiag_cl, (const void*)k_tridiag_big, (const void*)k_tridiag_panel}) {
             cudaFuncAttributes fb{};
             if ((err = cudaFuncGetAttributes(&fb, f)) != cudaSuccess) return bad("large tridiagonalisation attributes", err);
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fb.sharedSizeBytes)) !=
@@ -148,6 +148,9 @@ int device_ctx(DeviceCtx** out) {
         if ((err = cudaFuncSetAttribute(k_sp2_step_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf32_smem_bytes())) !=
             cudaSuccess)
             return bad("tf32 tile kernel smem attribute", err);
+        for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8})
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
+                return bad("trailing-update smem attribute", err);
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
@@ -985,12 +988,55 @@ int launch_big_bounds(Batch& b, cudaStream_t s) {
 
 // Householder reduction of the matrices too large for a cluster's shared memory (the first
 // entries of d_tri, largest first)
-int launch_big_tridiag(Batch& b, cudaStream_t s) {
+// The whole-GPU reduction of one matrix: blocked (panels of TRP_B columns with tensor-core
+// trailing updates) unless AM1GPU_TRIDIAG=unblocked selects the one-column-per-step kernel (kept
+// for comparison).
+bool tridiag_blocked() {
+    static const bool v = [] {
+        const char* e = std::getenv("AM1GPU_TRIDIAG");
+        return !(e && std::strcmp(e, "unblocked") == 0);
+    }();
+    return v;
+}
+
+int blocked_tridiag(TriJob tj, cudaStream_t s, int64_t* launches) {
+    const int n = tj.n;
+    tj.work = (double*)(((uintptr_t)tj.work + 15) & ~(uintptr_t)15);  // 16-byte copies of V, W
+    CK(cudaMemcpyAsync(tj.W, tj.A, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+    const size_t smem = tridiag_panel_smem_bytes(n);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel, TRIB_THREADS, smem));
+    const int grid = std::min(per_sm, 2) * g_sms;
+    if (per_sm < 1 || (long long)grid * 64 < n) return fail(AM1GPU_DEVICE_ERROR, "blocked tridiagonalisation does not fit the GPU");
+    for (int k = 0; k < n - 1; k += TRP_B) {
+        int bw = std::min(TRP_B, n - 1 - k);
+        void* args[] = {&tj, &k, &bw};
+        CK(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel, dim3(grid), dim3(TRIB_THREADS), args, smem, s));
+        ++*launches;
+        if (k + bw < n - 1) {  // not the last panel: the trailing update of [k + TRP_B, n)
+            const int t0 = k + TRP_B, nt = (n - t0 + 64 - 1) / 64;
+            const unsigned tiles = (unsigned)nt * (nt + 1) / 2;
+            if (n % 2 == 0) k_tridiag_syr2k16<<<tiles, 128, dgemm_smem_bytes(), s>>>(tj, t0);  // 16-byte copies
+            else k_tridiag_syr2k8<<<tiles, 128, dgemm_smem_bytes(), s>>>(tj, t0);
+            CK(cudaGetLastError());
+            ++*launches;
+        }
+    }
+    return AM1GPU_OK;
+}
+
+int launch_big_tridiag(Batch& b, cudaStream_t s, int64_t* launches) {
     const int count = (int)b.tri_big.size();
     if (count == 0) return AM1GPU_OK;
     const int k = big_split(count, [&](int i) { return b.tri_big[i].n; });
-    for (int i = 0; i < k; ++i) {  // one cooperative launch per matrix, as many CTAs as fit at once
+    for (int i = 0; i < k; ++i) {  // the whole GPU per matrix
+        if (tridiag_blocked()) {
+            int rc = blocked_tridiag(b.tri_big[i], s, launches);
+            if (rc) return rc;
+            continue;
+        }
         TriJob arg = b.tri_big[i];
+        ++*launches;
         const size_t smem = tridiag_big_smem_bytes(arg.n);
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_big, TRIB_THREADS, smem));
@@ -1004,6 +1050,7 @@ int launch_big_tridiag(Batch& b, cudaStream_t s) {
         void* args[] = {&jobs};
         CK(launch_clusters((const void*)k_tridiag_cl, big_cluster(count - k, g_sms), count - k, TRIB_THREADS,
                            tridiag_big_smem_bytes(b.tri_big[k].n), s, args));
+        ++*launches;
     }
     return AM1GPU_OK;
 }
@@ -1170,13 +1217,12 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     k_final_energy<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, nblk);
     // eigenvalues of the last F* (mo_energies, HOMO/LUMO): tridiagonalisation + bisection
     if ((rc = launch_tridiag(b, ws))) return rc;
-    if ((rc = launch_big_tridiag(b, s))) return rc;
+    int64_t big_tri_launches = 0;
+    if ((rc = launch_big_tridiag(b, s, &big_tri_launches))) return rc;
     k_bisect<<<dim3(njobs, cdiv(b.maxn, 512)), 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
-    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() +
-                                         big_launches(big_split((int)b.tri_big.size(), [&](int i) { return b.tri_big[i].n; }),
-                                                      (int)b.tri_big.size()));
+    run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() + (int)big_tri_launches);
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_FINAL, ph))) return rc;
     size_t t1;
@@ -1669,6 +1715,66 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_o
     return AM1GPU_OK;
 }
 
+// Eigenvalues only, of one symmetric matrix of up to kMaxAo rows: the final-spectrum path of the
+// SCF (on-chip cluster reduction while the matrix fits a cluster's shared memory, a cluster over
+// global memory below kBigGridN rows, the blocked whole-GPU reduction above), then bisection.
+int symmetric_eigenvalues_one(int n, const double* a, double* w) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && (!a || !w))) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (n == 0) return AM1GPU_OK;
+    if (n > kMaxAo) return fail(AM1GPU_UNSUPPORTED, "matrix with " + std::to_string(n) + " rows exceeds " + std::to_string(kMaxAo));
+    for (long long i = 0; i < (long long)n * n; ++i)
+        if (!std::isfinite(a[i])) return fail(AM1GPU_LINALG, "the matrix handed to the eigensolver is not finite");
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    const size_t nn = (size_t)n * n;
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        off = align256(off);
+        const size_t o2 = off;
+        off += bytes;
+        return o2;
+    };
+    const size_t o_a = take(nn * 8), o_w = take(nn * 8), o_k = take(std::max(nn, (size_t)4 * TRP_B * n + 2 * n + 1024 * (2 * TRP_B + 2)) * 8),
+                 o_d = take((size_t)n * 8), o_e = take((size_t)n * 8), o_eps = take((size_t)n * 8), o_job = take(sizeof(TriJob));
+    Workspace* ws;
+    rc = workspace(&ws, align256(off), align256(o_k));
+    if (rc) return rc;
+    char* D = ws->dpool;
+    TriJob tj{};
+    tj.A = (const double*)(D + o_a);
+    tj.W = (double*)(D + o_w);
+    tj.work = (double*)(D + o_k);
+    tj.d = (double*)(D + o_d);
+    tj.e = (double*)(D + o_e);
+    tj.eps = (double*)(D + o_eps);
+    tj.n = n;
+    tj.mol = 0;
+    std::memcpy(ws->hpin, a, nn * 8);  // the matrix through pinned staging, then the job record
+    std::memcpy(ws->hpin + align256(nn * 8), &tj, sizeof tj);
+    CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, ws->stream));
+    CK(cudaMemcpyAsync(D + o_job, ws->hpin + align256(nn * 8), sizeof tj, cudaMemcpyHostToDevice, ws->stream));
+    Batch b;
+    b.d_tri = (TriJob*)(D + o_job);
+    b.maxn = n;
+    const int C = tridiag_cluster(n);
+    if (C) {
+        b.tri_buckets = {{0, 1, C, tridiag_smem_bytes(n, C)}};
+        rc = launch_tridiag(b, ws);
+    } else {
+        b.tri_big = {tj};
+        int64_t launches = 0;
+        rc = launch_big_tridiag(b, ws->stream, &launches);
+    }
+    if (rc) return rc;
+    k_bisect<<<dim3(1, cdiv(n, 512)), 512, 2 * sizeof(double) * n, ws->stream>>>(b.d_tri, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(w, D + o_eps, (size_t)n * 8, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaStreamSynchronize(ws->stream));
+    return AM1GPU_OK;
+}
+
 // Many independent symmetric eigenproblems in one set of launches: the subsystem blocks of the
 // divide-and-conquer SCF (solve_subsystems, src/divide_conquer.rs:587-617), each of which the
 // reference diagonalises with its own symmetric_eigen call.  Every matrix gets the cluster Jacobi
@@ -1904,6 +2010,8 @@ int am1gpu_symmetric_eigen_batch(int32_t count, const int32_t* n, const double* 
                                  int32_t* status) {
     return am1::symmetric_eigen_batch(count, n, a, w, v, status);
 }
+
+int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w) { return am1::symmetric_eigenvalues_one(n, a, w); }
 
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {
     return am1::symmetric_eigen_one(n, a, w, v);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "am1gpu_internal.h"
+#include "dmma_gemm.cuh"
 #include "kernels.h"
 
 namespace am1 {
@@ -427,5 +428,238 @@ __global__ void k_bisect(const TriJob* __restrict__ jobs, const int* __restrict_
         jb.eps[k] = 0.5 * (lo + hi);
     }
 }
+
+}  // namespace am1
+
+namespace am1 {
+
+// ---------------------------------------------------------------------------------------------
+// Blocked Householder reduction for the largest matrices (the whole GPU per matrix): panels of
+// TRP_B columns, each reduced by one cooperative launch (k_tridiag_panel, the DLATRD scheme) with
+// the trailing matrix left untouched, then the trailing matrix updated once per panel,
+// A <- A - V W^T - W V^T, by a rank-2 TRP_B product on the FP64 tensor cores (k_tridiag_syr2k*).
+// Per column the panel kernel reads the trailing matrix once (A v) instead of reading and writing
+// it (the unblocked k_tridiag_big), and the writes happen once per panel.
+//
+// Column c = k + j of the panel (V, W: the panel's reflectors and their w vectors so far, rows
+// > c; V_c., W_c. row c of them):
+//   x_i  = A_ic - sum_{l<j} (V_il W_cl + W_il V_cl)               i >= c   (column c, updated)
+//   d_c  = x_c;  alpha = |x_{c+1:}|,  v = x_{c+1:} + sign(x_{c+1}) alpha e_1,
+//   beta = 1 / (alpha (alpha + |x_{c+1}|)),  e_c = -sign(x_{c+1}) alpha
+//   p    = beta (A v - V (W^T v) - W (V^T v))                      over rows and columns > c
+//   w    = p - (beta/2)(p . v) v,  V_.j = v,  W_.j = w
+// W^T v and V^T v come from W^T x and V^T x (summed with |x|^2 in the first grid barrier) and
+// row c+1 of W and V.  Two grid barriers per column: row c+1's newest entries of V and W, which
+// its owner writes after the second barrier, every CTA forms itself (v_{c+1} and p_{c+1} are
+// known to all by then) for the next column's first phase.  Rows are cyclic over the CTAs (r % G).
+// Scratch (job.work, 16-byte aligned): VW[n][2B] = [V | W] | WVt[2B][n] = [W | V]^T | x[n] |
+// p[n] | share[G][2B + 2]; dynamic shared memory: v (n doubles) and W^T v, V^T v.
+// ---------------------------------------------------------------------------------------------
+
+size_t tridiag_panel_smem_bytes(int n) { return sizeof(double) * ((size_t)n + 2 * TRP_B); }
+
+__global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_panel(TriJob jb, int k, int bw) {
+    cg::grid_group grid = cg::this_grid();
+    const int G = (int)gridDim.x, gi = (int)blockIdx.x;
+    const int n = jb.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = TRIB_THREADS / 32;
+    constexpr int B = TRP_B, SW = 2 * TRP_B + 2;
+    double* A = jb.W;
+    double* VW = jb.work;
+    double* WVt = VW + (size_t)2 * B * n;
+    double* xb = WVt + (size_t)2 * B * n;
+    double* pb = xb + n;
+    double* share = pb + n;
+    extern __shared__ double psh[];
+    double* sv = psh;      // v, rows c+1..n-1
+    double* st = psh + n;  // [0, B): W^T v;  [B, 2B): V^T v
+    __shared__ double xr[64];  // this CTA's x_i of the current column (its rows > c, at most 64 of them)
+    __shared__ int xi_row[64];
+    __shared__ double red[NW];
+    // the panel's V and W on this CTA's own rows (row gi + q G in slot q), kept here as they are
+    // formed: the per-column corrections read them from shared memory, not global
+    __shared__ double svw[64][2 * TRP_B];
+    __shared__ double rowc[2];  // V and W of row c in the previous column (formed locally)
+    __shared__ double red4[4][NW];
+    for (int j = 0; j < bw; ++j) {
+        const int c = k + j;
+        __syncthreads();  // own rows' V, W of the previous column, and rowc, are written
+        // ---- phase 1: column c for own rows i >= c, and this CTA's shares of |x|^2, W^T x, V^T x
+        const int first = c + ((gi - c % G) % G + G) % G;  // first own row >= c
+        int nr = 0;
+        for (int i = first; i < n; i += G) ++nr;  // own rows >= c (<= 64: n <= 8192 and G >= 128)
+        const int q0 = (first - gi) / G;  // slot of the first own row >= c
+        if (tid < nr) {
+            const int i = first + tid * G;
+            const double* Vi = svw[q0 + tid];
+            const double* Vc = VW + (size_t)c * 2 * B;
+            double x = __ldcg(A + (size_t)i * n + c);
+            for (int l = 0; l < j; ++l) {
+                // row c's entries of the previous column are not yet visible from its owner
+                const double vc = l + 1 == j ? rowc[0] : __ldcg(Vc + l), wc = l + 1 == j ? rowc[1] : __ldcg(Vc + B + l);
+                x -= Vi[l] * wc + Vi[B + l] * vc;
+            }
+            xr[tid] = x;
+            xi_row[tid] = i;
+            xb[i] = x;
+            if (i == c) jb.d[c] = x;
+        }
+        __syncthreads();
+        if (tid < 2 * j + 1) {  // share slot 0: |x_{>c}|^2; 1..j: W^T x; j+1..2j: V^T x
+            double s = 0.0;
+            for (int q = 0; q < nr; ++q) {
+                const int i = xi_row[q];
+                if (i <= c) continue;
+                const double x = xr[q];
+                if (tid == 0) s += x * x;
+                else if (tid <= j) s += svw[q0 + q][B + (tid - 1)] * x;
+                else s += svw[q0 + q][tid - 1 - j] * x;
+            }
+            share[(size_t)gi * SW + tid] = s;
+        }
+        grid.sync();
+        // ---- the reflector (every CTA forms the same values: fixed-order sums of the shares)
+        const bool has_next = c + 2 < n;
+        const double x1 = __ldcg(xb + c + 1);
+        if (!has_next) {  // the last 2 x 2 block: e[n-2], and d[n-1] with this panel's updates
+            if (gi == (n - 1) % G && tid == 0) {
+                jb.e[c] = x1;
+                double dn = __ldcg(A + (size_t)(n - 1) * n + n - 1);
+                const double* Vn = VW + (size_t)(n - 1) * 2 * B;
+                for (int l = 0; l < j; ++l) dn -= 2.0 * __ldcg(Vn + l) * __ldcg(Vn + B + l);
+                jb.d[n - 1] = dn;
+            }
+            break;
+        }
+        double nrm2 = 0.0;
+        for (int q = lane; q < G; q += 32) nrm2 += __ldcg(share + (size_t)q * SW);
+        for (int o = 16; o > 0; o >>= 1) nrm2 += __shfl_xor_sync(0xffffffffu, nrm2, o);
+        const double alpha = sqrt(nrm2);
+        const double sg = x1 >= 0.0 ? 1.0 : -1.0;
+        const double beta = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x1)));
+        const double* V1 = VW + (size_t)(c + 1) * 2 * B;
+        // W^T v and V^T v: slot s < 2j summed over the CTAs by one warp, lane-strided in a fixed
+        // order (as group_share_sum), plus the e_{c+1} part of v = x + sg alpha e_{c+1}
+        for (int sl = warp; sl < 2 * j; sl += NW) {
+            double t = 0.0;
+            for (int q = lane; q < G; q += 32) t += __ldcg(share + (size_t)q * SW + 1 + sl);
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) {
+                const int l = sl < j ? sl : sl - j;
+                t += sg * alpha * (sl < j ? __ldcg(V1 + B + l) : __ldcg(V1 + l));
+                st[sl < j ? l : B + l] = t;
+            }
+        }
+        for (int i = c + 1 + tid; i < n; i += TRIB_THREADS) sv[i] = __ldcg(xb + i);
+        __syncthreads();
+        if (tid == 0) sv[c + 1] = x1 + sg * alpha;
+        __syncthreads();
+        // ---- phase 2a: p_i for own rows i > c, this CTA's share of p . v.  Rows go in groups of
+        // four; every thread takes a stride of the columns for all four (many loads in flight),
+        // and the partial sums are reduced over the CTA in a fixed order.
+        double part = 0.0;
+        for (int g0 = first > c ? 0 : 1; g0 < nr; g0 += 4) {
+            const int gr = min(4, nr - g0);
+            const double* Ar[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) Ar[u] = A + (size_t)(first + (g0 + (u < gr ? u : 0)) * G) * n;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+            for (int m = c + 1 + tid; m < n; m += TRIB_THREADS) {
+                const double vm = sv[m];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u] = fma(__ldcg(Ar[u] + m), vm, acc[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                for (int o = 16; o > 0; o >>= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
+            if (lane == 0)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) red4[u][warp] = acc[u];
+            __syncthreads();
+            if (tid < gr) {
+                const int q = g0 + tid, i = first + q * G;
+                double t = 0.0;
+                for (int w = 0; w < NW; ++w) t += red4[tid][w];
+                const double* Vi = svw[q0 + q];
+                for (int l = 0; l < j; ++l) t -= Vi[l] * st[l] + Vi[B + l] * st[B + l];
+                const double pi = beta * t;
+                pb[i] = pi;
+                part += pi * sv[i];
+            }
+            __syncthreads();
+        }
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int q = 0; q < NW; ++q) t += red[q];
+            share[(size_t)gi * SW + SW - 1] = t;
+        }
+        grid.sync();
+        // ---- phase 2b: w = p - kk v for own rows i > c; column j of V and W in both layouts
+        double pv = 0.0;
+        for (int q = lane; q < G; q += 32) pv += __ldcg(share + (size_t)q * SW + SW - 1);
+        for (int o = 16; o > 0; o >>= 1) pv += __shfl_xor_sync(0xffffffffu, pv, o);
+        const double kk = 0.5 * beta * pv;
+        if (tid < nr) {
+            const int i = first + tid * G;
+            if (i > c) {
+                const double v = sv[i], w = __ldcg(pb + i) - kk * v;
+                svw[q0 + tid][j] = v;
+                svw[q0 + tid][B + j] = w;
+                VW[(size_t)i * 2 * B + j] = v;
+                VW[(size_t)i * 2 * B + B + j] = w;
+                WVt[(size_t)j * n + i] = w;
+                WVt[(size_t)(B + j) * n + i] = v;
+            }
+        }
+        if (gi == c % G && tid == 0) jb.e[c] = alpha == 0.0 ? 0.0 : -sg * alpha;
+        if (tid == 0) {  // row c+1's entries of this column, for the next column's phase 1
+            rowc[0] = sv[c + 1];
+            rowc[1] = __ldcg(pb + c + 1) - kk * sv[c + 1];
+        }
+    }
+}
+
+// A[t0 + r][t0 + q] -= (V W^T + W V^T)[t0 + r][t0 + q] over the upper-triangle 64 x 64 tiles of the
+// trailing block (t0 = k + TRP_B), mirrored: C = [V | W][rows] . [W | V]^T[:, cols], K = 2 TRP_B.
+template <bool PAIRS>
+__device__ __forceinline__ void syr2k_body(TriJob jb, int t0) {
+    extern __shared__ __align__(16) double dsm[];
+    const int n = jb.n, T = n - t0;
+    const int nt = (T + DG_TILE - 1) / DG_TILE;
+    int rem = blockIdx.x, tm = 0;
+    while (rem >= nt - tm) {
+        rem -= nt - tm;
+        ++tm;
+    }
+    const int tn = tm + rem;
+    const int m0 = tm * DG_TILE, n0 = tn * DG_TILE;
+    const double* VW = jb.work;
+    const double* WVt = VW + (size_t)2 * TRP_B * n;
+    const bool compute = dg_quarter_on(m0, n0, T, T, tm == tn);
+    double acc[2][4][4];
+    dg_mainloop<PAIRS>(dsm, VW + (size_t)t0 * 2 * TRP_B, 2 * TRP_B, WVt + t0, n, T, T, 2 * TRP_B, m0, n0, acc, compute);
+    double* A = jb.W + (size_t)t0 * n + t0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = m0 + dg_row(i, e), c = n0 + dg_col(j, e);
+                if (compute && r <= c && c < T) {
+                    const double y = A[(size_t)r * n + c] - acc[i][j][e];
+                    A[(size_t)r * n + c] = y;
+                    if (r < c) A[(size_t)c * n + r] = y;
+                }
+            }
+}
+
+__global__ void __launch_bounds__(DG_THREADS, 4) k_tridiag_syr2k16(TriJob jb, int t0) { syr2k_body<true>(jb, t0); }
+__global__ void __launch_bounds__(DG_THREADS, 4) k_tridiag_syr2k8(TriJob jb, int t0) { syr2k_body<false>(jb, t0); }
 
 }  // namespace am1

@@ -167,6 +167,17 @@ constexpr int TRIB_THREADS = 512;
 __global__ void k_tridiag_big(TriJob job);
 __global__ void k_tridiag_cl(const TriJob* jobs);
 size_t tridiag_big_smem_bytes(int n);
+// blocked reduction of one large matrix (job.W, a copy of job.A): for each panel of TRP_B columns
+// starting at k (bw columns; the last panel ends at column n - 2), one cooperative launch of
+// k_tridiag_panel (tridiag_panel_smem_bytes(n); grid <= co-resident CTAs and >= n / 64), then,
+// unless it was the last panel, the trailing update over the upper tiles of [k + TRP_B, n)
+// (k_tridiag_syr2k16 when n is even, else ...8; dgemm_smem_bytes()).  job.work: 16-byte aligned,
+// 4 TRP_B n + 2 n + grid (2 TRP_B + 2) doubles.
+constexpr int TRP_B = 32;
+__global__ void k_tridiag_panel(TriJob job, int k, int bw);
+__global__ void k_tridiag_syr2k16(TriJob job, int t0);
+__global__ void k_tridiag_syr2k8(TriJob job, int t0);
+size_t tridiag_panel_smem_bytes(int n);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
 #ifdef __CUDACC__

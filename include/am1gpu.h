@@ -172,6 +172,14 @@ int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* 
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 
 /*
+ * Eigenvalues only (ascending), for a symmetric matrix of up to 8192 rows: the first half of
+ * symmetric_eigen (src/linalg.rs:276-331), by the SCF's final-spectrum path (Householder
+ * tridiagonalisation, blocked with FP64 tensor-core trailing updates from 2048 rows, then Sturm
+ * bisection).  a is n*n row-major; non-finite input returns AM1GPU_LINALG.
+ */
+int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
+
+/*
  * count independent symmetric eigendecompositions in one call (each as am1gpu_symmetric_eigen,
  * n[i] <= 448): replaces the per-subsystem symmetric_eigen calls of the divide-and-conquer SCF
  * (solve_subsystems, src/divide_conquer.rs:587-617).  a[i], w[i], v[i] as above for matrix i;

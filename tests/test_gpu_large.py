@@ -97,3 +97,17 @@ def test_many_large_molecules_match_solo(gpu):
         assert solo["iterations"] == g["iterations"]
         assert abs(solo["heat_of_formation_kcal"] - g["heat_of_formation_kcal"]) < 1e-8
         assert np.max(np.abs(solo["mo_energies"] - g["mo_energies"])) < 1e-9
+
+
+@pytest.mark.parametrize("n", [300, 1000, 2050, 3001, 4096])
+def test_eigenvalues_of_large_matrices(gpu, n):
+    # the final-spectrum path on its own: on-chip cluster (300), cluster over global memory (1000),
+    # blocked whole-GPU reduction with tensor-core trailing updates (2050, 4096; 3001 odd: 8-byte
+    # copies), then bisection; against LAPACK through numpy
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n))
+    a = (a + a.T) * 0.5 + np.diag(np.linspace(-3.0, 3.0, n))
+    w = gpu.eigvalsh(a)
+    ref = np.linalg.eigvalsh(a)
+    assert np.all(np.diff(w) >= 0.0)
+    assert np.max(np.abs(w - ref)) < 1e-10 * max(1.0, float(np.max(np.abs(ref))))
