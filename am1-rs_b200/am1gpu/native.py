@@ -166,6 +166,11 @@ def last_call_stats() -> dict:
     return _abi.stats_dict(st)
 
 
+def set_stream_priority(priority: int) -> None:
+    """CUDA priority of this host thread's stream (0 default, negative higher)."""
+    _check(_abi.lib().am1gpu_set_stream_priority(int(priority)))
+
+
 def set_timing(enable: bool) -> None:
     _abi.lib().am1gpu_set_timing(1 if enable else 0)
 

@@ -9,6 +9,11 @@ the same time on the device, so the work of different batches overlaps there.  I
 every molecule keeps its own SCF trajectory and convergence test and retires in place, so a
 result is the same whether the molecule was solved alone or in any mix (tested).
 
+With ``small_lane`` set, requests of at most that many orbitals go to a lane of their own, served
+by ``small_workers`` further threads: a small molecule then waits for other small ones, not behind a
+batch of 1000-orbital molecules (the lanes share the device, each batch on its own stream, and the
+small lane's streams have the higher CUDA priority).
+
 The budget is a fraction of the free device memory when the server starts; each request is
 charged an estimate of its device footprint (the per-channel matrix slots, the packed DIIS
 histories and the integral store).  The library's per-thread device pool only grows, so one
@@ -29,6 +34,12 @@ import time
 from dataclasses import dataclass, field
 
 import numpy as np
+
+
+def orbitals(numbers) -> int:
+    """Valence orbitals of a molecule (4 per heavy atom, 1 per hydrogen)."""
+    z = np.asarray(numbers)
+    return int(4 * np.count_nonzero(z != 1) + np.count_nonzero(z == 1))
 
 
 def device_bytes(numbers, multiplicity: int = 1) -> int:
@@ -70,25 +81,33 @@ class ScfServer:
     """
 
     def __init__(self, workers: int = 3, max_batch: int = 2048, budget_bytes: int | None = None,
-                 budget_fraction: float = 0.7, solve=None, **opts):
+                 budget_fraction: float = 0.7, solve=None, small_lane: int | None = None, small_workers: int = 2,
+                 **opts):
+        self._lane_start = None
         if solve is None:
             from . import native
 
             def solve(mols, _o=opts):
                 return native.scf_batch(mols, want_matrices=False, **_o)
+
+            # the small-request lane's streams go first on the SMs
+            self._lane_start = lambda lane: native.set_stream_priority(-1 if lane == 1 else 0)
         self._solve = solve
         if budget_bytes is None:
             budget_bytes = int(budget_fraction * _free_device_bytes())
         self.budget = int(budget_bytes)
-        self.share = self.budget // max(1, int(workers))
+        self.small_lane = small_lane
+        lanes = [0] * int(workers) + ([1] * int(small_workers) if small_lane is not None else [])
+        self.share = self.budget // max(1, len(lanes))
         self.max_batch = int(max_batch)
-        self._queue: collections.deque[_Pending] = collections.deque()
+        self._queues: list[collections.deque[_Pending]] = [collections.deque(), collections.deque()]
         self._cv = threading.Condition()
         self._in_flight = 0
         self._running_batches = 0
         self._closed = False
         self.stats = ServerStats()
-        self._threads = [threading.Thread(target=self._worker, name=f"scf-worker-{i}", daemon=True) for i in range(workers)]
+        self._threads = [threading.Thread(target=self._worker, args=(lane,), name=f"scf-worker-{i}", daemon=True)
+                         for i, lane in enumerate(lanes)]
         for t in self._threads:
             t.start()
 
@@ -97,11 +116,12 @@ class ScfServer:
         fut: concurrent.futures.Future = concurrent.futures.Future()
         p = _Pending((np.asarray(numbers, dtype=np.int32), np.asarray(xyz_bohr, dtype=np.float64), float(charge), int(multiplicity)),
                      device_bytes(numbers, multiplicity), fut, time.perf_counter())
+        lane = 1 if self.small_lane is not None and orbitals(numbers) <= self.small_lane else 0
         with self._cv:
             if self._closed:
                 raise RuntimeError("server closed")
-            self._queue.append(p)
-            self._cv.notify()
+            self._queues[lane].append(p)
+            self._cv.notify_all()
         return fut
 
     def close(self, wait: bool = True) -> None:
@@ -119,24 +139,27 @@ class ScfServer:
         self.close()
 
     # -- scheduling --------------------------------------------------------------------------
-    def _take(self) -> list[_Pending]:
-        """Pending requests that fit the budget, in arrival order (called with the lock held)."""
+    def _take(self, lane: int) -> list[_Pending]:
+        """The lane's pending requests that fit the budget, in arrival order (lock held)."""
+        q = self._queues[lane]
         batch: list[_Pending] = []
         room = min(self.budget - self._in_flight, self.share)
-        while self._queue and len(batch) < self.max_batch:
-            p = self._queue[0]
+        while q and len(batch) < self.max_batch:
+            p = q[0]
             if p.cost > room and (batch or self._in_flight > 0):
                 break  # wait for memory to free up
-            batch.append(self._queue.popleft())
+            batch.append(q.popleft())
             room -= p.cost
         return batch
 
-    def _worker(self) -> None:
+    def _worker(self, lane: int) -> None:
+        if self._lane_start is not None:
+            self._lane_start(lane)
         while True:
             with self._cv:
                 while True:
-                    batch = self._take()
-                    if batch or (self._closed and not self._queue):
+                    batch = self._take(lane)
+                    if batch or (self._closed and not self._queues[lane]):
                         break
                     self._cv.wait()
                 if not batch:
@@ -202,6 +225,13 @@ def run_stream(requests, server: ScfServer, time_scale: float = 1.0):
     return out, wall
 
 
+def _pct(lat_s):
+    if not lat_s:
+        return None
+    a = np.array(lat_s) * 1e3
+    return {"n": int(a.size), "p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99))}
+
+
 def _main():
     import argparse
 
@@ -212,6 +242,9 @@ def _main():
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--small-lane", type=int, default=None,
+                    help="orbital count up to which requests get their own lane (and --small-workers threads)")
+    ap.add_argument("--small-workers", type=int, default=2)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="arithmetic of the batched solves (mixed: TF32 purification in the early iterations)")
     args = ap.parse_args()
@@ -219,7 +252,8 @@ def _main():
     from . import _abi
 
     native.ensure_loaded()
-    with ScfServer(workers=args.workers, precision=args.precision) as srv:
+    with ScfServer(workers=args.workers, precision=args.precision, small_lane=args.small_lane,
+                   small_workers=args.small_workers) as srv:
         # warm every worker's workspace once
         warm = [srv.submit(r.mol.numbers, _abi.angstrom_to_bohr(r.mol.xyz), r.mol.charge, r.mol.multiplicity) for r in reqs[:64]]
         for f in warm:
@@ -241,6 +275,9 @@ def _main():
         "plain_solves_per_s": plain, "batches": stats.batches, "mean_batch": float(np.mean(stats.batch_sizes)),
         "largest_batch": stats.largest_batch, "max_concurrent_batches": stats.max_concurrent_batches,
         "max_in_flight_gb": stats.max_in_flight_bytes / 1e9, "workers": args.workers, "precision": args.precision,
+        "small_lane": args.small_lane, "small_workers": args.small_workers if args.small_lane is not None else 0,
+        "latency_ms_small": _pct([o[2] for o, r in zip(out, reqs) if args.small_lane is not None and orbitals(r.mol.numbers) <= args.small_lane]),
+        "latency_ms_large": _pct([o[2] for o, r in zip(out, reqs) if args.small_lane is not None and orbitals(r.mol.numbers) > args.small_lane]),
     }
     print(json.dumps(line))
 

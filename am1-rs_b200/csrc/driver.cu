@@ -167,6 +167,7 @@ int device_ctx(DeviceCtx** out) {
 // ---------------------------------------------------------------------------------------
 struct Mem {
     int dev = -1;
+    int priority = 0;  // the stream's CUDA priority (0 default, negative higher)
     cudaStream_t stream = nullptr;
     char* dpool = nullptr;
     size_t dcap = 0;
@@ -175,13 +176,17 @@ struct Mem {
     std::vector<cudaEvent_t> events;  // timing events, reused across calls
 };
 
+// Stream priority asked for by the calling host thread (am1gpu_set_stream_priority).
+thread_local int tl_priority = 0;
+
 int mem_ensure(Mem& w, size_t dbytes, size_t hbytes) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (w.dev != dev) {  // first use on this device
         w = Mem();
         w.dev = dev;
-        CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+        w.priority = tl_priority;
+        CK(cudaStreamCreateWithPriority(&w.stream, cudaStreamNonBlocking, w.priority));
     }
     if (dbytes > w.dcap) {
         if (w.dpool) CK(cudaFree(w.dpool));
@@ -2098,6 +2103,23 @@ void am1gpu_batch_destroy(am1gpu_batch* h) {
 }
 
 void am1gpu_set_timing(int32_t enable) { am1::g_timing.store(enable ? 1 : 0); }
+
+int am1gpu_set_stream_priority(int32_t priority) {
+    using namespace am1;
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));  // lo: least (0), hi: greatest (negative)
+    const int p = std::max(hi, std::min(lo, (int)priority));
+    tl_priority = p;
+    Mem& w = tl_mem;
+    if (w.stream && w.priority != p) {  // the thread's stream so far: replace it (nothing is in flight between calls)
+        CK(cudaStreamSynchronize(w.stream));
+        CK(cudaStreamDestroy(w.stream));
+        w.stream = nullptr;
+        CK(cudaStreamCreateWithPriority(&w.stream, cudaStreamNonBlocking, p));
+        w.priority = p;
+    }
+    return AM1GPU_OK;
+}
 
 int am1gpu_last_call_stats(am1gpu_call_stats* out) {
     if (!out) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");

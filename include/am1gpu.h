@@ -258,6 +258,14 @@ typedef struct {
 
 /* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */
 void am1gpu_set_timing(int32_t enable);
+
+/*
+ * CUDA priority of the calling host thread's stream, on which its calls run (0 the default,
+ * negative higher; clamped to the device's range).  A serving loop gives its small-request workers
+ * a higher priority, so their kernels go before long batches' on the SMs.  No counterpart in the
+ * reference (which has no device stream).
+ */
+int am1gpu_set_stream_priority(int32_t priority);
 int am1gpu_last_call_stats(am1gpu_call_stats* out);
 int am1gpu_batch_stats(const am1gpu_batch* batch, am1gpu_call_stats* out);
 

@@ -103,3 +103,31 @@ def test_no_request_is_lost_when_closing_with_a_queue():
     assert max(rec.batches) <= 4
     with pytest.raises(RuntimeError):
         srv.submit(*_mol(1))
+
+
+def test_small_lane_does_not_wait_behind_large_molecules():
+    # a solver whose time grows with the largest molecule of its batch: with a lane for small
+    # requests, they finish while the large batch is still running
+    done = {}
+
+    def solve(mols):
+        big = max(int(m[0].size) for m in mols)
+        time.sleep(0.6 if big > 60 else 0.01)
+        return [0] * len(mols), [{"natoms": int(m[0].size)} for m in mols]
+
+    with serve.ScfServer(workers=1, budget_bytes=1 << 40, solve=solve, small_lane=100, small_workers=1) as srv:
+        large = srv.submit(*_mol(40))  # 160 + 80 orbitals: the large lane
+        time.sleep(0.05)
+        t = time.perf_counter()
+        small = [srv.submit(*_mol(3)) for _ in range(5)]  # 18 orbitals each
+        for f in small:
+            f.result(timeout=30)
+        done["small"] = time.perf_counter() - t
+        assert not large.done()  # still running
+        assert large.result(timeout=30)[1]["natoms"] == 120
+    assert done["small"] < 0.4
+
+
+def test_orbital_count():
+    assert serve.orbitals(np.array([8, 1, 1])) == 6
+    assert serve.orbitals(np.array([6, 6, 1, 1, 1, 1, 1, 1])) == 14
