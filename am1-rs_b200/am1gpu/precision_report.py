@@ -73,10 +73,10 @@ def _main():
     args = ap.parse_args()
     native.ensure_loaded()
     if args.workload == "batch":
-        ms = W.config2()
+        ms = W.alkane_water_radical_batch()
         name = "4096 molecules (2048 alkanes n~U{1..40}, 2048 water clusters k~U{1..64}, seed 1) + 512 UHF alkyl radicals"
     else:
-        ms = [W.config4()]
+        ms = [W.water1024_cluster()]
         name = "1024 H2O, 3072 atoms, 6144 orbitals, seed 3"
     mols = [(m.numbers, _abi.angstrom_to_bohr(m.xyz), m.charge, m.multiplicity) for m in ms]
     for method in args.methods.split(","):

@@ -248,7 +248,7 @@ def _main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="arithmetic of the batched solves (mixed: TF32 purification in the early iterations)")
     args = ap.parse_args()
-    reqs = W.config3(args.requests, args.rate, seed=2)
+    reqs = W.serving_stream(args.requests, args.rate, seed=2)
     from . import _abi
 
     native.ensure_loaded()

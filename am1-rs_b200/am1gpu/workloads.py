@@ -1,4 +1,4 @@
-"""Seeded synthetic molecules for the benchmark configurations.
+"""Seeded synthetic molecules for the benchmark workloads.
 
 No public dataset is involved: every molecule is generated here with numpy's PCG64
 (``numpy.random.default_rng(seed)``), so the library, the CPU oracle and the CPU baseline
@@ -137,14 +137,14 @@ def alkane(n: int, rng: np.random.Generator, jitter: float = 0.05, radical: bool
 
 
 # ---------------------------------------------------------------------------------------
-# The benchmark configurations
+# The benchmark workloads
 # ---------------------------------------------------------------------------------------
-def config0() -> Mol:
+def water32_cluster() -> Mol:
     """32 H2O on a 4x4x2 grid, seed 0 (96 atoms, 192 AOs)."""
     return water_cluster(32, np.random.default_rng(0), grid=(4, 4, 2))
 
 
-def config1(n_alkanes: int = 2048, n_waters: int = 2048) -> list[Mol]:
+def alkane_water_batch(n_alkanes: int = 2048, n_waters: int = 2048) -> list[Mol]:
     """4096 molecules of uneven size, seed 1: alkanes n ~ U{1..40}, water clusters k ~ U{1..64}."""
     rng = np.random.default_rng(1)
     ns = rng.integers(1, 41, n_alkanes)
@@ -154,8 +154,8 @@ def config1(n_alkanes: int = 2048, n_waters: int = 2048) -> list[Mol]:
     return mols
 
 
-def config2(n_radicals: int = 512) -> list[Mol]:
-    """config1 plus 512 alkyl radicals (one terminal H removed, doublets) from the same stream."""
+def alkane_water_radical_batch(n_radicals: int = 512) -> list[Mol]:
+    """alkane_water_batch plus 512 alkyl radicals (one terminal H removed, doublets) from the same stream."""
     rng = np.random.default_rng(1)
     ns = rng.integers(1, 41, 2048)
     ks = rng.integers(1, 65, 2048)
@@ -166,7 +166,7 @@ def config2(n_radicals: int = 512) -> list[Mol]:
     return mols
 
 
-def config4() -> Mol:
+def water1024_cluster() -> Mol:
     """1024 H2O on a jittered 16x8x8 grid, seed 3 (3072 atoms, 6144 AOs)."""
     return water_cluster(1024, np.random.default_rng(3), grid=(16, 8, 8))
 
@@ -177,7 +177,7 @@ class Request:
     mol: Mol
 
 
-def config3(n_requests: int = 100_000, rate: float = 2000.0, seed: int = 2) -> list[Request]:
+def serving_stream(n_requests: int = 100_000, rate: float = 2000.0, seed: int = 2) -> list[Request]:
     """Open-loop Poisson stream: sizes log-uniform on [3, 600] atoms, RHF:UHF = 9:1."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, n_requests)

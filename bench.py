@@ -56,7 +56,7 @@ def parse():
 def workload(nmol):
     from am1gpu import workloads as W, _abi
 
-    mols = W.config1(n_alkanes=nmol // 2, n_waters=nmol - nmol // 2)
+    mols = W.alkane_water_batch(n_alkanes=nmol // 2, n_waters=nmol - nmol // 2)
     return [(m.numbers, _abi.angstrom_to_bohr(m.xyz), 0.0, 1) for m in mols]
 
 

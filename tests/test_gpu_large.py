@@ -48,11 +48,11 @@ def test_large_molecule_refuses_eigenvectors(gpu):
     assert abs(np.trace(r["density"]) - 8.0 * 80) < 1e-8
 
 
-def test_config4_full_size(gpu):
+def test_water1024_cluster_full_size(gpu):
     # 1024 waters, 6144 orbitals: size-independent checks (no CPU oracle at this size)
     from am1gpu import workloads as W, _abi
 
-    m = W.config4()
+    m = W.water1024_cluster()
     xyz = _abi.angstrom_to_bohr(m.xyz)
     a = gpu.scf(m.numbers, xyz, want_matrices=False)
     assert a["status"] == 0 and a["converged"]

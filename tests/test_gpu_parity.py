@@ -179,14 +179,14 @@ def test_error_codes(gpu):
     assert r["status"] == _abi.SCF_NOT_CONVERGED and r["iterations"] == 2 and np.isfinite(r["residual"])
 
 
-def test_config0_water32(gpu, oracle):
+def test_water32_cluster(gpu, oracle):
     from am1gpu import workloads as W, _abi
 
-    m = W.config0()
+    m = W.water32_cluster()
     xyz = _abi.angstrom_to_bohr(m.xyz)
     g = gpu.scf(m.numbers, xyz)
     o = oracle.scf(m.numbers, xyz)
-    _compare_scf(g, o, "config0")
+    _compare_scf(g, o, "water32_cluster")
 
 
 def test_batch_matches_oracle_and_solo(gpu, oracle):

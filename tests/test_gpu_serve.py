@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 def test_stream_results_equal_solo_runs(gpu):
     from am1gpu import serve, workloads as W, _abi
 
-    reqs = [r for r in W.config3(400, rate=1000.0, seed=5) if r.mol.numbers.size <= 150][:120]
+    reqs = [r for r in W.serving_stream(400, rate=1000.0, seed=5) if r.mol.numbers.size <= 150][:120]
     assert len(reqs) >= 60 and any(r.mol.multiplicity > 1 for r in reqs)
     with serve.ScfServer(workers=3, budget_bytes=8 << 30, small_lane=64, small_workers=2) as srv:
         m0 = reqs[0].mol

@@ -7,8 +7,8 @@ import numpy as np
 from am1gpu import workloads as W
 
 
-def test_config0_shape():
-    m = W.config0()
+def test_water32_cluster_shape():
+    m = W.water32_cluster()
     assert m.natoms == 96 and m.nao() == 192
     assert int(np.sum(m.numbers == 8)) == 32
     # O-H bonds of every monomer are 0.9572 A
@@ -18,9 +18,9 @@ def test_config0_shape():
         assert abs(np.linalg.norm(h2 - o) - 0.9572) < 1e-12
 
 
-def test_config1_is_deterministic_and_sized():
-    a = W.config1(n_alkanes=16, n_waters=16)
-    b = W.config1(n_alkanes=16, n_waters=16)
+def test_alkane_water_batch_is_deterministic_and_sized():
+    a = W.alkane_water_batch(n_alkanes=16, n_waters=16)
+    b = W.alkane_water_batch(n_alkanes=16, n_waters=16)
     assert len(a) == 32
     for x, y in zip(a, b):
         assert np.array_equal(x.numbers, y.numbers) and np.array_equal(x.xyz, y.xyz)
@@ -48,8 +48,8 @@ def test_alkane_geometry():
     assert r.multiplicity == 2 and r.natoms == 13
 
 
-def test_config3_stream():
-    reqs = W.config3(n_requests=200)
+def test_serving_stream():
+    reqs = W.serving_stream(n_requests=200)
     t = np.array([r.arrival_s for r in reqs])
     assert np.all(np.diff(t) > 0)
     uhf = sum(r.mol.multiplicity == 2 for r in reqs)
