@@ -1097,7 +1097,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     // mixed precision: every molecule starts with TF32 purification (k_converge ends that phase)
     const bool mixed = o.precision == AM1GPU_PRECISION_MIXED && density_mode() == 0;
     bool lowp_left = mixed;  // some molecule may still be in its TF32 phase
-    k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.nmol, mixed ? 1 : 0);
+    k_state_init<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_st, b.d_mols, b.nmol, mixed ? 1 : 0);
     run.launched(AM1GPU_PHASE_CORE);
     rc = launch_core(b, ws, dp, &run);
     if (rc) return rc;
@@ -1147,16 +1147,14 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 for (int step = 0; step < kSp2MaxSteps; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
-                    // FP64 steps (none in the first iteration of the mixed path: every molecule is
-                    // in its TF32 phase), then the TF32 steps while any molecule may be in it
+                    // FP64 steps (jobs in a TF32 run skip them), then the TF32 steps while any
+                    // molecule may be in its TF32 phase
                     int nl = 0;
-                    if (!(mixed && done == 0)) {
-                        launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-                            if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                            else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                            ++nl;
-                        });
-                    }
+                    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+                        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+                        ++nl;
+                    });
                     if (lowp_left) {
                         launch_tiles(b, s, [&](const GemmTile* t, int nt, bool) {
                             k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);

@@ -54,12 +54,15 @@ __global__ void k_sad_init(const MolDesc* __restrict__ mols, const int* __restri
 }
 
 // Fresh SCF state for every molecule of a batch (each run starts from the SAD guess).
-__global__ void k_state_init(MolState* __restrict__ st, int nmol, int lowp) {
+__global__ void k_state_init(MolState* __restrict__ st, const MolDesc* __restrict__ mols, int nmol, int lowp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nmol) return;
     MolState s{};
     s.active = 1;
-    s.lowp = lowp;
+    // mixed precision: every closed shell, and the open shells that keep the eigensolver fallback
+    // (at most kLowpMaxOpenShellAo orbitals).  Large radicals start FP64: a TF32 start left a few
+    // of them (3 of about 1900 in a 100 000-request stream) in a UHF basin that CDIIS did not leave.
+    s.lowp = lowp && (mols[i].nch == 1 || mols[i].nao <= kLowpMaxOpenShellAo);
     s.residual = __longlong_as_double(0x7ff0000000000000LL);  // +inf
     st[i] = s;
 }

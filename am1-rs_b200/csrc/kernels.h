@@ -204,7 +204,9 @@ __device__ __forceinline__ double group_share_sum(const double* share, int G) {
 __global__ void k_sad_init(const MolDesc* mols, const int* atom_mol, int natoms_total, const DevElem* params,
                            const int* atom_z, double* arena);
 __global__ void k_identity(const ChanJob* jobs);
-__global__ void k_state_init(MolState* st, int nmol, int lowp);
+// largest open-shell molecule (orbitals) that takes the mixed path's TF32 phase
+constexpr int kLowpMaxOpenShellAo = 448;
+__global__ void k_state_init(MolState* st, const MolDesc* mols, int nmol, int lowp);
 __global__ void k_post_fock(const ChanJob* jobs, const MolDesc* mols, const MolState* st, int nblk, int energy_only,
                             int force);
 __global__ void k_diis_solve(const MolDesc* mols, const ChanJob* jobs, const int* mol_job0, int nmol, MolState* st,

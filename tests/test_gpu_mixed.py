@@ -71,3 +71,23 @@ def test_plain_path_stays_fp64(gpu):
     z, x, q, m = _mols(32)[7]
     gpu.scf(z, x, q, m, precision="mixed", want_matrices=False)
     assert gpu.last_call_stats()["lowp_purification_steps"] == 0
+
+
+def test_large_radicals_stay_fp64_on_the_mixed_path(gpu):
+    # requests 58497, 77601 and 85316 of the serving stream (100 000 requests, seed 2): alkyl
+    # radicals of 595-1021 orbitals that a TF32 start left unconverged; open shells above 448
+    # orbitals now run FP64 on the mixed path, beside closed shells that take TF32
+    from am1gpu import workloads as W, _abi
+
+    rng = np.random.default_rng(58497)
+    rad = W.alkane(170, rng, radical=True)  # 1021 orbitals
+    clo = W.water_cluster(90, rng)          # 540 orbitals, closed shell
+    mols = [(rad.numbers, _abi.angstrom_to_bohr(rad.xyz), 0.0, 2), (clo.numbers, _abi.angstrom_to_bohr(clo.xyz), 0.0, 1)]
+    s64, r64 = gpu.scf_batch(mols, want_matrices=False)
+    smx, rmx = gpu.scf_batch(mols, want_matrices=False, precision="mixed")
+    st = gpu.last_call_stats()
+    assert all(x == 0 for x in s64) and all(x == 0 for x in smx), (s64, smx)
+    assert st["lowp_purification_steps"] > 0  # the closed shell still took TF32 steps
+    assert r64[0]["iterations"] == rmx[0]["iterations"]  # the radical ran FP64 throughout
+    assert abs(r64[0]["heat_of_formation_kcal"] - rmx[0]["heat_of_formation_kcal"]) < 1e-9
+    assert abs(r64[1]["heat_of_formation_kcal"] - rmx[1]["heat_of_formation_kcal"]) < DHF_BAR
