@@ -128,7 +128,7 @@ class Batch:
         return out
 
 
-def gradient(numbers, xyz_bohr, charge=0.0, multiplicity=1, **opts) -> dict:
+def scf_gradient(numbers, xyz_bohr, charge=0.0, multiplicity=1, **opts) -> dict:
     """SCF plus the closed-form nuclear gradient through ``am1gpu_gradient`` (positions in Bohr).
     Returns the SCF result dict with ``gradient`` (natoms x 3, eV/Bohr) and ``forces``."""
     mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
@@ -330,6 +330,39 @@ def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multipl
         "converged": r["converged"],
         "iterations": r["iterations"],
         "unrestricted": r["unrestricted"],
+    }
+
+
+def gradient(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
+             reference: str = "auto", method: str = "am1", electric_field=None) -> dict:
+    """Energy and closed-form nuclear gradient; the dictionary of am1_rs.native.gradient
+    (src/python.rs:201-277): positions in Angstrom, the gradient in Hartree/Bohr and eV/Angstrom
+    (forces = -gradient), with the SCF properties of the same run."""
+    if electric_field is not None:
+        raise ValueError("electric_field is not supported on the GPU path")
+    z, xyz = _prep(numbers, positions)
+    m = _method_name(method)
+    r = scf_gradient(z, xyz, charge, multiplicity, reference=_reference_name(reference), method=m)
+    _check(r["status"])
+    g = r["gradient"]
+    return {
+        "energy_hartree": r["energy_hartree"],
+        "energy_ev": r["energy_ev"],
+        "heat_of_formation_kcal": r["heat_of_formation_kcal"],
+        "electronic_ev": r["electronic_ev"],
+        "core_ev": r["core_ev"],
+        "homo_ev": None if np.isnan(r["homo_ev"]) else r["homo_ev"],
+        "lumo_ev": None if np.isnan(r["lumo_ev"]) else r["lumo_ev"],
+        "gradient_hartree_per_bohr": (g * _abi.EV_TO_HARTREE).tolist(),
+        "gradient_ev_per_angstrom": (g * _abi.ANGSTROM_TO_BOHR).tolist(),
+        "charges": [float(x) for x in r["charges"]],
+        "dipole_debye": r["dipole_debye"],
+        "dipole_magnitude": r["dipole_magnitude"],
+        "max_gradient_hartree_per_bohr": float(np.max(np.abs(g))) * _abi.EV_TO_HARTREE if g.size else 0.0,
+        "converged": r["converged"],
+        "iterations": r["iterations"],
+        "unrestricted": r["unrestricted"],
+        "method": m,
     }
 
 

@@ -63,7 +63,7 @@ def fd_gradient(energy, xyz, step=1e-4):
 @pytest.mark.parametrize("case", MOLS, ids=[m[0] for m in MOLS])
 def test_gradient_matches_fixed_density_differences(gpu, oracle, case):
     name, z, xyz, mult, method = case
-    g = gpu.gradient(z, xyz, 0.0, mult, method=method)
+    g = gpu.scf_gradient(z, xyz, 0.0, mult, method=method)
     assert g["status"] == 0 and g["converged"]
     s = gpu.scf(z, xyz, 0.0, mult, method=method, want_matrices=True)  # the same converged density
     assert s["energy_ev"] == g["energy_ev"]
@@ -83,7 +83,7 @@ def test_gradient_matches_fixed_density_differences(gpu, oracle, case):
 def test_gradient_matches_scf_differences(gpu, oracle, case):
     # the reference's own bar for its closed-form gradient (tests/rm1.rs:195-219)
     name, z, xyz, mult, method = case
-    g = gpu.gradient(z, xyz, 0.0, mult, method=method)
+    g = gpu.scf_gradient(z, xyz, 0.0, mult, method=method)
     ref = fd_gradient(lambda X: oracle.scf(z, X, 0.0, mult, method=method, want_matrices=False)["energy_ev"], xyz)
     assert np.max(np.abs(g["gradient"] - ref)) < 5e-5, (name, g["gradient"], ref)
 
@@ -101,6 +101,24 @@ def test_gradient_batch_matches_solo(gpu):
     status, res = gpu.gradient_batch(mols)
     assert all(s == 0 for s in status), status
     for m, r in zip(mols, res):
-        solo = gpu.gradient(*m)
+        solo = gpu.scf_gradient(*m)
         assert np.max(np.abs(solo["gradient"] - r["gradient"])) < 1e-9
         assert np.max(np.abs(r["gradient"].sum(axis=0))) < 1e-8
+
+
+def test_front_end_gradient_dictionary(gpu):
+    # am1_rs.native.gradient's dictionary (src/python.rs:201-277): Angstrom in, Hartree/Bohr and
+    # eV/Angstrom out, with the SCF properties
+    import numpy as np
+
+    from am1gpu import _abi
+
+    name, z, xyz, mult, method = MOLS[1]
+    d = gpu.gradient(z, xyz * 0.529167, method=method)
+    g = gpu.scf_gradient(z, xyz, method=method)["gradient"]
+    assert set(d) >= {"energy_hartree", "energy_ev", "heat_of_formation_kcal", "gradient_hartree_per_bohr",
+                      "gradient_ev_per_angstrom", "charges", "dipole_debye", "converged", "method",
+                      "max_gradient_hartree_per_bohr"}
+    np.testing.assert_allclose(np.array(d["gradient_hartree_per_bohr"]), g * _abi.EV_TO_HARTREE, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(np.array(d["gradient_ev_per_angstrom"]), g * _abi.ANGSTROM_TO_BOHR, rtol=1e-12, atol=1e-12)
+    assert d["method"] == "AM1" or d["method"].lower() == "am1"

@@ -68,7 +68,7 @@ def test_heavy_gradient_through_the_quadrature(gpu, oracle, z, bond):
 
     zz, x = _hydride(z, bond)
     mult = _mult(z, oracle)
-    g = gpu.gradient(zz, x, 0.0, mult)
+    g = gpu.scf_gradient(zz, x, 0.0, mult)
     s = gpu.scf(zz, x, 0.0, mult, want_matrices=True)
     ref = fd_gradient(lambda X: fixed_density_energy(oracle, zz, X, s["density"], s.get("spin_density"), "am1"), x)
     assert np.max(np.abs(g["gradient"] - ref)) < 2e-6, (g["gradient"], ref)
