@@ -82,7 +82,7 @@ class ScfServer:
 
     def __init__(self, workers: int = 3, max_batch: int = 2048, budget_bytes: int | None = None,
                  budget_fraction: float = 0.7, solve=None, small_lane: int | None = None, small_workers: int = 2,
-                 **opts):
+                 on_worker_start=None, **opts):
         self._lane_start = None
         if solve is None:
             from . import native
@@ -92,6 +92,8 @@ class ScfServer:
 
             # the small-request lane's streams go first on the SMs
             self._lane_start = lambda lane: native.set_stream_priority(-1 if lane == 1 else 0)
+        if on_worker_start is not None:  # called in each worker thread with its lane (0 large, 1 small)
+            self._lane_start = on_worker_start
         self._solve = solve
         if budget_bytes is None:
             budget_bytes = int(budget_fraction * _free_device_bytes())
@@ -154,7 +156,10 @@ class ScfServer:
 
     def _worker(self, lane: int) -> None:
         if self._lane_start is not None:
-            self._lane_start(lane)
+            try:
+                self._lane_start(lane)
+            except Exception:  # the priority only orders the work; the lane still serves without it
+                pass
         while True:
             with self._cv:
                 while True:

@@ -131,3 +131,15 @@ def test_small_lane_does_not_wait_behind_large_molecules():
 def test_orbital_count():
     assert serve.orbitals(np.array([8, 1, 1])) == 6
     assert serve.orbitals(np.array([6, 6, 1, 1, 1, 1, 1, 1])) == 14
+
+
+def test_a_failing_lane_start_does_not_stop_the_lane():
+    rec = _Recorder(delay=0.0)
+
+    def boom(lane):
+        raise RuntimeError("no device")
+
+    with serve.ScfServer(workers=1, budget_bytes=1 << 40, solve=rec, small_lane=100, small_workers=1,
+                         on_worker_start=boom) as srv:
+        futs = [srv.submit(*_mol(2)), srv.submit(*_mol(40))]  # one per lane
+        assert all(f.result(timeout=30)[0] == 0 for f in futs)
