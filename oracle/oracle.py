@@ -1,6 +1,6 @@
 """ctypes wrapper of the CPU oracle (``oracle/build/liboracle.so``).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` (as the checker)
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` (to check its results)
 and by ``bench.py``'s CPU-baseline leg.  The oracle restates am1-rs's SCF on the CPU in FP64
 (see ``am1_oracle.cpp``); it shares the C structs of ``include/am1gpu.h`` with the library so
 one ctypes layout describes both.
