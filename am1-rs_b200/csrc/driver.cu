@@ -148,9 +148,17 @@ int device_ctx(DeviceCtx** out) {
         if ((err = cudaFuncSetAttribute(k_sp2_step_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf32_smem_bytes())) !=
             cudaSuccess)
             return bad("tf32 tile kernel smem attribute", err);
-        for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8})
+        for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8, (const void*)k_dgemm16,
+                              (const void*)k_dgemm8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
-                return bad("trailing-update smem attribute", err);
+                return bad("trailing-update / back-transformation smem attribute", err);
+        {
+            cudaFuncAttributes fo{};
+            if ((err = cudaFuncGetAttributes(&fo, k_stein_orth)) != cudaSuccess) return bad("cluster orthogonalisation attributes", err);
+            if ((err = cudaFuncSetAttribute(k_stein_orth, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fo.sharedSizeBytes)) !=
+                cudaSuccess)
+                return bad("cluster orthogonalisation smem attribute", err);
+        }
     });
     if (c.rc != AM1GPU_OK) return fail(c.rc, c.err);
     g_jacobi_budget = c.jacobi_smem;
@@ -1333,10 +1341,7 @@ int write_result(Batch& b, Mem* ws, int mi, am1gpu_result* r, am1gpu_call_stats*
         const ChanJob& jc = b.jobs[b.job0[mi] + c];
         if (e_out) std::memcpy(e_out, b.h_eps + (jc.eps - b.d_eps), sizeof(double) * n);  // fetched in bulk
         if (c_out) {
-            if (p.cluster == 0)
-                return fail(AM1GPU_UNSUPPORTED, "eigenvectors (mo_coeff) are available up to 448 orbitals; this molecule has " +
-                                                    std::to_string(n) + " (every other result is filled)");
-            if (density_mode() == 0) {
+            if (density_mode() == 0 || p.cluster == 0) {
                 // the purification path has no eigenvectors: diagonalise the last F* now
                 int rc = fetch_matrix(ws, jc.Fx, n, t0, stats);
                 if (rc) return rc;
@@ -1627,6 +1632,129 @@ int g_matrix_batch(const am1gpu_molecule* mol, int method, int nrhs, const doubl
     return AM1GPU_OK;
 }
 
+// C_z (=, or -= when sub) A_z B_z for z < batch on the FP64 tensor cores, in the 64 x 64 output
+// tiles of 128 threads of dmma_gemm.cuh (k_dgemm16 when both operands allow 16-byte copies).
+int dgemm(cudaStream_t s, const double* A, int lda, long long sA, const double* B, int ldb, long long sB, double* C, int ldc,
+          long long sC, int M, int N, int K, int sub, int batch) {
+    if (M <= 0 || N <= 0 || batch <= 0) return AM1GPU_OK;
+    const dim3 grid((unsigned)cdiv(N, 64), (unsigned)cdiv(M, 64), (unsigned)batch);
+    const bool pairs = ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0) && lda % 2 == 0 && ldb % 2 == 0 && K % 2 == 0 &&
+                       N % 2 == 0 && sA % 2 == 0 && sB % 2 == 0;
+    if (pairs) k_dgemm16<<<grid, 128, dgemm_smem_bytes(), s>>>(A, lda, sA, B, ldb, sB, C, ldc, sC, M, N, K, sub);
+    else k_dgemm8<<<grid, 128, dgemm_smem_bytes(), s>>>(A, lda, sA, B, ldb, sB, C, ldc, sC, M, N, K, sub);
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+// Eigenvalues and eigenvectors of one symmetric matrix above the cluster Jacobi's capacity (up to
+// kMaxAo rows; `a` finite, its lower triangle read): the global-memory Householder reduction of
+// the final-spectrum path (a cluster per matrix below kBigGridN rows, the blocked whole-GPU
+// reduction above; both leave the reflectors in W), bisection, inverse iteration on the
+// tridiagonal and the compact-WY back-transformation (k_stein.cu).  v[i * n + k] = component i of
+// eigenvector k, eigenvalues ascending in w.
+int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem_override) {
+    const size_t nn = (size_t)n * n;
+    const int nref = n - 2;
+    const int P = cdiv(nref, kWyNb) * kWyNb, nblk = P / kWyNb;
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        off = align256(off);
+        const size_t o2 = off;
+        off += bytes;
+        return o2;
+    };
+    const size_t kwork = (size_t)4 * TRP_B * n + 2 * (size_t)n + 1024 * (2 * TRP_B + 2) + 8;
+    const size_t o_a = take(nn * 8), o_w = take(nn * 8), o_k = take(kwork * 8), o_z = take(nn * 8),
+                 o_u = take(3 * std::max(nn, (size_t)P * n) * 8), o_s = take((size_t)2 * nblk * kWyNb * kWyNb * 8),
+                 o_y = take((size_t)kWyNb * n * 8), o_d = take((size_t)n * 8), o_e = take((size_t)n * 8),
+                 o_eps = take((size_t)n * 8), o_sh = take((size_t)n * 8), o_sc = take((size_t)n * 8), o_cl = take((size_t)n * 4),
+                 o_cll = take((size_t)n * 4), o_cnt = take(16), o_tn = take(16), o_job = take(sizeof(TriJob));
+    const size_t hbytes = align256(nn * 8) + 256;
+    Workspace* ws;
+    int rc;
+    if (mem_override) {
+        rc = mem_ensure(*mem_override, align256(off), hbytes);
+        ws = mem_override;
+    } else {
+        rc = workspace(&ws, align256(off), hbytes);
+    }
+    if (rc) return rc;
+    char* D = ws->dpool;
+    const cudaStream_t s = ws->stream;
+    TriJob tj{};
+    tj.A = (const double*)(D + o_a);
+    tj.W = (double*)(D + o_w);
+    tj.work = (double*)(D + o_k);
+    tj.d = (double*)(D + o_d);
+    tj.e = (double*)(D + o_e);
+    tj.eps = (double*)(D + o_eps);
+    tj.n = n;
+    tj.mol = 0;
+    double* h = (double*)ws->hpin;
+    for (int i = 0; i < n; ++i)  // the lower triangle, mirrored (the reference's Side::Lower)
+        for (int j = 0; j < n; ++j) h[(size_t)i * n + j] = i >= j ? a[(size_t)i * n + j] : a[(size_t)j * n + i];
+    std::memcpy(ws->hpin + align256(nn * 8), &tj, sizeof tj);
+    CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(D + o_job, ws->hpin + align256(nn * 8), sizeof tj, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(D + o_cnt, 0, 16, s));
+    Batch b;
+    b.d_tri = (TriJob*)(D + o_job);
+    b.maxn = n;
+    b.tri_big = {tj};
+    int64_t launches = 0;
+    if ((rc = launch_big_tridiag(b, s, &launches))) return rc;
+    k_bisect<<<dim3(1, cdiv(n, 512)), 512, 2 * sizeof(double) * n, s>>>(b.d_tri, nullptr);
+    CK(cudaGetLastError());
+    SteinJob sj{};
+    sj.d = tj.d;
+    sj.e = tj.e;
+    sj.eps = tj.eps;
+    sj.shift = (double*)(D + o_sh);
+    sj.cl = (int*)(D + o_cl);
+    sj.cl_list = (int*)(D + o_cll);
+    sj.counts = (int*)(D + o_cnt);
+    sj.scale = (double*)(D + o_sc);
+    sj.tn = (double*)(D + o_tn);
+    sj.Z = (double*)(D + o_z);
+    sj.U = (double*)(D + o_u);
+    sj.Zt = (double*)(D + o_a);  // the input is dead after the reduction
+    sj.n = n;
+    k_stein_prep<<<1, 1024, 0, s>>>(sj);
+    for (int it = 0; it < 4; ++it) {
+        k_stein_solve<<<cdiv(n, 64), 64, 0, s>>>(sj, it == 0 ? 1 : 0);
+        k_stein_orth<<<std::max(1, n / 2), 256, sizeof(double) * n, s>>>(sj);
+    }
+    k_stein_scale<<<8 * g_sms, 256, 0, s>>>(sj);
+    CK(cudaGetLastError());
+    // back-transformation: Vt | V | U_wy in the (now dead) factor storage, then S | T, Y
+    double* Vt = (double*)(D + o_u);
+    double* V = Vt + (size_t)P * n;
+    double* Uw = V + (size_t)n * P;
+    double* S = (double*)(D + o_s);
+    double* T = S + (size_t)nblk * kWyNb * kWyNb;
+    double* Y = (double*)(D + o_y);
+    double* Z = sj.Z;
+    const long long blk = (long long)kWyNb * kWyNb, panel = (long long)kWyNb * n;
+    k_wy_split<<<dim3((unsigned)cdiv(n, 32), (unsigned)(P / 32)), dim3(32, 8), 0, s>>>(tj.W, n, nref, P, Vt, V);
+    CK(cudaGetLastError());
+    if ((rc = dgemm(s, Vt, n, panel, V, P, kWyNb, S, kWyNb, blk, kWyNb, kWyNb, n, 0, nblk))) return rc;  // S_b = Vt_b V_b
+    k_wy_tfactor<<<nblk, kWyNb, 0, s>>>(S, tj.W, tj.e, n, nref, T);
+    CK(cudaGetLastError());
+    if ((rc = dgemm(s, T, kWyNb, blk, Vt, n, panel, Uw, n, panel, kWyNb, n, kWyNb, 0, nblk))) return rc;  // U_b = T_b Vt_b
+    for (int bi = nblk - 1; bi >= 0; --bi) {
+        const int k = bi * kWyNb;  // column k of U_b and row k of V_b are zero: the products start there
+        if ((rc = dgemm(s, Uw + (size_t)bi * panel + k, n, 0, Z + (size_t)k * n, n, 0, Y, n, 0, kWyNb, n, n - k, 0, 1))) return rc;
+        if ((rc = dgemm(s, V + (size_t)k * P + k, P, 0, Y, n, 0, Z + (size_t)k * n, n, 0, n - k, n, kWyNb, 1, 1))) return rc;
+    }
+    int counts[2] = {0, 0};
+    CK(cudaMemcpyAsync(w, D + o_eps, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(v, Z, nn * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(counts, D + o_cnt, sizeof counts, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (counts[1]) return fail(AM1GPU_LINALG, "inverse iteration produced an eigenvector of zero or non-finite norm");
+    return AM1GPU_OK;
+}
+
 int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_override = nullptr) {
     g_err.clear();
     if (n < 0 || (n > 0 && (!a || !w || !v))) return fail(AM1GPU_INVALID_INPUT, "null argument");
@@ -1641,8 +1769,10 @@ int symmetric_eigen_one(int n, const double* a, double* w, double* v, Mem* mem_o
     int rc = device_ctx(&ctx);
     if (rc) return rc;
     int npad, C;
-    if (!choose_cluster(n, &npad, &C))
-        return fail(AM1GPU_UNSUPPORTED, "matrix larger than the cluster eigensolver's shared-memory capacity");
+    if (!choose_cluster(n, &npad, &C)) {
+        if (n > kMaxAo) return fail(AM1GPU_UNSUPPORTED, "matrix with " + std::to_string(n) + " rows exceeds " + std::to_string(kMaxAo));
+        return symmetric_eigen_large(n, a, w, v, mem_override);
+    }
     // layout: Gt (n*n, the lower triangle mirrored), Ct (n*n identity), Vs (npad*n), lam, colid, eps, rowmin, state
     const size_t nn = (size_t)n * n;
     size_t off = 0;

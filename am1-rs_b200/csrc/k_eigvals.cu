@@ -222,7 +222,8 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
 //   group barrier
 //   every warp sums the G shares in the same order, so all hold the same kk_s = beta_s (p.v) / 2.
 // Global scratch (job.work): v[2][n] | p[2][n] | share[G] | beta[2]; dynamic shared memory: 3 n
-// doubles (tridiag_big_smem_bytes).
+// doubles (tridiag_big_smem_bytes).  Row s of W ends holding reflector v_s in columns s+1..n-1
+// (its first entry corrected after the norm), for the eigenvector back-transformation.
 constexpr int TRIB_BATCH = 8;
 
 size_t tridiag_big_smem_bytes(int n) { return sizeof(double) * 3 * (size_t)n; }
@@ -294,7 +295,10 @@ __device__ void tridiag_group(const TriJob& jb, int G, int gi, Sync sync) {
                 if (has_next) {
                     jb.e[s] = alpha == 0.0 ? 0.0 : -sg * alpha;
                     bb[nxt] = alpha == 0.0 ? 0.0 : 1.0 / (alpha * (alpha + fabs(x0)));
-                    if (alpha != 0.0) vn[s + 1] = x0 + sg * alpha;
+                    if (alpha != 0.0) {
+                        vn[s + 1] = x0 + sg * alpha;
+                        row[s + 1] = x0 + sg * alpha;  // row s now holds v_s exactly (read by no later step)
+                    }
                 } else {
                     jb.e[s] = row[s + 1];  // the last 2 x 2 block: e[n-2]
                 }
@@ -453,7 +457,8 @@ namespace am1 {
 // its owner writes after the second barrier, every CTA forms itself (v_{c+1} and p_{c+1} are
 // known to all by then) for the next column's first phase.  Rows are cyclic over the CTAs (r % G).
 // Scratch (job.work, 16-byte aligned): VW[n][2B] = [V | W] | WVt[2B][n] = [W | V]^T | x[n] |
-// p[n] | share[G][2B + 2]; dynamic shared memory: v (n doubles) and W^T v, V^T v.
+// p[n] | share[G][2B + 2]; dynamic shared memory: v (n doubles) and W^T v, V^T v.  As in
+// tridiag_group, row c of job.W ends holding reflector v_c in columns c+1..n-1.
 // ---------------------------------------------------------------------------------------------
 
 size_t tridiag_panel_smem_bytes(int n) { return sizeof(double) * ((size_t)n + 2 * TRP_B); }
@@ -614,6 +619,7 @@ __global__ void __launch_bounds__(TRIB_THREADS) k_tridiag_panel(TriJob jb, int k
                 VW[(size_t)i * 2 * B + B + j] = w;
                 WVt[(size_t)j * n + i] = w;
                 WVt[(size_t)(B + j) * n + i] = v;
+                A[(size_t)c * n + i] = v;  // reflector c into row c (columns > c), which nothing reads again
             }
         }
         if (gi == c % G && tid == 0) jb.e[c] = alpha == 0.0 ? 0.0 : -sg * alpha;

@@ -180,6 +180,46 @@ __global__ void k_tridiag_syr2k8(TriJob job, int t0);
 size_t tridiag_panel_smem_bytes(int n);
 size_t jacobi_smem_bytes(int n, int npad, int C);
 
+// Eigenvectors of one large matrix (k_stein.cu): after the global-memory reduction (reflector s
+// in row s of W, columns > s) and k_bisect.  Inverse iteration on T: k_stein_prep (one block of
+// 1024), then four times k_stein_solve (grid ceil(n / 64) x 64, first = 1 the first time) and
+// k_stein_orth (grid max(1, n / 2) x 256, n doubles of dynamic shared memory), then k_stein_scale.
+// Z[i * n + k] = component i of eigenvector k.
+constexpr double kSteinOrtol = 1e-4;  // eigenvalues closer than this times ||T|| share a cluster
+struct SteinJob {
+    const double* d;    // tridiagonal: diagonal (n), off-diagonal (n - 1)
+    const double* e;
+    const double* eps;  // its eigenvalues, ascending
+    double* shift;      // n: the solve's shift of each vector
+    int* cl;            // n: first vector of each vector's cluster
+    int* cl_list;       // n / 2: first vector of every cluster of two or more
+    int* counts;        // [0]: clusters of two or more; [1]: error bits (a vector of zero or non-finite norm)
+    double* scale;      // n: pending 1 / norm of each vector
+    double* tn;         // [2]: ||T||_inf and the pivot floor eps ||T||
+    double* Z;          // n x n
+    double* U;          // 3 n x n: the three diagonals of the pivoted factor (same layout as Z)
+    double* Zt;         // n x n scratch: the vectors of the clusters, vector-major
+    int n;
+};
+__global__ void k_stein_prep(SteinJob sj);
+__global__ void k_stein_solve(SteinJob sj, int first);
+__global__ void k_stein_orth(SteinJob sj);
+__global__ void k_stein_scale(SteinJob sj);
+// Back-transformation in compact WY blocks of kWyNb reflectors (nref = n - 2 reflectors, P =
+// nref rounded up to kWyNb): k_wy_split (block (32, 8), grid (ceil(n / 32), P / 32)) gives Vt
+// (P x n) and V = Vt^T (n x P); S_b = Vt_b V_b by k_dgemm; k_wy_tfactor (grid P / kWyNb, kWyNb
+// threads) gives T_b; U_b = T_b Vt_b by k_dgemm; then per block, last first, Y = U_b Z and Z -= V_b Y.
+constexpr int kWyNb = 64;
+__global__ void k_wy_split(const double* W, int n, int nref, int P, double* Vt, double* V);
+__global__ void k_wy_tfactor(const double* Sg, const double* W, const double* e, int n, int nref, double* Tg);
+// C_z = A_z B_z (sub = 0) or C_z -= A_z B_z (sub = 1), z = blockIdx.z, operands advanced by the
+// strides; grid (ceil(N / 64), ceil(M / 64), batch), 128 threads, dgemm_smem_bytes().  k_dgemm16:
+// 16-byte aligned A and B, even lda, ldb, K and N.
+__global__ void k_dgemm16(const double* A, int lda, long long sA, const double* B, int ldb, long long sB, double* C, int ldc,
+                          long long sC, int M, int N, int K, int sub);
+__global__ void k_dgemm8(const double* A, int lda, long long sA, const double* B, int ldb, long long sB, double* C, int ldc,
+                         long long sC, int M, int N, int K, int sub);
+
 #ifdef __CUDACC__
 // FP32 -> nearest TF32 value (ties away from zero), kept in an FP32 register
 __device__ __forceinline__ float tf32_round(float x) {

@@ -3,8 +3,10 @@
 The SCF itself has no size limit below 8192 orbitals: integrals, Fock build, commutator and
 purification are all tiled.  Above 448 orbitals the final spectrum comes from the grid-wide
 tridiagonalisation (or a 16-CTA cluster while the matrix still fits one) and the purification
-bounds from the grid-wide Lanczos run; eigenvectors and the eigensolver fallback are not
-available, and asking for them is refused with UNSUPPORTED.
+bounds from the grid-wide Lanczos run.  Eigenvectors (mo_coeff, am1gpu_symmetric_eigen) come from
+the same reduction with its reflectors kept, inverse iteration on the tridiagonal and the
+compact-WY back-transformation.  Tolerances of the eigenvector checks: residual |A V - V L| and
+orthogonality |V^T V - I| within 1e-10 (times the largest |eigenvalue| for the residual).
 """
 
 from __future__ import annotations
@@ -36,16 +38,84 @@ def test_large_water_cluster_matches_oracle(gpu, oracle):
     assert abs(g["iterations"] - o["iterations"]) <= 1
 
 
-def test_large_molecule_refuses_eigenvectors(gpu):
-    from am1gpu import _abi
+def test_large_molecule_eigenvectors_match_oracle(gpu, oracle):
+    # 80 waters, 480 orbitals: MO coefficients from the large-matrix eigensolver
+    z, xyz = _water(80, 8)
+    g = gpu.scf(z, xyz, want_matrices=True)
+    assert g["status"] == 0 and g["converged"], g.get("error")
+    c, k, eps = g["mo_coeff"], g["n_occ"], g["mo_energies"]
+    assert c.shape == (480, 480)
+    orth = np.max(np.abs(c.T @ c - np.eye(480)))
+    assert orth < 1e-10, orth
+    assert np.max(np.abs(2.0 * c[:, :k] @ c[:, :k].T - g["density"])) < 1e-8
+    o = oracle.scf(z, xyz, want_matrices=True)
+    co = o["mo_coeff"]
+    assert np.max(np.abs(eps - o["mo_energies"])) < 1e-7
+    # orbitals whose eigenvalue is isolated (1e-3 eV from both neighbours) agree up to sign
+    gap = np.minimum(np.r_[np.inf, np.diff(eps)], np.r_[np.diff(eps), np.inf])
+    iso = gap > 1e-3
+    overlap = np.abs(np.sum(c * co, axis=0))
+    assert np.all(overlap[iso] > 1.0 - 1e-7), np.min(overlap[iso])
+    # and every occupied space is the same: the projectors agree
+    assert np.max(np.abs(c[:, :k] @ c[:, :k].T - co[:, :k] @ co[:, :k].T)) < 1e-8
 
-    z, xyz = _water(80, 8)  # 480 orbitals
-    r = gpu.scf(z, xyz, want_matrices=True)
-    assert r["status"] == _abi.UNSUPPORTED
-    plain = gpu.scf(z, xyz, want_matrices=False)
-    assert plain["status"] == 0
-    # the SCF itself ran: the density that was filled before the refusal is the converged one
-    assert abs(np.trace(r["density"]) - 8.0 * 80) < 1e-8
+
+def test_large_radical_eigenvectors(gpu):
+    # C75H151 (451 orbitals), UHF: alpha and beta coefficients rebuild the density and spin density
+    from am1gpu import workloads as W, _abi
+
+    m = W.alkane(75, np.random.default_rng(3), radical=True)
+    g = gpu.scf(m.numbers, _abi.angstrom_to_bohr(m.xyz), multiplicity=2, want_matrices=True)
+    assert g["status"] == 0 and g["converged"], g.get("error")
+    assert g["nao"] == 451
+    ca, cb = g["mo_coeff"], g["beta_coeff"]
+    for c in (ca, cb):
+        assert np.max(np.abs(c.T @ c - np.eye(451))) < 1e-10
+    pa = ca[:, : g["n_occ"]] @ ca[:, : g["n_occ"]].T
+    pb = cb[:, : g["n_occ_beta"]] @ cb[:, : g["n_occ_beta"]].T
+    assert np.max(np.abs(pa + pb - g["density"])) < 1e-8
+    assert np.max(np.abs(pa - pb - g["spin_density"])) < 1e-8
+
+
+def _check_eigh(gpu, a):
+    n = a.shape[0]
+    w, v = gpu.eigh(a)
+    wn = np.linalg.eigvalsh(a)
+    scale = max(1.0, float(np.max(np.abs(wn))))
+    assert np.all(np.diff(w) >= 0)
+    assert np.max(np.abs(w - wn)) < 1e-12 * scale * max(1.0, n / 100), np.max(np.abs(w - wn))
+    res = np.max(np.abs(a @ v - v * w)) / scale
+    orth = np.max(np.abs(v.T @ v - np.eye(n)))
+    assert res < 1e-10 and orth < 1e-10, (n, res, orth)
+
+
+@pytest.mark.parametrize("n", [449, 700, 1500, 2050, 2051])
+def test_symmetric_eigen_large(gpu, n):
+    # past the cluster Jacobi: a 16-CTA cluster reduction below 2048 rows, the blocked whole-GPU
+    # reduction above (even n: 16-byte tile copies in the back-transformation, odd n: 8-byte)
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n))
+    _check_eigh(gpu, a + a.T)
+
+
+def test_symmetric_eigen_large_degenerate(gpu):
+    rng = np.random.default_rng(11)
+    n = 520
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    _check_eigh(gpu, q @ np.diag(np.repeat(rng.standard_normal(n // 4), 4)) @ q.T)  # four-fold eigenvalues
+    b = rng.standard_normal((260, 260))
+    a = np.zeros((n, n))
+    a[:260, :260] = a[260:, 260:] = b + b.T  # two identical blocks: every eigenvalue double
+    _check_eigh(gpu, a)
+    _check_eigh(gpu, np.zeros((460, 460)))  # one cluster of 460 vectors
+
+
+def test_symmetric_eigen_large_reads_the_lower_triangle(gpu):
+    rng = np.random.default_rng(12)
+    a = rng.standard_normal((500, 500))
+    w, v = gpu.eigh(a)  # not symmetric: the lower triangle, mirrored, is the matrix
+    low = np.tril(a) + np.tril(a, -1).T
+    assert np.max(np.abs(w - np.linalg.eigvalsh(low))) < 1e-11 * np.max(np.abs(w))
 
 
 def test_water1024_cluster_full_size(gpu):
