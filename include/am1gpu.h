@@ -31,8 +31,7 @@ enum am1gpu_status {
     AM1GPU_SCF_NOT_CONVERGED = 3,          /* Am1Error::ScfNotConverged          (error.rs:35-38) */
     AM1GPU_SCF_DIVERGED = 4,               /* Am1Error::ScfDiverged              (error.rs:45-47) */
     AM1GPU_LINALG = 5,                     /* Am1Error::LinearAlgebra            (error.rs:33) */
-    AM1GPU_UNSUPPORTED = 6,                /* more than 8192 orbitals; eigenvectors (mo_coeff)
-                                              of a molecule with more than 448 orbitals */
+    AM1GPU_UNSUPPORTED = 6,                /* more than 8192 orbitals */
     AM1GPU_DEVICE_ERROR = 7                /* CUDA failure or no device */
 };
 
@@ -166,8 +165,10 @@ int am1gpu_build_fock(const am1gpu_molecule* mol, int32_t method, const double* 
 
 /*
  * Symmetric eigendecomposition: replaces symmetric_eigen (src/linalg.rs:276-331).
- * a is n*n row-major; w receives ascending eigenvalues; v (row-major) the eigenvectors as
- * columns.  Non-finite input returns AM1GPU_LINALG, as the reference refuses it.
+ * a is n*n row-major (its lower triangle is read); w receives ascending eigenvalues; v
+ * (row-major) the eigenvectors as columns.  Up to 448 rows a cluster Jacobi on chip; up to 8192
+ * the Householder reduction, bisection, inverse iteration on the tridiagonal and a blocked
+ * back-transformation.  Non-finite input returns AM1GPU_LINALG, as the reference refuses it.
  */
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 
