@@ -1931,6 +1931,7 @@ int symmetric_eigen_batch(int count, const int32_t* ns, const double* const* a, 
         size_t o_g, o_c, o_v, o_l, o_id, o_e, o_r;
     };
     std::vector<Item> items;
+    std::vector<int> large;
     size_t off = 0;
     auto take = [&off](size_t bytes) {
         off = align256(off);
@@ -1954,7 +1955,10 @@ int symmetric_eigen_batch(int count, const int32_t* ns, const double* const* a, 
         }
         Item it{i, n, 0, 0};
         if (!choose_cluster(n, &it.npad, &it.C)) {
-            set(i, AM1GPU_UNSUPPORTED, "matrix " + std::to_string(i) + " is larger than the cluster eigensolver's capacity");
+            if (n > kMaxAo)
+                set(i, AM1GPU_UNSUPPORTED, "matrix " + std::to_string(i) + " has more than " + std::to_string(kMaxAo) + " rows");
+            else
+                large.push_back(i);  // past the cluster Jacobi: the large-matrix path, one at a time, after the batch
             continue;
         }
         const size_t nn = (size_t)n * n;
@@ -1967,85 +1971,93 @@ int symmetric_eigen_batch(int count, const int32_t* ns, const double* const* a, 
         it.o_r = take((size_t)n * 8);
         items.push_back(it);
     }
-    if (items.empty()) {
-        if (first) g_err = first_msg;
-        return first;
-    }
-    // cluster-size groups, largest clusters (and matrices) first, as the batched SCF orders them
-    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.C != y.C ? x.C > y.C : x.n > y.n; });
-    const int m = (int)items.size();
-    const size_t o_st = take(sizeof(MolState) * m), o_status = take(sizeof(int) * m), o_job = take(sizeof(EigJob) * m);
-    DeviceCtx* ctx;
-    int rc = device_ctx(&ctx);
-    if (rc) return rc;
-    Workspace* ws;
-    rc = workspace(&ws, align256(off), align256(off));
-    if (rc) return rc;
-    char* D = ws->dpool;
-    char* Hh = ws->hpin;
-    Batch b;
-    b.buckets.clear();
-    for (int k = 0; k < m; ++k) {
-        const Item& it = items[k];
-        const int n = it.n;
-        const double* ak = a[it.i];
-        double* g = (double*)(Hh + it.o_g);
-        double* c = (double*)(Hh + it.o_c);
-        double* rmin = (double*)(Hh + it.o_r);
-        for (int r = 0; r < n; ++r) {
-            double bound = 0.0;
-            for (int q = 0; q < n; ++q) {
-                const double x = r >= q ? ak[(size_t)r * n + q] : ak[(size_t)q * n + r];  // lower triangle
-                g[(size_t)r * n + q] = x;
-                c[(size_t)r * n + q] = r == q ? 1.0 : 0.0;
-                if (r != q) bound += std::fabs(x);
+    if (!items.empty()) {
+        // cluster-size groups, largest clusters (and matrices) first, as the batched SCF orders them
+        std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.C != y.C ? x.C > y.C : x.n > y.n; });
+        const int m = (int)items.size();
+        const size_t o_st = take(sizeof(MolState) * m), o_status = take(sizeof(int) * m), o_job = take(sizeof(EigJob) * m);
+        DeviceCtx* ctx;
+        int rc = device_ctx(&ctx);
+        if (rc) return rc;
+        Workspace* ws;
+        rc = workspace(&ws, align256(off), align256(off));
+        if (rc) return rc;
+        char* D = ws->dpool;
+        char* Hh = ws->hpin;
+        Batch b;
+        b.buckets.clear();
+        for (int k = 0; k < m; ++k) {
+            const Item& it = items[k];
+            const int n = it.n;
+            const double* ak = a[it.i];
+            double* g = (double*)(Hh + it.o_g);
+            double* c = (double*)(Hh + it.o_c);
+            double* rmin = (double*)(Hh + it.o_r);
+            for (int r = 0; r < n; ++r) {
+                double bound = 0.0;
+                for (int q = 0; q < n; ++q) {
+                    const double x = r >= q ? ak[(size_t)r * n + q] : ak[(size_t)q * n + r];  // lower triangle
+                    g[(size_t)r * n + q] = x;
+                    c[(size_t)r * n + q] = r == q ? 1.0 : 0.0;
+                    if (r != q) bound += std::fabs(x);
+                }
+                rmin[r] = g[(size_t)r * n + r] - bound;
             }
-            rmin[r] = g[(size_t)r * n + r] - bound;
+            MolState* hs = (MolState*)(Hh + o_st) + k;
+            *hs = MolState{};
+            hs->active = 1;
+            EigJob* ej = (EigJob*)(Hh + o_job) + k;
+            *ej = EigJob{};
+            ej->Gt = (double*)(D + it.o_g);
+            ej->Ct = (double*)(D + it.o_c);
+            ej->Vs = (double*)(D + it.o_v);
+            ej->lam = (double*)(D + it.o_l);
+            ej->colid_out = (int*)(D + it.o_id);
+            ej->eps = (double*)(D + it.o_e);
+            ej->Ct_out = (double*)(D + it.o_c);
+            ej->rowmin = (double*)(D + it.o_r);
+            ej->n = n;
+            ej->npad = it.npad;
+            ej->mol = k;
+            const size_t sm = jacobi_smem_bytes(n, it.npad, it.C);
+            if (b.buckets.empty() || b.buckets.back().C != it.C) b.buckets.push_back({k, 0, it.C, 0});
+            b.buckets.back().count++;
+            b.buckets.back().smem = std::max(b.buckets.back().smem, sm);
         }
-        MolState* hs = (MolState*)(Hh + o_st) + k;
-        *hs = MolState{};
-        hs->active = 1;
-        EigJob* ej = (EigJob*)(Hh + o_job) + k;
-        *ej = EigJob{};
-        ej->Gt = (double*)(D + it.o_g);
-        ej->Ct = (double*)(D + it.o_c);
-        ej->Vs = (double*)(D + it.o_v);
-        ej->lam = (double*)(D + it.o_l);
-        ej->colid_out = (int*)(D + it.o_id);
-        ej->eps = (double*)(D + it.o_e);
-        ej->Ct_out = (double*)(D + it.o_c);
-        ej->rowmin = (double*)(D + it.o_r);
-        ej->n = n;
-        ej->npad = it.npad;
-        ej->mol = k;
-        const size_t sm = jacobi_smem_bytes(n, it.npad, it.C);
-        if (b.buckets.empty() || b.buckets.back().C != it.C) b.buckets.push_back({k, 0, it.C, 0});
-        b.buckets.back().count++;
-        b.buckets.back().smem = std::max(b.buckets.back().smem, sm);
+        std::memset(Hh + o_status, 0, sizeof(int) * m);
+        CK(cudaMemcpyAsync(D, Hh, align256(off), cudaMemcpyHostToDevice, ws->stream));
+        b.d_eig = (EigJob*)(D + o_job);
+        b.d_st = (MolState*)(D + o_st);
+        b.d_status = (int*)(D + o_status);
+        b.neig = m;
+        rc = launch_jacobi(b, ws, 1);
+        if (rc) return rc;
+        k_eig_sort<<<m, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1, nullptr);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(Hh, D, align256(off), cudaMemcpyDeviceToHost, ws->stream));
+        CK(cudaStreamSynchronize(ws->stream));
+        for (int k = 0; k < m; ++k) {
+            const Item& it = items[k];
+            const int n = it.n;
+            if (((int*)(Hh + o_status))[k]) {
+                set(it.i, AM1GPU_LINALG, "matrix " + std::to_string(it.i) + ": Jacobi eigensolver did not converge");
+                continue;
+            }
+            std::memcpy(w[it.i], Hh + it.o_e, sizeof(double) * n);
+            const double* ct = (const double*)(Hh + it.o_c);
+            for (int q = 0; q < n; ++q)
+                for (int r = 0; r < n; ++r) v[it.i][(size_t)r * n + q] = ct[(size_t)q * n + r];
+        }
     }
-    std::memset(Hh + o_status, 0, sizeof(int) * m);
-    CK(cudaMemcpyAsync(D, Hh, align256(off), cudaMemcpyHostToDevice, ws->stream));
-    b.d_eig = (EigJob*)(D + o_job);
-    b.d_st = (MolState*)(D + o_st);
-    b.d_status = (int*)(D + o_status);
-    b.neig = m;
-    rc = launch_jacobi(b, ws, 1);
-    if (rc) return rc;
-    k_eig_sort<<<m, 512, 0, ws->stream>>>(b.d_eig, b.d_st, 1, nullptr);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(Hh, D, align256(off), cudaMemcpyDeviceToHost, ws->stream));
-    CK(cudaStreamSynchronize(ws->stream));
-    for (int k = 0; k < m; ++k) {
-        const Item& it = items[k];
-        const int n = it.n;
-        if (((int*)(Hh + o_status))[k]) {
-            set(it.i, AM1GPU_LINALG, "matrix " + std::to_string(it.i) + ": Jacobi eigensolver did not converge");
-            continue;
-        }
-        std::memcpy(w[it.i], Hh + it.o_e, sizeof(double) * n);
-        const double* ct = (const double*)(Hh + it.o_c);
-        for (int q = 0; q < n; ++q)
-            for (int r = 0; r < n; ++r) v[it.i][(size_t)r * n + q] = ct[(size_t)q * n + r];
+    if (!large.empty()) {
+        DeviceCtx* ctx;
+        const int rc = device_ctx(&ctx);
+        if (rc) return rc;
+    }
+    for (int i : large) {
+        const int rc = symmetric_eigen_large(ns[i], a[i], w[i], v[i], nullptr);
+        if (rc == AM1GPU_DEVICE_ERROR) return rc;
+        set(i, rc, rc ? "matrix " + std::to_string(i) + ": " + g_err : std::string());
     }
     if (first) g_err = first_msg;
     return first;

@@ -181,8 +181,8 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
 
 /*
- * count independent symmetric eigendecompositions in one call (each as am1gpu_symmetric_eigen,
- * n[i] <= 448): replaces the per-subsystem symmetric_eigen calls of the divide-and-conquer SCF
+ * count independent symmetric eigendecompositions in one call (each as am1gpu_symmetric_eigen:
+ * those of n[i] <= 448 in one set of launches, larger ones after them, one at a time): replaces the per-subsystem symmetric_eigen calls of the divide-and-conquer SCF
  * (solve_subsystems, src/divide_conquer.rs:587-617).  a[i], w[i], v[i] as above for matrix i;
  * status[i] (may be NULL) receives its code, and the first nonzero one is returned.
  */

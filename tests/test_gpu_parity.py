@@ -283,6 +283,9 @@ def test_symmetric_eigen_batch(gpu):
     for n in sizes:
         a = rng.standard_normal((n, n))
         mats.append(a + a.T)
+    b = rng.standard_normal((600, 600))  # past the cluster Jacobi: the large-matrix path, after the batch
+    sizes.append(600)
+    mats.append(b + b.T)
     mats.append(np.array([[1.0, np.nan], [np.nan, 1.0]]))  # refused alone, the rest still solved
     status, out = gpu.eigh_batch(mats)
     from am1gpu import _abi
