@@ -1690,12 +1690,13 @@ int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem
     tj.eps = (double*)(D + o_eps);
     tj.n = n;
     tj.mol = 0;
-    double* h = (double*)ws->hpin;
-    for (int i = 0; i < n; ++i)  // the lower triangle, mirrored (the reference's Side::Lower)
-        for (int j = 0; j < n; ++j) h[(size_t)i * n + j] = i >= j ? a[(size_t)i * n + j] : a[(size_t)j * n + i];
+    std::memcpy(ws->hpin, a, nn * 8);
     std::memcpy(ws->hpin + align256(nn * 8), &tj, sizeof tj);
     CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(D + o_job, ws->hpin + align256(nn * 8), sizeof tj, cudaMemcpyHostToDevice, s));
+    // the lower triangle, mirrored (the reference's Side::Lower)
+    k_mirror_lower<<<dim3((unsigned)cdiv(n, 32), (unsigned)cdiv(n, 32)), dim3(32, 8), 0, s>>>((double*)(D + o_a), n);
+    CK(cudaGetLastError());
     CK(cudaMemsetAsync(D + o_cnt, 0, 16, s));
     Batch b;
     b.d_tri = (TriJob*)(D + o_job);

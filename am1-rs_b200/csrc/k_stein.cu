@@ -243,6 +243,25 @@ __global__ void k_stein_scale(SteinJob sj) {
         sj.Z[idx] *= sj.scale[idx % n];
 }
 
+// A[r][c] = A[c][r] for r < c: the lower triangle mirrored into the upper one (the reference reads
+// the lower triangle, Side::Lower).  Block (32, 8) per 32 x 32 tile pair (tile row tr <= tile column
+// tc): the lower tile (tc, tr) goes through shared memory into the upper tile (tr, tc); a diagonal
+// tile is read whole before any of it is written.  Grid (ceil(n / 32), ceil(n / 32)).
+__global__ void k_mirror_lower(double* A, int n) {
+    __shared__ double tile[32][33];
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    if (tr > tc) return;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = tc * 32 + y, c = tr * 32 + threadIdx.x;  // lower source rows / columns
+        tile[y][threadIdx.x] = (r < n && c < n) ? A[(size_t)r * n + c] : 0.0;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = tr * 32 + y, c = tc * 32 + threadIdx.x;  // upper destination
+        if (r < n && c < n && r < c) A[(size_t)r * n + c] = tile[threadIdx.x][y];
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Back-transformation
 // ---------------------------------------------------------------------------------------------

@@ -205,6 +205,8 @@ __global__ void k_stein_prep(SteinJob sj);
 __global__ void k_stein_solve(SteinJob sj, int first);
 __global__ void k_stein_orth(SteinJob sj);
 __global__ void k_stein_scale(SteinJob sj);
+// A[r][c] = A[c][r] for r < c; block (32, 8), grid (ceil(n / 32), ceil(n / 32))
+__global__ void k_mirror_lower(double* A, int n);
 // Back-transformation in compact WY blocks of kWyNb reflectors (nref = n - 2 reflectors, P =
 // nref rounded up to kWyNb): k_wy_split (block (32, 8), grid (ceil(n / 32), P / 32)) gives Vt
 // (P x n) and V = Vt^T (n x P); S_b = Vt_b V_b by k_dgemm; k_wy_tfactor (grid P / kWyNb, kWyNb
