@@ -1,7 +1,9 @@
 """A NumPy model of the blocked Householder reduction of k_tridiag_panel / k_tridiag_syr2k
 (csrc/k_eigvals.cu), step for step: per column the corrected column x, the reflector, p and w
 against the trailing matrix as it stood at the panel's start, then one rank-2B update per panel.
-The model's tridiagonal must have the matrix's eigenvalues (CPU only, no device)."""
+The model's tridiagonal must have the matrix's eigenvalues, and the reflectors it leaves in the rows of
+the working copy (as k_tridiag_panel writes them) must back-transform the tridiagonal's eigenvectors into
+the matrix's (CPU only, no device)."""
 
 from __future__ import annotations
 
@@ -9,7 +11,8 @@ import numpy as np
 import pytest
 
 
-def blocked_tridiag(a: np.ndarray, B: int) -> tuple[np.ndarray, np.ndarray]:
+def blocked_tridiag(a: np.ndarray, B: int, keep: bool = False):
+    """d, e (and, with keep, the working copy whose row c holds reflector v_c in columns > c)."""
     A = a.copy()
     n = A.shape[0]
     d = np.zeros(n)
@@ -40,6 +43,7 @@ def blocked_tridiag(a: np.ndarray, B: int) -> tuple[np.ndarray, np.ndarray]:
             kk = 0.5 * beta * (p @ v)
             V[r, j] = v
             W[r, j] = p - kk * v
+            A[c, c + 1:] = v  # row c is never read again
             e[c] = 0.0 if alpha == 0.0 else -sg * alpha
         if k + bw < n - 1:  # the trailing update, rank 2B
             t = slice(k + B, n)
@@ -47,7 +51,7 @@ def blocked_tridiag(a: np.ndarray, B: int) -> tuple[np.ndarray, np.ndarray]:
         k += B
     if n == 1:
         d[0] = A[0, 0]
-    return d, e
+    return (d, e, A) if keep else (d, e)
 
 
 @pytest.mark.parametrize("n,B", [(2, 32), (3, 32), (33, 32), (64, 32), (97, 32), (150, 8), (200, 32)])
@@ -69,3 +73,16 @@ def test_blocked_model_equals_the_unblocked_reduction():
     d1, e1 = blocked_tridiag(a, 1)
     d32, e32 = blocked_tridiag(a, 32)
     assert np.max(np.abs(d1 - d32)) < 1e-11 and np.max(np.abs(e1 - e32)) < 1e-11
+
+
+@pytest.mark.parametrize("n,B", [(66, 32), (131, 32), (200, 8)])
+def test_blocked_reflectors_back_transform(n, B):
+    from test_stein_model import back_transform_emulated
+
+    rng = np.random.default_rng(n + B)
+    a = rng.standard_normal((n, n))
+    a = a + a.T
+    d, e, Wk = blocked_tridiag(a, B, keep=True)
+    w, v = back_transform_emulated(Wk, d, np.r_[e, 0.0])
+    assert np.max(np.abs(a @ v - v * w)) < 1e-12 * np.max(np.abs(w))
+    assert np.max(np.abs(v.T @ v - np.eye(n))) < 1e-12

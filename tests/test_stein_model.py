@@ -183,14 +183,19 @@ def dgemm(A, a0, lda, sA, B, b0, ldb, sB, C, c0, ldc, sC, M, N, K, sub, batch):
 
 
 def eigen_large(a):
-    n = a.shape[0]
+    Wf, d, e = reduce_store(a)
+    return back_transform_emulated(Wf.reshape(a.shape), d, e)
+
+
+def back_transform_emulated(Wm, d, e):
+    """Everything after the reduction: Wm's row s holds v_s (columns > s), d and e the tridiagonal."""
+    n = Wm.shape[0]
     nn = n * n
     nref = n - 2
     P = -(-nref // NB) * NB
     nblk = P // NB
-    Wf, d, e = reduce_store(a)
     W = Buf(nn)
-    W.a[:] = Wf
+    W.a[:] = Wm.ravel()
     eps = np.linalg.eigvalsh(np.diag(d) + np.diag(e[: n - 1], 1) + np.diag(e[: n - 1], -1))
     tn, floor_, shift, cl, cl_list = stein_prep(d, e, eps)
     Z = Buf(nn)
