@@ -1889,6 +1889,9 @@ int symmetric_eigenvalues_one(int n, const double* a, double* w) {
     std::memcpy(ws->hpin + align256(nn * 8), &tj, sizeof tj);
     CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, ws->stream));
     CK(cudaMemcpyAsync(D + o_job, ws->hpin + align256(nn * 8), sizeof tj, cudaMemcpyHostToDevice, ws->stream));
+    // the lower triangle, mirrored (the reference's Side::Lower, as am1gpu_symmetric_eigen)
+    k_mirror_lower<<<dim3((unsigned)cdiv(n, 32), (unsigned)cdiv(n, 32)), dim3(32, 8), 0, ws->stream>>>((double*)(D + o_a), n);
+    CK(cudaGetLastError());
     Batch b;
     b.d_tri = (TriJob*)(D + o_job);
     b.maxn = n;

@@ -176,7 +176,7 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
  * Eigenvalues only (ascending), for a symmetric matrix of up to 8192 rows: the first half of
  * symmetric_eigen (src/linalg.rs:276-331), by the SCF's final-spectrum path (Householder
  * tridiagonalisation, blocked with FP64 tensor-core trailing updates from 2048 rows, then Sturm
- * bisection).  a is n*n row-major; non-finite input returns AM1GPU_LINALG.
+ * bisection).  a is n*n row-major (its lower triangle is read); non-finite input returns AM1GPU_LINALG.
  */
 int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
 

@@ -110,6 +110,16 @@ def test_symmetric_eigen_large_degenerate(gpu):
     _check_eigh(gpu, np.zeros((460, 460)))  # one cluster of 460 vectors
 
 
+@pytest.mark.parametrize("n", [300, 1000, 2050])
+def test_eigenvalues_read_the_lower_triangle(gpu, n):
+    # on chip, a cluster over global memory, the blocked reduction: all read the lower triangle
+    rng = np.random.default_rng(n + 1)
+    a = rng.standard_normal((n, n))
+    w = gpu.eigvalsh(a)
+    low = np.tril(a) + np.tril(a, -1).T
+    assert np.max(np.abs(w - np.linalg.eigvalsh(low))) < 1e-11 * np.max(np.abs(w))
+
+
 def test_symmetric_eigen_large_reads_the_lower_triangle(gpu):
     rng = np.random.default_rng(12)
     a = rng.standard_normal((500, 500))
