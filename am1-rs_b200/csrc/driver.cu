@@ -457,7 +457,8 @@ int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, M
     }
     if (!choose_cluster(p.nao, &p.npad, &p.cluster)) {
         // larger than the cluster eigensolver holds: the purification SCF and the final spectrum
-        // (grid-wide tridiagonalisation) still run; eigenvectors and the eigensolver path do not
+        // (grid-wide tridiagonalisation) still run, and eigenvectors on request come from the
+        // large-matrix path; the per-iteration eigensolver density path does not run
         if (p.nao > kMaxAo)
             return fail(AM1GPU_UNSUPPORTED, "molecule with " + std::to_string(p.nao) + " orbitals exceeds the limit of " +
                                                 std::to_string(kMaxAo));
