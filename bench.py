@@ -270,6 +270,8 @@ def run_ours(args):
     except Exception:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_peak_source = ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                       else "6.65 TB/s, an earlier copy-bandwidth measurement on B200 (of fallback: MEASURED_PEAKS.json absent)")
 
     native.set_timing(True)
     rb = native.ResidentBatch(mols)
@@ -441,7 +443,7 @@ def run_ours(args):
                          "share_of_step": sp2_ms / step_dev_ms, "purification_products_per_step": sp2_steps,
                          "eigensolver_fallbacks_per_step": fallbacks},
             "roofline_fock": {"kernel": "k_fock (G(P) build)", "bound": "hbm", "achieved": fock_gbs, "peak": hbm_peak,
-                              "unit": "GB/s", "frac": fock_gbs / hbm_peak, "traffic": None,
+                              "unit": "GB/s", "frac": fock_gbs / hbm_peak, "traffic": None, "peak_source": hbm_peak_source,
                               "share_of_step": ph["scf:fock"] / step_dev_ms},
             "phases_ms_per_step": ph,
             "cpu_baseline": {"value": cpu_rate, "unit": "solves/s", "cores": threads, "kind": "port",
