@@ -49,6 +49,7 @@ AM1_A0 = 0.529167
 ANGSTROM_TO_BOHR = 1.0 / AM1_A0
 EV_TO_KCAL = 23.061
 EV_TO_HARTREE = 1.0 / AM1_EV
+AU_DIPOLE_TO_DEBYE = 2.541746473  # src/constants.rs:32
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)

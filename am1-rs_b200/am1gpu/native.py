@@ -303,6 +303,23 @@ def _method_name(method: str) -> str:
     return m
 
 
+def constants() -> dict:
+    """The unit constants of the path; the dictionary of am1_rs.native.constants (src/python.rs:2514-2539):
+    MOPAC7's Hartree and Bohr (src/constants.rs:13-32), the kcal/mol factor, the dipole unit, and the two
+    factors of the infrared chain (src/ir.rs:73-76)."""
+    return {
+        "hartree_to_ev": _abi.AM1_EV,
+        "ev_to_hartree": _abi.EV_TO_HARTREE,
+        "angstrom_to_bohr": _abi.ANGSTROM_TO_BOHR,
+        "bohr_to_angstrom": _abi.AM1_A0,
+        "ev_to_kcal": _abi.EV_TO_KCAL,
+        "kcal_to_ev": 1.0 / _abi.EV_TO_KCAL,
+        "au_dipole_to_debye": _abi.AU_DIPOLE_TO_DEBYE,
+        "ir_intensity_km_per_mol": 42.2561,
+        "e_to_debye_per_angstrom": _abi.AU_DIPOLE_TO_DEBYE * _abi.ANGSTROM_TO_BOHR,
+    }
+
+
 def single_point(numbers: Sequence[int], positions, charge: float = 0.0, multiplicity: int = 1,
                  reference: str = "auto", method: str = "am1", electric_field=None) -> dict:
     """Single-point energy and properties; the dictionary of am1_rs.native.single_point."""

@@ -54,3 +54,16 @@ def test_basis_size_without_a_device():
         assert e.code == 2
     else:
         raise AssertionError("helium must be refused")
+
+
+def test_constants_are_the_reference_dictionary():
+    # am1_rs.native.constants (src/python.rs:2514-2539) over src/constants.rs:13-32 and src/ir.rs:73-76
+    from am1gpu import native
+
+    c = native.constants()
+    assert set(c) == {"hartree_to_ev", "ev_to_hartree", "angstrom_to_bohr", "bohr_to_angstrom", "ev_to_kcal",
+                      "kcal_to_ev", "au_dipole_to_debye", "ir_intensity_km_per_mol", "e_to_debye_per_angstrom"}
+    assert (c["hartree_to_ev"], c["bohr_to_angstrom"], c["ev_to_kcal"]) == (27.21, 0.529167, 23.061)
+    assert c["ev_to_hartree"] == 1.0 / 27.21 and c["angstrom_to_bohr"] == 1.0 / 0.529167 and c["kcal_to_ev"] == 1.0 / 23.061
+    assert c["au_dipole_to_debye"] == 2.541746473 and c["ir_intensity_km_per_mol"] == 42.2561
+    assert c["e_to_debye_per_angstrom"] == 2.541746473 * (1.0 / 0.529167)
