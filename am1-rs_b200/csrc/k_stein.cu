@@ -2,7 +2,7 @@
 // src/linalg.rs:276-331, at every size): A = Q T Q^T by the Householder reduction of k_eigvals.cu
 // (which leaves reflector s in row s of its working copy W, columns s+1..n-1, and e[s]),
 // eigenvalues of T by bisection, then
-//   inverse iteration on T (Wilkinson; the cluster handling of LAPACK's dstein, Dhillon 1998):
+//   inverse iteration on T (Wilkinson; the cluster handling of LAPACK's dstein):
 //     every eigenvector solves (T - sigma_k I) x = y by Gaussian elimination with partial pivoting,
 //     one thread per eigenvector, four times; eigenvalues closer than kSteinOrtol ||T|| form a
 //     cluster, whose shifts are pulled at least 10 eps ||T|| apart and whose vectors are
