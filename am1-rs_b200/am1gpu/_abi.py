@@ -108,6 +108,53 @@ class Result(ctypes.Structure):
     ]
 
 
+# am1gpu_element: Am1Element (src/params.rs:24-55), field for field
+ELEMENT_SCALARS = ["u_ss", "u_pp", "zeta_s", "zeta_p", "beta_s", "beta_p", "g_ss", "g_sp", "g_pp", "g_p2", "h_sp", "alpha"]
+ELEMENT_DERIVED = ["core_charge", "eheat_ev", "e_isol", "dd", "qq", "rho0", "rho1", "rho2"]
+
+
+class Element(ctypes.Structure):
+    _fields_ = (
+        [("z", ctypes.c_int32), ("n", ctypes.c_int32), ("n_orb", ctypes.c_int32), ("n_gauss", ctypes.c_int32)]
+        + [(f, ctypes.c_double) for f in ELEMENT_SCALARS]
+        + [("gauss_k", ctypes.c_double * 4), ("gauss_l", ctypes.c_double * 4), ("gauss_m", ctypes.c_double * 4)]
+        + [(f, ctypes.c_double) for f in ELEMENT_DERIVED]
+    )
+
+
+class ParamTable(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("count", ctypes.c_int32), ("elements", ctypes.POINTER(Element))]
+
+
+def element_to_dict(e: Element) -> dict:
+    d = {"z": e.z, "n": e.n, "n_orb": e.n_orb}
+    for f in ELEMENT_SCALARS + ELEMENT_DERIVED:
+        d[f] = getattr(e, f)
+    d["gauss"] = [(e.gauss_k[k], e.gauss_l[k], e.gauss_m[k]) for k in range(e.n_gauss)]
+    return d
+
+
+def element_from_dict(d: dict) -> Element:
+    g = list(d.get("gauss", []))
+    if len(g) > 4:
+        raise ValueError(f"element {d['z']}: at most 4 core-core Gaussians")
+    e = Element(z=int(d["z"]), n=int(d["n"]), n_orb=int(d["n_orb"]), n_gauss=len(g))
+    for f in ELEMENT_SCALARS + ELEMENT_DERIVED:
+        setattr(e, f, float(d[f]))
+    for k, (kk, ll, mm) in enumerate(g):
+        e.gauss_k[k], e.gauss_l[k], e.gauss_m[k] = float(kk), float(ll), float(mm)
+    return e
+
+
+class ParamBuffers:
+    """Keeps the element array behind an ``am1gpu_param_table`` alive."""
+
+    def __init__(self, elements: dict, method: int):
+        recs = [element_from_dict(elements[z]) for z in sorted(elements)]
+        self.arr = (Element * max(1, len(recs)))(*recs)
+        self.table = ParamTable(method=int(method), count=len(recs), elements=self.arr)
+
+
 class CallStats(ctypes.Structure):
     _fields_ = [
         ("device_ms", ctypes.c_double),
@@ -147,6 +194,22 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(Options), ctypes.POINTER(Result),
          ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), _ip],
+    ),
+    "am1gpu_element_params": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Element)]),
+    "am1gpu_derive_element": (ctypes.c_int, [ctypes.c_int32, _dp, _dp, ctypes.POINTER(Element)]),
+    "am1gpu_scf_params": (
+        ctypes.c_int,
+        [ctypes.POINTER(Molecule), ctypes.POINTER(ParamTable), ctypes.POINTER(Options), ctypes.POINTER(Result)],
+    ),
+    "am1gpu_scf_batch_params": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(ParamTable), ctypes.POINTER(Options),
+         ctypes.POINTER(Result), _ip],
+    ),
+    "am1gpu_gradient_batch_params": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.POINTER(Molecule), ctypes.POINTER(ParamTable), ctypes.POINTER(Options),
+         ctypes.POINTER(Result), ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), _ip],
     ),
     "am1gpu_build_core": (ctypes.c_int, [ctypes.POINTER(Molecule), ctypes.c_int32, _dp, _dp]),
     "am1gpu_build_fock": (

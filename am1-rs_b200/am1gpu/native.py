@@ -48,6 +48,91 @@ def _nao(numbers, method) -> int:
     return out.value
 
 
+class Am1Parameters:
+    """A parameter set, as the reference's ``Am1Parameters`` (src/params.rs:61-70): ``elements``
+    maps Z to a dict of ``Am1Element``'s fields (src/params.rs:24-55; ``gauss`` is the list of
+    (K, L, M) triples) and ``method`` names the parameterization ("am1" or "rm1"), which is the
+    method of every calculation run with the set.  Entries may be edited or replaced; the
+    calculation uses them as given (no field is re-derived)."""
+
+    def __init__(self, elements: dict, method: str = "am1"):
+        self.elements = {int(z): dict(e) for z, e in elements.items()}
+        self.method = method.lower()
+        if self.method not in _abi.METHOD:
+            raise ValueError(f"unknown method {method!r}")
+
+    @classmethod
+    def for_method(cls, method: str = "am1") -> "Am1Parameters":
+        """The built-in set (Am1Parameters::for_method, src/params.rs:88-90)."""
+        m = _abi.METHOD[method.lower()]
+        els = {}
+        e = _abi.Element()
+        for z in range(1, 87):
+            if _abi.lib().am1gpu_element_params(m, z, ctypes.byref(e)) == _abi.OK:
+                els[z] = _abi.element_to_dict(e)
+        return cls(els, method)
+
+    standard = for_method
+
+    @classmethod
+    def from_csv(cls, text: str, method: str = "am1") -> "Am1Parameters":
+        """Am1Parameters::from_csv (src/params.rs:139-263): '#' lines skipped, the first other line
+        is the header (names with spaces removed), a cell that does not parse reads 0, rows with
+        U_ss = beta_s = 0 are skipped; each row is derived by ``am1gpu_derive_element``."""
+        lines = [ln for ln in text.splitlines() if not ln.lstrip().startswith("#")]
+        if not lines:
+            raise ValueError("empty parameter CSV")
+        cols = [c.strip().replace(" ", "") for c in lines[0].split(",")]
+
+        def col(name):
+            if name not in cols:
+                raise ValueError(f"missing parameter column {name}")
+            return cols.index(name)
+
+        raw_cols = [col(n) for n in ("U_ss", "U_pp", "zeta_s", "zeta_p", "beta_s", "beta_p", "g_ss", "g_sp", "g_pp",
+                                     "g_p2", "h_sp", "alpha")]
+        gcols = [col(f"Gaussian{k}_{x}") for k in range(1, 5) for x in ("K", "L", "M")]
+        cn = col("N")
+
+        def num(cell):
+            try:
+                return float(cell.strip())
+            except ValueError:
+                return 0.0
+
+        els = {}
+        for line in lines[1:]:
+            line = line.strip()
+            if not line:
+                continue
+            f = [num(c) for c in line.split(",")]
+            z = int(f[cn])
+            if f[raw_cols[0]] == 0.0 and f[raw_cols[4]] == 0.0:
+                continue
+            raw = (ctypes.c_double * 12)(*[f[c] for c in raw_cols])
+            gauss = (ctypes.c_double * 12)(*[f[c] for c in gcols])
+            e = _abi.Element()
+            _check(_abi.lib().am1gpu_derive_element(z, raw, gauss, ctypes.byref(e)))
+            els[z] = _abi.element_to_dict(e)
+        if not els:
+            raise ValueError("no AM1 elements parsed from parameter table")
+        return cls(els, method)
+
+    def element(self, z: int) -> dict:
+        if int(z) not in self.elements:
+            raise Am1GpuError(_abi.ELEMENT_NOT_PARAMETERIZED, f"{self.method.upper()} has no parameters for element Z={z}")
+        return self.elements[int(z)]
+
+    def copy(self) -> "Am1Parameters":
+        return Am1Parameters({z: dict(e, gauss=list(e["gauss"])) for z, e in self.elements.items()}, self.method)
+
+    def buffers(self) -> _abi.ParamBuffers:
+        return _abi.ParamBuffers(self.elements, _abi.METHOD[self.method])
+
+    def nao(self, numbers) -> int:
+        return int(sum(self.element(int(z))["n_orb"] for z in np.asarray(numbers).reshape(-1)))
+
+
 def _result_dict(rb: _abi.ResultBuffers, rc: int, want_matrices: bool) -> dict:
     r = rb.res
     d = {
@@ -85,17 +170,34 @@ def _result_dict(rb: _abi.ResultBuffers, rc: int, want_matrices: bool) -> dict:
     return d
 
 
-def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, raise_on_error=False, **opts) -> dict:
-    """One molecule through ``am1gpu_scf`` (the plain FP64 drop-in).  Positions in Bohr."""
+def _nao_for(numbers, method, params):
+    """AOs of a molecule under a method's built-in set or a caller's set (0 when an element is
+    missing: the library reports that error itself)."""
+    z = np.asarray(numbers).reshape(-1)
+    if not z.size:
+        return 0
+    try:
+        return params.nao(z) if params is not None else _nao(z, method)
+    except Am1GpuError:
+        return 0
+
+
+def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, raise_on_error=False, params=None,
+        **opts) -> dict:
+    """One molecule through ``am1gpu_scf`` (the plain FP64 drop-in), or ``am1gpu_scf_params`` with
+    ``params`` (an :class:`Am1Parameters`, whose method then applies).  Positions in Bohr."""
     mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
     o = _abi.default_options(**opts)
     method = opts.get("method", "am1")
-    try:
-        nao = _nao(mb.z, method) if mb.z.size else 0
-    except Am1GpuError:
-        nao, want_matrices = 0, False  # the library reports the element error itself
+    nao = _nao_for(mb.z, method, params)
+    if nao == 0 and mb.z.size:
+        want_matrices = False
     rb = _abi.ResultBuffers(mb.z.shape[0], nao, want_matrices)
-    rc = _abi.lib().am1gpu_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
+    if params is None:
+        rc = _abi.lib().am1gpu_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
+    else:
+        pb = params.buffers()
+        rc = _abi.lib().am1gpu_scf_params(ctypes.byref(mb.mol), ctypes.byref(pb.table), ctypes.byref(o), ctypes.byref(rb.res))
     if raise_on_error:
         _check(rc, allow_not_converged=False)
     d = _result_dict(rb, rc, want_matrices)
@@ -107,24 +209,33 @@ def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, raise
 class Batch:
     """Host buffers of one batched call; reusable across calls with the same molecules."""
 
-    def __init__(self, mols, method="am1", want_matrices=False):
+    def __init__(self, mols, method="am1", want_matrices=False, params=None):
         self.mbs = [_abi.MolBuffers(*m) for m in mols]
         self.arr = (_abi.Molecule * len(self.mbs))(*[m.mol for m in self.mbs])
-        self.rbs = [_abi.ResultBuffers(m.z.shape[0], _nao(m.z, method) if m.z.size else 0, want_matrices,
-                                       unrestricted=(m.mol.multiplicity > 1)) for m in self.mbs]
+        if params is None:
+            naos = [_nao(m.z, method) if m.z.size else 0 for m in self.mbs]
+        else:
+            naos = [_nao_for(m.z, method, params) for m in self.mbs]
+        self.rbs = [_abi.ResultBuffers(m.z.shape[0], nao, want_matrices and (nao > 0 or not m.z.size),
+                                       unrestricted=(m.mol.multiplicity > 1)) for m, nao in zip(self.mbs, naos)]
         self.res = (_abi.Result * len(self.rbs))(*[r.res for r in self.rbs])
         self.status = (ctypes.c_int32 * len(self.mbs))()
         self.want_matrices = want_matrices
+        self.params = params
+        self.pbuf = params.buffers() if params is not None else None
 
     def run(self, **opts) -> int:
         o = _abi.default_options(**opts)
+        if self.pbuf is not None:
+            return _abi.lib().am1gpu_scf_batch_params(len(self.mbs), self.arr, ctypes.byref(self.pbuf.table), ctypes.byref(o),
+                                                      self.res, self.status)
         return _abi.lib().am1gpu_scf_batch(len(self.mbs), self.arr, ctypes.byref(o), self.res, self.status)
 
     def results(self) -> list[dict]:
         out = []
         for i, rb in enumerate(self.rbs):
             rb.res = self.res[i]
-            out.append(_result_dict(rb, int(self.status[i]), self.want_matrices))
+            out.append(_result_dict(rb, int(self.status[i]), self.want_matrices and rb.density is not None))
         return out
 
 
@@ -146,13 +257,18 @@ def scf_gradient(numbers, xyz_bohr, charge=0.0, multiplicity=1, **opts) -> dict:
     return d
 
 
-def gradient_batch(mols, **opts):
-    """Batched ``am1gpu_gradient_batch``: (status list, result dicts with ``gradient``)."""
-    b = Batch(mols, opts.get("method", "am1"), False)
+def gradient_batch(mols, params=None, **opts):
+    """Batched ``am1gpu_gradient_batch`` (``am1gpu_gradient_batch_params`` with ``params``):
+    (status list, result dicts with ``gradient``)."""
+    b = Batch(mols, opts.get("method", "am1"), False, params=params)
     gs = [np.zeros((m.z.shape[0], 3)) for m in b.mbs]
     ptrs = (ctypes.POINTER(ctypes.c_double) * len(gs))(*[g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for g in gs])
     o = _abi.default_options(**opts)
-    _abi.lib().am1gpu_gradient_batch(len(b.mbs), b.arr, ctypes.byref(o), b.res, ptrs, b.status)
+    if b.pbuf is not None:
+        _abi.lib().am1gpu_gradient_batch_params(len(b.mbs), b.arr, ctypes.byref(b.pbuf.table), ctypes.byref(o), b.res, ptrs,
+                                                b.status)
+    else:
+        _abi.lib().am1gpu_gradient_batch(len(b.mbs), b.arr, ctypes.byref(o), b.res, ptrs, b.status)
     res = b.results()
     for r, g in zip(res, gs):
         r["gradient"] = g
@@ -209,10 +325,10 @@ class ResidentBatch:
             pass
 
 
-def scf_batch(mols, want_matrices=False, **opts):
-    """Batched solve.  ``mols``: sequence of (numbers, xyz_bohr, charge, multiplicity).
-    Returns (status list, result dicts)."""
-    b = Batch(mols, opts.get("method", "am1"), want_matrices)
+def scf_batch(mols, want_matrices=False, params=None, **opts):
+    """Batched solve.  ``mols``: sequence of (numbers, xyz_bohr, charge, multiplicity); ``params``
+    an optional :class:`Am1Parameters`.  Returns (status list, result dicts)."""
+    b = Batch(mols, opts.get("method", "am1"), want_matrices, params=params)
     b.run(**opts)
     return list(b.status), b.results()
 

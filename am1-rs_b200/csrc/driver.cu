@@ -26,6 +26,7 @@
 namespace am1 {
 
 const DevElem* host_param_table();
+DevElem derive_from_raw(int z, const double raw[12], const double gauss[12]);
 
 namespace {
 
@@ -50,6 +51,81 @@ const char* kSymbols[] = {"X",  "H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  
                           "Re", "Os", "Ir", "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn"};
 
 inline const DevElem& helem(int method, int z) { return host_param_table()[method * (MAX_Z + 1) + z]; }
+
+// ---------------------------------------------------------------------------------------
+// Caller parameter sets (am1gpu_param_table, the reference's Am1Parameters) <-> device records
+// ---------------------------------------------------------------------------------------
+void element_to_abi(const DevElem& e, int z, am1gpu_element* o) {
+    *o = am1gpu_element{};
+    o->z = z;
+    o->n = e.n;
+    o->n_orb = e.norb;
+    o->n_gauss = e.ngauss;
+    o->u_ss = e.u_ss; o->u_pp = e.u_pp; o->zeta_s = e.zeta_s; o->zeta_p = e.zeta_p; o->beta_s = e.beta_s; o->beta_p = e.beta_p;
+    o->g_ss = e.g_ss; o->g_sp = e.g_sp; o->g_pp = e.g_pp; o->g_p2 = e.g_p2; o->h_sp = e.h_sp; o->alpha = e.alpha;
+    for (int k = 0; k < 4; ++k) {
+        o->gauss_k[k] = k < e.ngauss ? e.gk[k] : 0.0;
+        o->gauss_l[k] = k < e.ngauss ? e.gl[k] : 0.0;
+        o->gauss_m[k] = k < e.ngauss ? e.gm[k] : 0.0;
+    }
+    o->core_charge = e.core_charge; o->eheat_ev = e.eheat_ev; o->e_isol = e.e_isol;
+    o->dd = e.dd; o->qq = e.qq; o->rho0 = e.rho0; o->rho1 = e.rho1; o->rho2 = e.rho2;
+}
+
+// A caller's element record to the device record; false (with the reason) when it cannot be used.
+bool element_from_abi(const am1gpu_element& a, DevElem& e, std::string& why) {
+    if (a.z < 1 || a.z > MAX_Z) { why = "atomic number " + std::to_string(a.z) + " outside 1.." + std::to_string(MAX_Z); return false; }
+    const std::string who = std::string("element ") + kSymbols[a.z];
+    if (a.n_orb != 1 && a.n_orb != 4) { why = who + ": n_orb must be 1 or 4"; return false; }
+    if (a.n_gauss < 0 || a.n_gauss > 4) { why = who + ": n_gauss must be 0..4"; return false; }
+    if (a.n < 1 || a.n > 6) { why = who + ": principal quantum number must be 1..6"; return false; }
+    const double v[] = {a.u_ss, a.u_pp, a.zeta_s, a.zeta_p, a.beta_s, a.beta_p, a.g_ss, a.g_sp, a.g_pp, a.g_p2, a.h_sp, a.alpha,
+                        a.core_charge, a.eheat_ev, a.e_isol, a.dd, a.qq, a.rho0, a.rho1, a.rho2};
+    for (double x : v)
+        if (!std::isfinite(x)) { why = who + ": a parameter is not finite"; return false; }
+    for (int k = 0; k < a.n_gauss; ++k)
+        if (!std::isfinite(a.gauss_k[k]) || !std::isfinite(a.gauss_l[k]) || !std::isfinite(a.gauss_m[k])) {
+            why = who + ": a core-core Gaussian is not finite";
+            return false;
+        }
+    e = DevElem{};
+    e.present = 1;
+    e.n = a.n;
+    e.norb = a.n_orb;
+    e.ngauss = a.n_gauss;
+    e.u_ss = a.u_ss; e.u_pp = a.u_pp; e.zeta_s = a.zeta_s; e.zeta_p = a.zeta_p; e.beta_s = a.beta_s; e.beta_p = a.beta_p;
+    e.g_ss = a.g_ss; e.g_sp = a.g_sp; e.g_pp = a.g_pp; e.g_p2 = a.g_p2; e.h_sp = a.h_sp; e.alpha = a.alpha;
+    for (int k = 0; k < a.n_gauss; ++k) {
+        e.gk[k] = a.gauss_k[k];
+        e.gl[k] = a.gauss_l[k];
+        e.gm[k] = a.gauss_m[k];
+    }
+    e.core_charge = a.core_charge; e.eheat_ev = a.eheat_ev; e.e_isol = a.e_isol;
+    e.dd = a.dd; e.qq = a.qq; e.rho0 = a.rho0; e.rho1 = a.rho1; e.rho2 = a.rho2;
+    return true;
+}
+
+// The device table of a call with the caller's set: [method][Z] like the built-in upload, the
+// set's method slot holding exactly its elements (the other slot keeps the built-in numbers,
+// which nothing in the call reads).
+int custom_param_table(const am1gpu_param_table* t, std::vector<DevElem>& tab, int* method) {
+    if (t->method != AM1GPU_METHOD_AM1 && t->method != AM1GPU_METHOD_RM1)
+        return fail(AM1GPU_INVALID_INPUT, "unknown method " + std::to_string(t->method) + " in the parameter set");
+    if (t->count < 0 || (t->count > 0 && !t->elements)) return fail(AM1GPU_INVALID_INPUT, "null parameter set elements");
+    *method = t->method == AM1GPU_METHOD_RM1 ? 1 : 0;
+    tab.assign(host_param_table(), host_param_table() + 2 * (MAX_Z + 1));
+    DevElem* slot = tab.data() + *method * (MAX_Z + 1);
+    for (int z = 0; z <= MAX_Z; ++z) slot[z] = DevElem{};
+    for (int i = 0; i < t->count; ++i) {
+        DevElem e;
+        std::string why;
+        if (!element_from_abi(t->elements[i], e, why)) return fail(AM1GPU_INVALID_INPUT, "parameter set: " + why);
+        if (slot[t->elements[i].z].present)
+            return fail(AM1GPU_INVALID_INPUT, std::string("parameter set: element ") + kSymbols[t->elements[i].z] + " appears twice");
+        slot[t->elements[i].z] = e;
+    }
+    return AM1GPU_OK;
+}
 
 // ---------------------------------------------------------------------------------------
 // Device context: parameter table uploaded once per device
@@ -276,6 +352,18 @@ int lowp_max_iter() {
 
 // How the SCF step forms P from F*: 0 purification (default), 1 eigenvectors every iteration.
 // AM1GPU_DENSITY=jacobi selects the eigensolver path (kept for comparison and testing).
+// Purification steps before a molecule counts as stalled (AM1GPU_SP2_MAX_STEPS, 1..kSp2MaxSteps;
+// default kSp2MaxSteps).  A stalled molecule takes the eigensolver for that iteration; a small
+// cap exercises that path on every iteration.
+int sp2_max_steps() {
+    static const int v = [] {
+        const char* e = std::getenv("AM1GPU_SP2_MAX_STEPS");
+        const int k = e ? std::atoi(e) : kSp2MaxSteps;
+        return k < 1 ? kSp2MaxSteps : std::min(k, kSp2MaxSteps);
+    }();
+    return v;
+}
+
 int density_mode() {
     static const int mode = [] {
         const char* e = std::getenv("AM1GPU_DENSITY");
@@ -388,17 +476,18 @@ int choose_cluster(int n, int* npad_out, int* c_out) {
 }
 
 // Validates one molecule exactly as run_am1's head does (src/scf.rs:294-366) and plans it.
-int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, MolPlan& p) {
+// tab_all: the call's [method][Z] host table (NULL: the built-in one).
+int plan_molecule(const am1gpu_molecule& m, const am1gpu_options& o, int user, MolPlan& p, const DevElem* tab_all = nullptr) {
     if (m.natoms < 0 || (m.natoms > 0 && (!m.z || !m.xyz_bohr))) return fail(AM1GPU_INVALID_INPUT, "null molecule arrays");
     if (m.multiplicity < 1) return fail(AM1GPU_INVALID_INPUT, "multiplicity must be >= 1");
     const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
-    const DevElem* tab = host_param_table() + method * (MAX_Z + 1);  // once, not per atom
+    const DevElem* tab = (tab_all ? tab_all : host_param_table()) + method * (MAX_Z + 1);  // once, not per atom
     for (int i = 0; i < m.natoms; ++i) {
         const int z = m.z[i];
         if (z < 0 || z > MAX_Z || !tab[z].present) {
             std::string sup;
             for (int k = 1; k <= MAX_Z; ++k)
-                if (helem(method, k).present) sup += (sup.empty() ? "" : ", ") + std::string(kSymbols[k]);
+                if (tab[k].present) sup += (sup.empty() ? "" : ", ") + std::string(kSymbols[k]);
             const char* name = method ? "RM1" : "AM1";
             return fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, std::string(name) + " has no parameters for element Z=" +
                                                               std::to_string(z) + "; " + name + " covers " + sup);
@@ -520,11 +609,13 @@ struct Batch {
     double* h_grad;
     long long eps_total = 0;
     long long arena_doubles = 0;
+    const DevElem* d_params = nullptr;  // the call's own parameter table (staged with the inputs), or NULL: the built-in upload
+    int* d_big_stall = nullptr;  // per channel job: 1 when a large molecule's purification stalled this iteration
 };
 
 // Lays out the batch in one device pool and one pinned staging area, copies inputs.
 int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<MolPlan>&& plans, Batch& b, Mem& mem,
-                am1gpu_call_stats* stats, double spin_scale_override = -1.0) {
+                am1gpu_call_stats* stats, double spin_scale_override = -1.0, const DevElem* host_tab = nullptr) {
     b.plans = std::move(plans);
     b.nmol = (int)b.plans.size();
     const int method = o.method == AM1GPU_METHOD_RM1 ? 1 : 0;
@@ -582,6 +673,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
     const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
+    const size_t par_bytes = host_tab ? sizeof(DevElem) * 2 * (MAX_Z + 1) : 0;
+    const size_t o_par = take(st, par_bytes);
     const size_t staged = align256(st);
     // ---- device-only region
     size_t dv = staged;
@@ -610,6 +703,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     for (auto& p : b.plans) eps_total += (long long)p.nch * p.nao;
     const size_t o_eps = take(dv, sizeof(double) * std::max<long long>(eps_total, 1));
     const size_t o_grad = take(dv, sizeof(double) * 3 * std::max<long long>(natoms, 1));
+    const size_t o_bstall = take(dv, sizeof(int) * std::max<long long>(nch_total, 1));
     const size_t dtotal = align256(dv);
     // pinned staging also receives the outputs
     size_t hs = staged;
@@ -659,6 +753,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_charges = (double*)dptr(o_chg);
     b.d_eps = (double*)dptr(o_eps);
     b.d_grad = (double*)dptr(o_grad);
+    b.d_big_stall = (int*)dptr(o_bstall);
     b.eps_total = eps_total;
     b.h_active = (int*)(Hs + h_o_active);
     b.h_work = (double*)(Hs + h_o_work);
@@ -666,6 +761,11 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.h_charges = (double*)(Hs + h_o_chg);
     b.h_eps = (double*)(Hs + h_o_eps);
     b.h_grad = (double*)(Hs + h_o_grad);
+    b.d_params = nullptr;
+    if (host_tab) {
+        std::memcpy(Hs + o_par, host_tab, par_bytes);
+        b.d_params = (const DevElem*)dptr(o_par);
+    }
     // ---- fill the staged region
     MolDesc* hm = (MolDesc*)(Hs + o_mols);
     int* hz = (int*)(Hs + o_z);
@@ -902,10 +1002,33 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     if (stats) stats->h2d_bytes += (int64_t)staged;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, ws->stream));
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * arena, ws->stream));
+    CK(cudaMemsetAsync(b.d_big_stall, 0, sizeof(int) * std::max<long long>(nch_total, 1), ws->stream));
     return AM1GPU_OK;
 }
 
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace
+
+// Where the device part of the large-matrix eigensolver (eigen_large_run) leaves its results: Z
+// (n x n, component i of vector k at i * n + k), the ascending eigenvalues, the two failure
+// counters, and a scratch region of at least n * n doubles that is free once Z is formed.
+struct LargeEig {
+    double* Z;
+    double* eps;
+    int* counts;
+    double* spare;
+};
+
+// The device part of symmetric_eigen_large.  The matrix comes from host memory (a_host, staged
+// through m's pinned buffer) or from device memory (a_dev, copied on the device); everything runs
+// on stream s in m's device pool, and nothing is read back.
+int eigen_large_run(int n, const double* a_host, const double* a_dev, Mem& m, cudaStream_t s, LargeEig* out);
+
+// Stalled purifications of molecules above 448 orbitals: P from the large-matrix eigensolver.
+int big_fallback(Batch& b, Mem* ws);
+
+namespace {
 
 // The upper-triangle tile kernels run as up to two launches: the 16-byte-copy tiles, then the rest.
 template <class F>
@@ -1126,7 +1249,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     const int check = b.nmol > 64 ? 4 : 1;
     while (done < o.max_scf) {
         for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
-            CK(cudaMemsetAsync(b.d_active, 0, 2 * sizeof(int), s));
+            CK(cudaMemsetAsync(b.d_active, 0, 4 * sizeof(int), s));
             if ((rc = run.begin(&ph))) return rc;
             k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena,
                                                       b.d_st, 0);
@@ -1153,7 +1276,8 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                 run.launched(AM1GPU_PHASE_EIGEN,
                              3 + big_launches(big_split((int)b.sp2_big.size(), [&](int i) { return b.jobs[b.sp2_big[i]].n; }),
                                               (int)b.sp2_big.size()));
-                for (int step = 0; step < kSp2MaxSteps; ++step) {
+                const int sp2_max = sp2_max_steps();
+                for (int step = 0; step < sp2_max; ++step) {
                     size_t pc;
                     if ((rc = run.begin(&pc))) return rc;
                     // FP64 steps (jobs in a TF32 run skip them), then the TF32 steps while any
@@ -1173,7 +1297,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                     run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
                     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
                     CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
-                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, kSp2MaxSteps, b.d_sp2_active,
+                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, sp2_max, b.d_sp2_active,
                                                                   b.d_work);
                     run.launched(AM1GPU_PHASE_EIGEN);
                     if (step >= 12 && (step % 6) == 5) {
@@ -1183,9 +1307,10 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
                     }
                 }
                 const unsigned fin_blocks = std::max(8u, std::min(256u, cdiv((long long)b.maxn * b.maxn, 65536)));
-                k_sp2_finish<<<dim3(fin_blocks, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_status,
-                                                                     b.d_work);
+                k_sp2_finish<<<dim3(fin_blocks, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_work,
+                                                                     b.d_big_stall, b.d_active + 3);
                 run.launched(AM1GPU_PHASE_EIGEN);
+                if (!b.sp2_big.empty() && (rc = big_fallback(b, ws))) return rc;
                 // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
                 k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
                 if ((rc = launch_jacobi(b, ws, 0, b.d_need_eigen))) return rc;
@@ -1388,13 +1513,28 @@ void fill_empty(am1gpu_result* r) {
 }  // namespace
 
 // grads (optional): one caller buffer of 3 * natoms doubles per molecule for the nuclear gradient
-int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts, am1gpu_result* res, int* status,
-              double* const* grads = nullptr) {
+// params (optional): the caller's parameter set, whose method replaces opts->method
+int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts_in, am1gpu_result* res, int* status,
+              double* const* grads = nullptr, const am1gpu_param_table* params = nullptr) {
     g_err.clear();
     tl_stats = am1gpu_call_stats{};
-    if (nmol < 0 || (nmol > 0 && (!mols || !res)) || !opts) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (nmol < 0 || (nmol > 0 && (!mols || !res)) || !opts_in) return fail(AM1GPU_INVALID_INPUT, "null argument");
+    am1gpu_options opts_v = *opts_in;
+    const am1gpu_options* opts = &opts_v;
+    std::vector<DevElem> custom;
+    int rc;
+    if (params) {
+        int method = 0;
+        if ((rc = custom_param_table(params, custom, &method))) {
+            for (int i = 0; i < nmol; ++i)
+                if (status) status[i] = rc;
+            return rc;
+        }
+        opts_v.method = method == 1 ? AM1GPU_METHOD_RM1 : AM1GPU_METHOD_AM1;
+    }
+    const DevElem* tab_all = params ? custom.data() : nullptr;
     DeviceCtx* ctx;
-    int rc = device_ctx(&ctx);
+    rc = device_ctx(&ctx);
     if (rc) {
         for (int i = 0; i < nmol; ++i)
             if (status) status[i] = rc;
@@ -1412,7 +1552,7 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
                 rcs[i] = -1;  // solved: nothing to plan
                 continue;
             }
-            rcs[i] = plan_molecule(mols[i], *opts, i, all[i]);
+            rcs[i] = plan_molecule(mols[i], *opts, i, all[i], tab_all);
             if (rcs[i]) msgs[i] = g_err;
         }
     };
@@ -1442,9 +1582,10 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
         Batch b;
         Workspace* ws;
         rc = workspace(&ws, 0, 0);
-        if (!rc) rc = build_batch(mols, *opts, std::move(plans), b, *ws, &tl_stats);
-        if (!rc) rc = run_device(b, *ws, ctx->d_params, *opts, &tl_stats);
-        if (!rc && grads) rc = run_gradient(b, *ws, ctx->d_params, &tl_stats);
+        if (!rc) rc = build_batch(mols, *opts, std::move(plans), b, *ws, &tl_stats, -1.0, tab_all);
+        const DevElem* dp = b.d_params ? b.d_params : ctx->d_params;
+        if (!rc) rc = run_device(b, *ws, dp, *opts, &tl_stats);
+        if (!rc && grads) rc = run_gradient(b, *ws, dp, &tl_stats);
         if (!rc) rc = fetch_results(b, *ws, &tl_stats);
         if (rc) {
             for (auto& p : b.plans)
@@ -1654,6 +1795,30 @@ int dgemm(cudaStream_t s, const double* A, int lda, long long sA, const double* 
 // tridiagonal and the compact-WY back-transformation (k_stein.cu).  v[i * n + k] = component i of
 // eigenvector k, eigenvalues ascending in w.
 int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem_override) {
+    Workspace* ws;
+    int rc;
+    if (mem_override) {
+        rc = mem_ensure(*mem_override, 0, 0);
+        ws = mem_override;
+    } else {
+        rc = workspace(&ws, 0, 0);
+    }
+    if (rc) return rc;
+    LargeEig r{};
+    if ((rc = eigen_large_run(n, a, nullptr, *ws, ws->stream, &r))) return rc;
+    const cudaStream_t s = ws->stream;
+    const size_t nn = (size_t)n * n;
+    int counts[2] = {0, 0};
+    CK(cudaMemcpyAsync(w, r.eps, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(v, r.Z, nn * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(counts, r.counts, sizeof counts, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (counts[1] & 3) return fail(AM1GPU_LINALG, "inverse iteration produced an eigenvector of zero or non-finite norm");
+    if (counts[1] & 4) return fail(AM1GPU_LINALG, "inverse iteration did not converge for an eigenvector (growth below the dstein threshold)");
+    return AM1GPU_OK;
+}
+
+int eigen_large_run(int n, const double* a_host, const double* a_dev, Mem& m, cudaStream_t s, LargeEig* out) {
     const size_t nn = (size_t)n * n;
     const int nref = n - 2;
     const int P = cdiv(nref, kWyNb) * kWyNb, nblk = P / kWyNb;
@@ -1671,17 +1836,10 @@ int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem
                  o_eps = take((size_t)n * 8), o_sh = take((size_t)n * 8), o_sc = take((size_t)n * 8), o_cl = take((size_t)n * 4),
                  o_cll = take((size_t)n * 4), o_cnt = take(16), o_tn = take(16), o_job = take(sizeof(TriJob));
     const size_t hbytes = align256(nn * 8) + 256;
-    Workspace* ws;
-    int rc;
-    if (mem_override) {
-        rc = mem_ensure(*mem_override, align256(off), hbytes);
-        ws = mem_override;
-    } else {
-        rc = workspace(&ws, align256(off), hbytes);
-    }
+    int rc = mem_ensure(m, align256(off), hbytes);
     if (rc) return rc;
+    Workspace* ws = &m;
     char* D = ws->dpool;
-    const cudaStream_t s = ws->stream;
     TriJob tj{};
     tj.A = (const double*)(D + o_a);
     tj.W = (double*)(D + o_w);
@@ -1691,9 +1849,13 @@ int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem
     tj.eps = (double*)(D + o_eps);
     tj.n = n;
     tj.mol = 0;
-    std::memcpy(ws->hpin, a, nn * 8);
+    if (a_host) {
+        std::memcpy(ws->hpin, a_host, nn * 8);
+        CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, s));
+    } else {
+        CK(cudaMemcpyAsync(D + o_a, a_dev, nn * 8, cudaMemcpyDeviceToDevice, s));
+    }
     std::memcpy(ws->hpin + align256(nn * 8), &tj, sizeof tj);
-    CK(cudaMemcpyAsync(D + o_a, ws->hpin, nn * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(D + o_job, ws->hpin + align256(nn * 8), sizeof tj, cudaMemcpyHostToDevice, s));
     // the lower triangle, mirrored (the reference's Side::Lower)
     k_mirror_lower<<<dim3((unsigned)cdiv(n, 32), (unsigned)cdiv(n, 32)), dim3(32, 8), 0, s>>>((double*)(D + o_a), n);
@@ -1723,7 +1885,7 @@ int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem
     sj.n = n;
     k_stein_prep<<<1, 1024, 0, s>>>(sj);
     for (int it = 0; it < 4; ++it) {
-        k_stein_solve<<<cdiv(n, 64), 64, 0, s>>>(sj, it == 0 ? 1 : 0);
+        k_stein_solve<<<cdiv(n, 64), 64, 0, s>>>(sj, it == 0 ? 1 : 0, it == 3 ? 1 : 0);
         k_stein_orth<<<std::max(1, n / 2), 256, sizeof(double) * n, s>>>(sj);
     }
     k_stein_scale<<<8 * g_sms, 256, 0, s>>>(sj);
@@ -1748,12 +1910,54 @@ int symmetric_eigen_large(int n, const double* a, double* w, double* v, Mem* mem
         if ((rc = dgemm(s, Uw + (size_t)bi * panel + k, n, 0, Z + (size_t)k * n, n, 0, Y, n, 0, kWyNb, n, n - k, 0, 1))) return rc;
         if ((rc = dgemm(s, V + (size_t)k * P + k, P, 0, Y, n, 0, Z + (size_t)k * n, n, 0, n - k, n, kWyNb, 1, 1))) return rc;
     }
-    int counts[2] = {0, 0};
-    CK(cudaMemcpyAsync(w, D + o_eps, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(v, Z, nn * 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(counts, D + o_cnt, sizeof counts, cudaMemcpyDeviceToHost, s));
+    out->Z = Z;
+    out->eps = (double*)(D + o_eps);
+    out->counts = (int*)(D + o_cnt);
+    out->spare = (double*)(D + o_w);  // the reduction's working copy: free after the back-transformation
+    return AM1GPU_OK;
+}
+
+// A molecule above 448 orbitals has no cluster Jacobi job, so when its purification stalls (a
+// tiny HOMO-LUMO gap) its density comes from the large-matrix eigensolver instead: the
+// eigenvectors Z of its F* and P = w Z_occ Z_occ^T, as the reference forms every density from
+// an eigendecomposition (src/scf.rs:503-524, 654-657).  One flag read per iteration, only in
+// batches that hold such molecules; the rare stalled molecule is then solved on the batch's
+// stream, one at a time, in a separate device pool.
+int big_fallback(Batch& b, Mem* ws) {
+    const cudaStream_t s = ws->stream;
+    CK(cudaMemcpyAsync(b.h_active + 3, b.d_active + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (counts[1]) return fail(AM1GPU_LINALG, "inverse iteration produced an eigenvector of zero or non-finite norm");
+    if (b.h_active[3] == 0) return AM1GPU_OK;
+    std::vector<int> flags(b.jobs.size(), 0);
+    CK(cudaMemcpyAsync(flags.data(), b.d_big_stall, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    static const int kLinalg = AM1GPU_LINALG;
+    for (size_t j = 0; j < flags.size(); ++j) {
+        if (!flags[j]) continue;
+        const ChanJob& cj = b.jobs[j];
+        const MolDesc& md = b.mols[cj.mol];
+        const int n = cj.n, nocc = md.n_occ[cj.ch];
+        LargeEig r{};
+        int rc = eigen_large_run(n, nullptr, cj.Fx, tl_mem_eig, s, &r);
+        if (rc) return rc;
+        if (nocc > 0) {
+            k_transpose_cols<<<dim3(cdiv(n, 32), cdiv(nocc, 32)), dim3(32, 8), 0, s>>>(r.Z, n, nocc, r.spare);
+            CK(cudaGetLastError());
+            if ((rc = dgemm(s, r.Z, n, 0, r.spare, n, 0, cj.Pnew, n, 0, n, n, nocc, 0, 1))) return rc;
+            k_sym_scale<<<dim3(cdiv(n, 32), cdiv(n, 32)), dim3(32, 8), 0, s>>>(cj.Pnew, n, md.occ_weight);
+            CK(cudaGetLastError());
+        } else {
+            CK(cudaMemsetAsync(cj.Pnew, 0, sizeof(double) * n * n, s));
+        }
+        int counts[2] = {0, 0};
+        CK(cudaMemcpyAsync(counts, r.counts, sizeof counts, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (counts[1])  // no usable eigenvectors: the molecule ends with LINALG, as it did before this fallback
+            CK(cudaMemcpyAsync(b.d_status + cj.mol, &kLinalg, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(b.d_big_stall + j, 0, sizeof(int), s));
+    }
+    CK(cudaMemsetAsync(b.d_active + 3, 0, sizeof(int), s));
+    CK(cudaStreamSynchronize(s));
     return AM1GPU_OK;
 }
 
@@ -2113,6 +2317,42 @@ int am1gpu_basis_size(int32_t natoms, const int32_t* z, int32_t method, int32_t*
     }
     *nao = tot;
     return AM1GPU_OK;
+}
+
+int am1gpu_element_params(int32_t method, int32_t z, am1gpu_element* out) {
+    if (!out) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (method != AM1GPU_METHOD_AM1 && method != AM1GPU_METHOD_RM1) return am1::fail(AM1GPU_INVALID_INPUT, "unknown method");
+    if (z < 1 || z > am1::MAX_Z || !am1::helem(method == 1, z).present)
+        return am1::fail(AM1GPU_ELEMENT_NOT_PARAMETERIZED, std::string(method == 1 ? "RM1" : "AM1") + " has no parameters for element Z=" +
+                                                               std::to_string(z));
+    am1::element_to_abi(am1::helem(method == 1, z), z, out);
+    return AM1GPU_OK;
+}
+
+int am1gpu_derive_element(int32_t z, const double raw[12], const double gauss[12], am1gpu_element* out) {
+    if (!raw || !gauss || !out) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    if (z < 1 || z > am1::MAX_Z) return am1::fail(AM1GPU_INVALID_INPUT, "atomic number outside 1..86");
+    am1::element_to_abi(am1::derive_from_raw(z, raw, gauss), z, out);
+    return AM1GPU_OK;
+}
+
+int am1gpu_scf_params(const am1gpu_molecule* mol, const am1gpu_param_table* params, const am1gpu_options* opts, am1gpu_result* res) {
+    if (!mol || !opts || !res) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    int32_t st = 0;
+    am1gpu_options o = *opts;
+    o.precision = AM1GPU_PRECISION_FP64;  // the plain path is FP64 throughout
+    return am1::scf_batch(1, mol, &o, res, &st, nullptr, params);
+}
+
+int am1gpu_scf_batch_params(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_param_table* params, const am1gpu_options* opts,
+                            am1gpu_result* results, int32_t* status) {
+    return am1::scf_batch(nmol, mols, opts, results, status, nullptr, params);
+}
+
+int am1gpu_gradient_batch_params(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_param_table* params,
+                                 const am1gpu_options* opts, am1gpu_result* results, double* const* gradients, int32_t* status) {
+    if (nmol > 0 && !gradients) return am1::fail(AM1GPU_INVALID_INPUT, "null argument");
+    return am1::scf_batch(nmol, mols, opts, results, status, gradients, params);
 }
 
 int am1gpu_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res) {

@@ -564,19 +564,22 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
 }
 
 // P_new = w X (the converged X); molecules whose purification stalled are flagged for the
-// eigensolver path.
+// eigensolver path: need_eigen (cluster Jacobi, up to 448 orbitals) or big_stall per channel job
+// and the count in big_count (the large-matrix eigensolver, above 448).
 __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __restrict__ sst, const MolState* __restrict__ st,
-                             int* __restrict__ need_eigen, int* __restrict__ mol_status, double* __restrict__ work) {
+                             int* __restrict__ need_eigen, double* __restrict__ work, int* __restrict__ big_stall,
+                             int* __restrict__ big_count) {
     const Sp2Job jb = jobs[blockIdx.y];
     if (!st[jb.mol].active) return;
     const Sp2State& s = sst[blockIdx.y];
     if (!s.converged) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
+            atomicAdd(&work[2], 1.0);
             if (jb.fallback) {
                 need_eigen[jb.mol] = 1;
-                atomicAdd(&work[2], 1.0);
-            } else {
-                mol_status[jb.mol] = 5;  // AM1GPU_LINALG: no eigensolver for this size
+            } else {  // above the cluster Jacobi's size: the host runs the large-matrix eigensolver
+                big_stall[blockIdx.y] = 1;
+                atomicAdd(big_count, 1);
             }
         }
         return;

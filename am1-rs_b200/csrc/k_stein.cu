@@ -7,7 +7,8 @@
 //     one thread per eigenvector, four times; eigenvalues closer than kSteinOrtol ||T|| form a
 //     cluster, whose shifts are pulled at least 10 eps ||T|| apart and whose vectors are
 //     re-orthogonalised after every solve (two passes of classical Gram-Schmidt per vector, one
-//     CTA per cluster); a zero pivot becomes eps ||T||.
+//     CTA per cluster); a zero pivot becomes eps ||T||; the last solve's growth is tested as
+//     dstein tests its iterates, and a vector below the threshold fails the call (LINALG).
 //   back-transformation X = Q Z = H_0 (H_1 (... H_{n-3} Z)), H_s = I - beta_s v_s v_s^T, in
 //     blocks of kWyNb reflectors in the compact WY form H_k ... H_{k+nb-1} = I - V T V^T
 //     (Schreiber & Van Loan 1989): T from the Gram matrix V^T V, then per block
@@ -80,7 +81,12 @@ __global__ void k_stein_prep(SteinJob sj) {
 // x = (T - shift[k] I)^-1 y into Z[:, k], and scale[k] = 1 / ||x||.  Elimination with partial
 // pivoting: the current row keeps (diagonal, first superdiagonal) in registers; U row i (up to two
 // superdiagonals) goes to U0/U1/U2[i][k], the eliminated right-hand side to Z[i][k].
-__global__ void __launch_bounds__(64) k_stein_solve(SteinJob sj, int first) {
+// On the last solve (`last`), y has unit 2-norm, so ||x|| is the growth of the solve.  A shift
+// within rounding of an eigenvalue grows y by about 1 / (eps ||T||); the vector is accepted when
+// the growth reaches sqrt(0.1 / n) / (n eps ||T||): dstein's acceptance threshold sqrt(0.1 / n)
+// for an iterate whose right-hand side it scaled to n ||T|| eps.  Below it, bit 4 of counts[1]
+// marks the solve as not converged (dstein reports such vectors in INFO).
+__global__ void __launch_bounds__(64) k_stein_solve(SteinJob sj, int first, int last) {
     const int n = sj.n;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -152,6 +158,7 @@ __global__ void __launch_bounds__(64) k_stein_solve(SteinJob sj, int first) {
         sj.scale[k] = 1.0;
         return;
     }
+    if (last && nrm * ((double)n * kEps * sj.tn[0]) < sqrt(0.1 / (double)n)) atomicOr(sj.counts + 1, 4);
     sj.scale[k] = 1.0 / nrm;
 }
 
@@ -259,6 +266,42 @@ __global__ void k_mirror_lower(double* A, int n) {
     for (int y = threadIdx.y; y < 32; y += 8) {
         const int r = tr * 32 + y, c = tc * 32 + threadIdx.x;  // upper destination
         if (r < n && c < n && r < c) A[(size_t)r * n + c] = tile[threadIdx.x][y];
+    }
+}
+
+// Zt[k][i] = Z[i][k] for the first m columns, through a 32 x 32 shared-memory tile.
+__global__ void k_transpose_cols(const double* __restrict__ Z, int n, int m, double* __restrict__ Zt) {
+    __shared__ double tile[32][33];
+    const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int i = i0 + y, k = k0 + threadIdx.x;
+        tile[y][threadIdx.x] = (i < n && k < m) ? Z[(size_t)i * n + k] : 0.0;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int k = k0 + y, i = i0 + threadIdx.x;
+        if (k < m && i < n) Zt[(size_t)k * n + i] = tile[threadIdx.x][y];
+    }
+}
+
+// P = w (P + P^T) / 2: tile pair (tr <= tc) read whole into shared memory, then both written.
+__global__ void k_sym_scale(double* P, int n, double w) {
+    __shared__ double up[32][33], lo[32][33];
+    const int tr = blockIdx.y, tc = blockIdx.x;
+    if (tr > tc) return;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = tr * 32 + y, c = tc * 32 + threadIdx.x;
+        up[y][threadIdx.x] = (r < n && c < n) ? P[(size_t)r * n + c] : 0.0;
+        const int r2 = tc * 32 + y, c2 = tr * 32 + threadIdx.x;
+        lo[y][threadIdx.x] = (r2 < n && c2 < n) ? P[(size_t)r2 * n + c2] : 0.0;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = tr * 32 + y, c = tc * 32 + threadIdx.x;
+        const double v = 0.5 * w * (up[y][threadIdx.x] + lo[threadIdx.x][y]);
+        if (r < n && c < n) P[(size_t)r * n + c] = v;
+        const int r2 = tc * 32 + y, c2 = tr * 32 + threadIdx.x;
+        if (r2 < n && c2 < n) P[(size_t)r2 * n + c2] = 0.5 * w * (lo[y][threadIdx.x] + up[threadIdx.x][y]);
     }
 }
 

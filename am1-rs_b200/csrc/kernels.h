@@ -152,8 +152,8 @@ __global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int n
 __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
-__global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, int* mol_status,
-                             double* work);
+__global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
+                             int* big_stall, int* big_count);
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each
 __global__ void k_tridiag(const TriJob* jobs, const int* mask);
 size_t tridiag_smem_bytes(int n, int C);
@@ -182,7 +182,8 @@ size_t jacobi_smem_bytes(int n, int npad, int C);
 
 // Eigenvectors of one large matrix (k_stein.cu): after the global-memory reduction (reflector s
 // in row s of W, columns > s) and k_bisect.  Inverse iteration on T: k_stein_prep (one block of
-// 1024), then four times k_stein_solve (grid ceil(n / 64) x 64, first = 1 the first time) and
+// 1024), then four times k_stein_solve (grid ceil(n / 64) x 64, first = 1 the first time, last = 1
+// the fourth, which tests each vector's growth: bit 4 of counts[1] if it falls short) and
 // k_stein_orth (grid max(1, n / 2) x 256, n doubles of dynamic shared memory), then k_stein_scale.
 // Z[i * n + k] = component i of eigenvector k.
 constexpr double kSteinOrtol = 1e-4;  // eigenvalues closer than this times ||T|| share a cluster
@@ -202,11 +203,15 @@ struct SteinJob {
     int n;
 };
 __global__ void k_stein_prep(SteinJob sj);
-__global__ void k_stein_solve(SteinJob sj, int first);
+__global__ void k_stein_solve(SteinJob sj, int first, int last);
 __global__ void k_stein_orth(SteinJob sj);
 __global__ void k_stein_scale(SteinJob sj);
 // A[r][c] = A[c][r] for r < c; block (32, 8), grid (ceil(n / 32), ceil(n / 32))
 __global__ void k_mirror_lower(double* A, int n);
+// Zt[k][i] = Z[i][k] for k < m (Z n x n row-major, Zt m x n); block (32, 8), grid (ceil(n/32), ceil(m/32)).
+__global__ void k_transpose_cols(const double* Z, int n, int m, double* Zt);
+// P = w (P + P^T) / 2 in place (n x n); block (32, 8), grid (ceil(n/32), ceil(n/32)).
+__global__ void k_sym_scale(double* P, int n, double w);
 // Back-transformation in compact WY blocks of kWyNb reflectors (nref = n - 2 reflectors, P =
 // nref rounded up to kWyNb): k_wy_split (block (32, 8), grid (ceil(n / 32), P / 32)) gives Vt
 // (P x n) and V = Vt^T (n x P); S_b = Vt_b V_b by k_dgemm; k_wy_tfactor (grid P / kWyNb, kWyNb

@@ -13,9 +13,11 @@
 //
 // The host cannot use the array's name as a device address (in host code it names a host-side
 // stand-in), so at set-up -- on the first call on each device, with that device current -- the
-// address is fetched with cudaGetSymbolAddress and kept per device.  That first call must come
-// before any stream capture.  All calls share the one array: two calls whose kernels overlap
-// on the GPU (different streams, different host threads) race on it, so callers serialise them.
+// address is fetched with cudaGetSymbolAddress and kept per device (a set-up that fails is not
+// kept: the next call tries again).  That first call must come before any stream capture.  Every
+// call waits for its stream to finish before it returns, because it reads the solver's status
+// word back to the host.  All calls share the one array: two calls whose kernels overlap on the
+// GPU (different streams, different host threads) race on it, so callers serialise them.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -114,13 +116,37 @@ __global__ void k_noalloc_finish(double* __restrict__ w, double* __restrict__ v,
 
 namespace {
 
+// Per-device set-up, kept only once it has succeeded: a failed attempt (a transient error, or
+// a call made during someone else's stream capture) is retried by the next call.
 struct NoallocDevice {
-    std::once_flag once;
-    cudaError_t rc = cudaSuccess;
+    std::mutex mu;
+    bool done = false;
     double* scratch = nullptr;
     int smem_budget = 0;
 };
 NoallocDevice g_noalloc_dev[64];
+
+cudaError_t noalloc_setup(NoallocDevice& d, int dev) {
+    std::lock_guard<std::mutex> lock(d.mu);
+    if (d.done) return cudaSuccess;
+    // with that device current: the scratch array's device address and the eigensolver's launch
+    // attributes (no allocation)
+    double* scratch = nullptr;
+    cudaError_t rc;
+    if ((rc = cudaGetSymbolAddress((void**)&scratch, g_noalloc_scratch)) != cudaSuccess) return rc;
+    int optin = 0;
+    if ((rc = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return rc;
+    cudaFuncAttributes fa{};
+    if ((rc = cudaFuncGetAttributes(&fa, k_jacobi)) != cudaSuccess) return rc;
+    const int budget = optin - (int)fa.sharedSizeBytes;
+    if ((rc = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, budget)) != cudaSuccess) return rc;
+    if ((rc = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess) return rc;
+    if (!scratch) return cudaErrorInvalidSymbol;
+    d.scratch = scratch;
+    d.smem_budget = budget;
+    d.done = true;
+    return cudaSuccess;
+}
 
 // errors are reported through am1gpu_last_error, like every other entry point
 int noalloc_fail(int code, const std::string& msg) {
@@ -144,20 +170,8 @@ extern "C" int am1gpu_symmetric_eigen_noalloc(int32_t n, const double* a, double
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) return noalloc_fail(AM1GPU_DEVICE_ERROR, "no CUDA device");
     NoallocDevice& d = g_noalloc_dev[dev];
-    std::call_once(d.once, [&d, dev] {
-        // once per device, with that device current: the scratch array's device address and the
-        // eigensolver's launch attributes (no allocation)
-        if ((d.rc = cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch)) != cudaSuccess) return;
-        int optin = 0;
-        if ((d.rc = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return;
-        cudaFuncAttributes fa{};
-        if ((d.rc = cudaFuncGetAttributes(&fa, k_jacobi)) != cudaSuccess) return;
-        d.smem_budget = optin - (int)fa.sharedSizeBytes;
-        if ((d.rc = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, d.smem_budget)) != cudaSuccess) return;
-        d.rc = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    });
-    if (d.rc != cudaSuccess) return noalloc_fail(AM1GPU_DEVICE_ERROR, std::string("set-up failed: ") + cudaGetErrorString(d.rc));
-    if (!d.scratch) return noalloc_fail(AM1GPU_DEVICE_ERROR, "scratch address unavailable");
+    if ((e = noalloc_setup(d, dev)) != cudaSuccess)
+        return noalloc_fail(AM1GPU_DEVICE_ERROR, std::string("set-up failed: ") + cudaGetErrorString(e));
     // cluster size and padding as the batched solver chooses them
     int npad = 0, C = 0;
     static const int cs[5] = {1, 2, 4, 8, 16};

@@ -12,7 +12,7 @@ emitted exactly as it is spelled in the source so both sides parse the same deci
 a C header used by the CUDA library and by the CPU oracle.  Only elements the reference keeps
 are written: ``src/params.rs:186-188`` drops a row whose ``U_ss`` and ``beta_s`` are both 0.
 
-Usage:  python gen_param_table.py [REFERENCE_ROOT]   (default: /root/reference)
+Usage:  python gen_param_table.py REFERENCE_ROOT   (the am1-rs source tree, which holds src/data/*.csv)
 """
 
 from __future__ import annotations
@@ -83,7 +83,9 @@ def _table(name: str, rows) -> list[str]:
 
 
 def main() -> None:
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python gen_param_table.py REFERENCE_ROOT")
+    root = pathlib.Path(sys.argv[1])
     am1 = _csv_rows(root / "src/data/am1_parameters.csv")
     rm1 = _csv_rows(root / "src/data/rm1_parameters.csv")
     tables = (root / "src/data_tables.rs").read_text()

@@ -109,6 +109,18 @@ DevElem derive_element(const nddo_raw_element& row) {
 
 }  // namespace
 
+// One table row (raw numbers and Gaussians in the generated table's order) to the derived
+// element, as Am1Parameters::from_csv derives each CSV row (z in 0..MAX_Z).
+DevElem derive_from_raw(int z, const double raw[12], const double gauss[12]) {
+    nddo_raw_element row{};
+    row.z = z;
+    for (int k = 0; k < 12; ++k) {
+        row.raw[k] = raw[k];
+        row.gauss[k] = gauss[k];
+    }
+    return derive_element(row);
+}
+
 // Host copy of both methods' tables: [method][Z].
 const DevElem* host_param_table() {
     static DevElem table[2][MAX_Z + 1];

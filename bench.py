@@ -122,7 +122,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_sp2_step launch over the whole 512-molecule
 # batch (every molecule active), divided by that launch's algorithmic bytes 16 sum(n^2): 257.3 MB /
-# 297.0 MB (profiles/k_sp2_step__batch512_alkane_water.md).  Traffic grows with the molecules a launch
+# 297.0 MB, from one ncu capture of that launch.  Traffic grows with the molecules a launch
 # processes, so the per-launch traffic of this run is its algorithmic bytes times this ratio.
 SP2_DRAM_PER_ALG_BYTE = 0.866
 

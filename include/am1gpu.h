@@ -100,8 +100,56 @@ typedef struct {
     double* beta_coeff;     /* [nao*nao]  UHF only */
 } am1gpu_result;
 
+/*
+ * One element's parameters: Am1Element (src/params.rs:24-55), the published numbers and the
+ * quantities derived from them, field for field.  gauss_k/l/m hold the n_gauss nonzero core-core
+ * Gaussian triples (K, L, M) of Am1Element::gauss, in order.
+ */
+typedef struct {
+    int32_t z;
+    int32_t n;              /* valence principal quantum number */
+    int32_t n_orb;          /* valence AOs: 1 (s) or 4 (s, p) */
+    int32_t n_gauss;        /* 0..4 */
+    double u_ss, u_pp, zeta_s, zeta_p, beta_s, beta_p;
+    double g_ss, g_sp, g_pp, g_p2, h_sp, alpha;
+    double gauss_k[4], gauss_l[4], gauss_m[4];
+    double core_charge;     /* valence electrons */
+    double eheat_ev;        /* experimental atomic heat of formation, eV */
+    double e_isol;          /* isolated-atom electronic energy, eV */
+    double dd, qq;          /* dipole / quadrupole charge separations, Bohr */
+    double rho0, rho1, rho2;  /* Klopman-Ohno additive terms, Bohr */
+} am1gpu_element;
+
+/*
+ * A parameter set: Am1Parameters (src/params.rs:61-70).  elements[0..count) (distinct z) are
+ * every element a calculation may use; method names the parameterization the numbers belong
+ * to (AM1GPU_METHOD_*), which -- as in the reference, where the method travels with the
+ * parameters -- is the method of the calculation.
+ */
+typedef struct {
+    int32_t method;
+    int32_t count;
+    const am1gpu_element* elements;
+} am1gpu_param_table;
+
 /* Fill *opts with Am1Options::default() (src/scf.rs:174-197). */
 void am1gpu_default_options(am1gpu_options* opts);
+
+/*
+ * The built-in parameters of element z for a method: Am1Parameters::shared(method).element(z)
+ * (src/params.rs:100-130).  Returns AM1GPU_ELEMENT_NOT_PARAMETERIZED when the method does not
+ * cover z.  A caller starts a modified set from these records.
+ */
+int am1gpu_element_params(int32_t method, int32_t z, am1gpu_element* out);
+
+/*
+ * One row of a parameter table to an element: the per-row derivation of Am1Parameters::from_csv
+ * (src/params.rs:139-263; dd, qq, rho0..rho2 by MOPAC's closed forms and secant solves, e_isol,
+ * core charge and eheat from the element's tabulated facts).  raw: U_ss U_pp zeta_s zeta_p beta_s
+ * beta_p g_ss g_sp g_pp g_p2 h_sp alpha; gauss: K1 L1 M1 .. K4 L4 M4 (triples with K = L = 0 are
+ * dropped, as from_csv drops them).  Returns AM1GPU_INVALID_INPUT for z outside 1..86.
+ */
+int am1gpu_derive_element(int32_t z, const double raw[12], const double gauss[12], am1gpu_element* out);
 
 /* Number of valence AOs of a molecule: Basis::build (src/basis.rs:37-60).  Returns
  * AM1GPU_ELEMENT_NOT_PARAMETERIZED for an element the method does not cover. */
@@ -125,6 +173,21 @@ int am1gpu_scf_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_opt
                      am1gpu_result* results, int32_t* status);
 
 /*
+ * The same single points with the caller's parameter set: run_am1(molecule, params, options)
+ * (src/scf.rs:294) with any &Am1Parameters, e.g. one built by Am1Parameters::from_csv or with
+ * modified entries in its public elements map.  params == NULL uses the built-in set of
+ * opts->method; otherwise params->method is the method and opts->method is not read.  An
+ * element of the molecule that the set lacks returns AM1GPU_ELEMENT_NOT_PARAMETERIZED; a set
+ * with a repeated z, z outside 1..86, n_orb other than 1 or 4, n_gauss outside 0..4 or a
+ * non-finite number returns AM1GPU_INVALID_INPUT.  The set travels with the call's inputs
+ * (about 50 KB): nothing is cached between calls.
+ */
+int am1gpu_scf_params(const am1gpu_molecule* mol, const am1gpu_param_table* params, const am1gpu_options* opts,
+                      am1gpu_result* res);
+int am1gpu_scf_batch_params(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_param_table* params,
+                            const am1gpu_options* opts, am1gpu_result* results, int32_t* status);
+
+/*
  * SCF single point plus the closed-form nuclear gradient at its converged density: replaces
  * closed_form_gradient (src/gradient.rs:173-253) for a molecule (RHF and, through the same
  * spin-resolved pair formula, UHF: fixed_density_gradient_uhf, src/gradient.rs:495-544).
@@ -138,6 +201,12 @@ int am1gpu_gradient(const am1gpu_molecule* mol, const am1gpu_options* opts, am1g
 /* The batched form: gradients[i] (natoms_i * 3 doubles, or NULL to skip) per molecule. */
 int am1gpu_gradient_batch(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_options* opts,
                           am1gpu_result* results, double* const* gradients, int32_t* status);
+
+/* The gradient with the caller's parameter set (closed_form_gradient takes &Am1Parameters too);
+ * params as in am1gpu_scf_batch_params. */
+int am1gpu_gradient_batch_params(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_param_table* params,
+                                 const am1gpu_options* opts, am1gpu_result* results, double* const* gradients,
+                                 int32_t* status);
 
 /*
  * Core Hamiltonian and core-core energy of one molecule: replaces build_core_with_neighbors
@@ -203,7 +272,8 @@ const char* am1gpu_last_error(void);
  * returns when the results are in w and v.  Scratch is a fixed 512 KiB device array inside
  * the library, so n <= 128 (larger n returns AM1GPU_INVALID_INPUT) and no cudaMalloc/cudaFree
  * is ever called.  The first call on a device sets up (fetches the array's address) and must
- * come before any stream capture on that device.  Calls share the array: calls whose work
+ * come before any stream capture on that device; a set-up that fails is tried again by the next
+ * call.  Calls share the array: calls whose work
  * overlaps on the GPU race and must be serialised by the caller.  Non-finite input returns
  * AM1GPU_LINALG (w and v are then unspecified).
  */

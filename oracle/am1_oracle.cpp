@@ -37,6 +37,34 @@ constexpr double AU_DIPOLE_TO_DEBYE = 2.541746473;
 
 thread_local std::string g_err;
 
+// Threads for the O(n^3) loops inside one molecule (oracle_set_threads; 1 by default).  The
+// split is over independent output rows or columns only, so every element is summed in the
+// same order as the serial loop and results do not depend on the thread count.  Threads of
+// oracle_scf_batch, which already run molecules in parallel, keep these loops serial.
+std::atomic<int> g_inner_threads{1};
+thread_local bool t_serial = false;
+
+// f(lo, hi) over [0, n) in contiguous chunks; `work` is the loop's operation count, below
+// which threads are not worth starting.
+template <class F>
+void par_for(int n, double work, F&& f) {
+    int nt = g_inner_threads.load();
+    if (nt <= 1 || t_serial || work < 2.0e5 || n < 2 * nt) {
+        f(0, n);
+        return;
+    }
+    auto chunk = [&](int t) {
+        const int lo = (int)((long long)n * t / nt), hi = (int)((long long)n * (t + 1) / nt);
+        t_serial = true;
+        f(lo, hi);
+        t_serial = false;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(chunk, t);
+    chunk(0);
+    for (auto& t : pool) t.join();
+}
+
 // ----------------------------------------------------------------------------------------
 // Parameters: src/params.rs:139-330, src/data_tables.rs:53-224
 // ----------------------------------------------------------------------------------------
@@ -932,20 +960,24 @@ void householder_tridiag(int n, std::vector<double>& a, std::vector<double>& q, 
         betas[k] = beta;
         e[k] = -sgn * alpha;
         // p = beta * A_sub v, using the symmetric trailing block
+        par_for(m, (double)m * m, [&](int lo, int hi) {
+            for (int i = lo; i < hi; ++i) {
+                double acc = 0.0;
+                const double* row = &a[(size_t)(k + 1 + i) * n + k + 1];
+                for (int j = 0; j < m; ++j) acc += row[j] * v[j];
+                p[i] = beta * acc;
+            }
+        });
         double pv = 0.0;
-        for (int i = 0; i < m; ++i) {
-            double acc = 0.0;
-            const double* row = &a[(size_t)(k + 1 + i) * n + k + 1];
-            for (int j = 0; j < m; ++j) acc += row[j] * v[j];
-            p[i] = beta * acc;
-            pv += p[i] * v[i];
-        }
+        for (int i = 0; i < m; ++i) pv += p[i] * v[i];
         double kk = 0.5 * beta * pv;
         for (int i = 0; i < m; ++i) w[i] = p[i] - kk * v[i];
-        for (int i = 0; i < m; ++i) {
-            double* row = &a[(size_t)(k + 1 + i) * n + k + 1];
-            for (int j = 0; j < m; ++j) row[j] -= v[i] * w[j] + w[i] * v[j];
-        }
+        par_for(m, (double)m * m, [&](int lo, int hi) {
+            for (int i = lo; i < hi; ++i) {
+                double* row = &a[(size_t)(k + 1 + i) * n + k + 1];
+                for (int j = 0; j < m; ++j) row[j] -= v[i] * w[j] + w[i] * v[j];
+            }
+        });
     }
     for (int i = 0; i < n; ++i) d[i] = A(i, i);
     if (n >= 2) e[n - 2] = A(n - 1, n - 2);
@@ -957,17 +989,22 @@ void householder_tridiag(int n, std::vector<double>& a, std::vector<double>& q, 
         if (betas[k] == 0.0) continue;
         const std::vector<double>& v = vs[k];
         const int m = n - k - 1;
-        // Q_sub -= beta v (v^T Q_sub), Q_sub = rows/cols k+1..n-1
-        for (int j = 0; j < m; ++j) t[j] = 0.0;
-        for (int i = 0; i < m; ++i) {
-            const double* row = &q[(size_t)(k + 1 + i) * n + k + 1];
-            for (int j = 0; j < m; ++j) t[j] += v[i] * row[j];
-        }
-        for (int i = 0; i < m; ++i) {
-            double* row = &q[(size_t)(k + 1 + i) * n + k + 1];
-            double bv = betas[k] * v[i];
-            for (int j = 0; j < m; ++j) row[j] -= bv * t[j];
-        }
+        // Q_sub -= beta v (v^T Q_sub), Q_sub = rows/cols k+1..n-1 (t split by columns, the
+        // update by rows: each t[j] still sums its rows in order)
+        par_for(m, (double)m * m, [&](int lo, int hi) {
+            for (int j = lo; j < hi; ++j) t[j] = 0.0;
+            for (int i = 0; i < m; ++i) {
+                const double* row = &q[(size_t)(k + 1 + i) * n + k + 1];
+                for (int j = lo; j < hi; ++j) t[j] += v[i] * row[j];
+            }
+        });
+        par_for(m, (double)m * m, [&](int lo, int hi) {
+            for (int i = lo; i < hi; ++i) {
+                double* row = &q[(size_t)(k + 1 + i) * n + k + 1];
+                double bv = betas[k] * v[i];
+                for (int j = 0; j < m; ++j) row[j] -= bv * t[j];
+            }
+        });
     }
 }
 
@@ -979,6 +1016,10 @@ void qr_sweep(int n, int lo, int hi, std::vector<double>& d, std::vector<double>
     double b = e[hi - 1];
     double mu = d[hi] - b * b / (half + std::copysign(std::hypot(half, b), half));
     double x = d[lo] - mu, y = e[lo];
+    // The rotations only depend on d and e: chase the bulge first, then apply the sweep's
+    // rotations to z row by row (the same operations on each element, in the same order, with
+    // contiguous access).
+    std::vector<double> cs(hi - lo), sn(hi - lo);
     for (int k = lo; k < hi; ++k) {
         double r = std::hypot(x, y);
         double c = 1.0, s = 0.0;
@@ -986,6 +1027,8 @@ void qr_sweep(int n, int lo, int hi, std::vector<double>& d, std::vector<double>
             c = x / r;
             s = y / r;
         }
+        cs[k - lo] = c;
+        sn[k - lo] = s;
         if (k > lo) e[k - 1] = r;
         double ak = d[k], bk = e[k], an = d[k + 1];
         d[k] = ak * c * c + 2.0 * bk * c * s + an * s * s;
@@ -997,13 +1040,18 @@ void qr_sweep(int n, int lo, int hi, std::vector<double>& d, std::vector<double>
             e[k + 1] = c * f;
             x = e[k];
         }
-        for (int i = 0; i < n; ++i) {
-            double* row = &z[(size_t)i * n];
-            double zk = row[k], zn = row[k + 1];
-            row[k] = c * zk + s * zn;
-            row[k + 1] = -s * zk + c * zn;
-        }
     }
+    par_for(n, 6.0 * n * (hi - lo), [&](int i0, int i1) {
+        for (int i = i0; i < i1; ++i) {
+            double* row = &z[(size_t)i * n];
+            for (int k = lo; k < hi; ++k) {
+                const double c = cs[k - lo], s = sn[k - lo];
+                double zk = row[k], zn = row[k + 1];
+                row[k] = c * zk + s * zn;
+                row[k + 1] = -s * zk + c * zn;
+            }
+        }
+    });
 }
 
 bool tridiagonal_eigen(int n, std::vector<double>& d, std::vector<double>& e, std::vector<double>& z) {
@@ -1078,12 +1126,14 @@ Mat sad_density(const Molecule& mol, const Basis& basis, const ParamSet& ps) {
 Mat density_from_coeff(int n, const Mat& c, int n_occ, double weight) {
     Mat p((size_t)n * n, 0.0);
     if (n_occ == 0 || n == 0) return p;
-    for (int mu = 0; mu < n; ++mu)
-        for (int nu = 0; nu < n; ++nu) {
-            double acc = 0.0;
-            for (int k = 0; k < n_occ; ++k) acc += c[(size_t)mu * n + k] * c[(size_t)nu * n + k];
-            p[(size_t)mu * n + nu] = acc;
-        }
+    par_for(n, (double)n * n * n_occ, [&](int lo, int hi) {
+        for (int mu = lo; mu < hi; ++mu)
+            for (int nu = 0; nu < n; ++nu) {
+                double acc = 0.0;
+                for (int k = 0; k < n_occ; ++k) acc += c[(size_t)mu * n + k] * c[(size_t)nu * n + k];
+                p[(size_t)mu * n + nu] = acc;
+            }
+    });
     if (weight != 1.0)
         for (double& x : p) x *= weight;
     return p;
@@ -1092,12 +1142,17 @@ Mat density_from_coeff(int n, const Mat& c, int n_occ, double weight) {
 // src/scf.rs:531-544: e = FP - PF using PF = (FP)^T
 Mat commutator(int n, const Mat& f, const Mat& p) {
     Mat e((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-            double acc = 0.0;
-            for (int k = 0; k < n; ++k) acc += f[(size_t)i * n + k] * p[(size_t)k * n + j];
-            e[(size_t)i * n + j] = acc;
+    // (FP)_ij summed over k in ascending order, as a row of accumulators (contiguous reads of P)
+    par_for(n, (double)n * n * n, [&](int lo, int hi) {
+        for (int i = lo; i < hi; ++i) {
+            double* acc = &e[(size_t)i * n];
+            for (int k = 0; k < n; ++k) {
+                const double fik = f[(size_t)i * n + k];
+                const double* prow = &p[(size_t)k * n];
+                for (int j = 0; j < n; ++j) acc[j] += fik * prow[j];
+            }
         }
+    });
     for (int i = 0; i < n; ++i) {
         for (int j = i + 1; j < n; ++j) {
             double a = e[(size_t)i * n + j], b = e[(size_t)j * n + i];
@@ -1480,12 +1535,14 @@ void copy_out(double* dst, const std::vector<double>& src) {
 }
 
 // src/scf.rs:294-468
-int run_am1(const am1gpu_molecule* m, const am1gpu_options* o, am1gpu_result* res) {
+// custom: a caller's parameter set (run_am1 takes any &Am1Parameters); NULL: the built-in set
+// of o->method.
+int run_am1(const am1gpu_molecule* m, const am1gpu_options* o, am1gpu_result* res, const ParamSet* custom = nullptr) {
     g_err.clear();
     if (!m || !o || !res || m->natoms < 0 || (m->natoms > 0 && (!m->z || !m->xyz_bohr)))
         return set_error(AM1GPU_INVALID_INPUT, "null argument");
     if (m->multiplicity < 1) return set_error(AM1GPU_INVALID_INPUT, "multiplicity must be >= 1");
-    const ParamSet& ps = params_for(o->method);
+    const ParamSet& ps = custom ? *custom : params_for(o->method);
     Molecule mol = to_molecule(m);
     int rc = check_elements(mol, ps);
     if (rc) return rc;
@@ -1614,8 +1671,45 @@ int oracle_local_overlaps(int method, int za, int zb, double r, int numeric, dou
     return AM1GPU_OK;
 }
 
+// Threads for the O(n^3) loops of one molecule's SCF (default 1); results do not depend on it.
+void oracle_set_threads(int nthreads) { g_inner_threads.store(std::max(1, nthreads)); }
+
 int oracle_scf(const am1gpu_molecule* mol, const am1gpu_options* opts, am1gpu_result* res) {
     return run_am1(mol, opts, res);
+}
+
+// The SCF with a caller's parameter set (the elements of an Am1Parameters, src/params.rs:24-70),
+// taken as given: no field is re-derived.
+int oracle_scf_params(const am1gpu_molecule* mol, const am1gpu_param_table* t, const am1gpu_options* opts,
+                      am1gpu_result* res) {
+    if (!t || t->count < 0 || (t->count > 0 && !t->elements)) return set_error(AM1GPU_INVALID_INPUT, "null parameter set");
+    static thread_local ParamSet ps;
+    ps = ParamSet{};
+    ps.name = t->method == AM1GPU_METHOD_RM1 ? "RM1" : "AM1";
+    for (int i = 0; i < t->count; ++i) {
+        const am1gpu_element& a = t->elements[i];
+        if (a.z < 1 || a.z > NDDO_MAX_Z || ps.present[a.z] || a.n_gauss < 0 || a.n_gauss > 4)
+            return set_error(AM1GPU_INVALID_INPUT, "bad parameter set entry");
+        Elem e;
+        e.z = a.z;
+        e.n = a.n;
+        e.norb = a.n_orb;
+        e.ngauss = a.n_gauss;
+        e.u_ss = a.u_ss; e.u_pp = a.u_pp; e.zeta_s = a.zeta_s; e.zeta_p = a.zeta_p; e.beta_s = a.beta_s; e.beta_p = a.beta_p;
+        e.g_ss = a.g_ss; e.g_sp = a.g_sp; e.g_pp = a.g_pp; e.g_p2 = a.g_p2; e.h_sp = a.h_sp; e.alpha = a.alpha;
+        for (int k = 0; k < 4; ++k) {
+            e.gk[k] = a.gauss_k[k];
+            e.gl[k] = a.gauss_l[k];
+            e.gm[k] = a.gauss_m[k];
+        }
+        e.core_charge = a.core_charge; e.eheat_ev = a.eheat_ev; e.e_isol = a.e_isol;
+        e.dd = a.dd; e.qq = a.qq; e.rho0 = a.rho0; e.rho1 = a.rho1; e.rho2 = a.rho2;
+        ps.by_z[a.z] = e;
+        ps.present[a.z] = true;
+    }
+    am1gpu_options o = *opts;
+    o.method = t->method;
+    return run_am1(mol, &o, res, &ps);
 }
 
 // Molecules are independent; a pool of host threads takes them one at a time (CPU baseline).
@@ -1624,7 +1718,10 @@ int oracle_scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options
     int first = AM1GPU_OK;
     std::atomic<int> next{0};
     auto worker = [&]() {
+        const bool was = t_serial;
+        t_serial = true;  // molecules already run in parallel: keep each one's loops serial
         for (int i = next++; i < nmol; i = next++) status[i] = run_am1(&mols[i], opts, &res[i]);
+        t_serial = was;
     };
     int nt = std::max(1, nthreads);
     std::vector<std::thread> pool;

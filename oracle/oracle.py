@@ -42,6 +42,9 @@ _SIGS = {
     "oracle_bintgs": (None, [ctypes.c_double, _dp]),
     "oracle_local_overlaps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]),
     "oracle_last_error": (ctypes.c_char_p, []),
+    "oracle_set_threads": (None, [ctypes.c_int]),
+    "oracle_scf_params": (ctypes.c_int, [ctypes.POINTER(_abi.Molecule), ctypes.POINTER(_abi.ParamTable),
+                                         ctypes.POINTER(_abi.Options), ctypes.POINTER(_abi.Result)]),
 }
 
 _lib = None
@@ -116,12 +119,26 @@ def nao_of(numbers, method="am1") -> int:
     return tot
 
 
-def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, **opts) -> dict:
+def set_threads(nthreads: int) -> None:
+    """Host threads for the O(n^3) loops inside one molecule's SCF (default 1).  Every element
+    is summed in the same order whatever the count, so results are the same bit for bit."""
+    lib().oracle_set_threads(int(nthreads))
+
+
+def scf(numbers, xyz_bohr, charge=0.0, multiplicity=1, want_matrices=True, params=None, **opts) -> dict:
+    """params: an optional am1gpu.native.Am1Parameters (elements as given, its method applies)."""
     mb = _abi.MolBuffers(numbers, xyz_bohr, charge, multiplicity)
     o = _abi.plain_default_options(**opts)
-    nao = nao_of(numbers, opts.get("method", "am1"))
+    if params is None:
+        nao = nao_of(numbers, opts.get("method", "am1"))
+    else:
+        nao = int(sum(params.elements[int(z)]["n_orb"] for z in np.asarray(numbers).reshape(-1)))
     rb = _abi.ResultBuffers(mb.z.shape[0], nao, want_matrices)
-    rc = lib().oracle_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
+    if params is None:
+        rc = lib().oracle_scf(ctypes.byref(mb.mol), ctypes.byref(o), ctypes.byref(rb.res))
+    else:
+        pb = _abi.ParamBuffers(params.elements, _abi.METHOD[params.method])
+        rc = lib().oracle_scf_params(ctypes.byref(mb.mol), ctypes.byref(pb.table), ctypes.byref(o), ctypes.byref(rb.res))
     d = result_dict(rb, rc, mb.z.shape[0])
     if rc:
         d["error"] = lib().oracle_last_error().decode()

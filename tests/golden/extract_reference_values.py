@@ -12,7 +12,7 @@ read as text:
 * ``src/scf.rs`` tests: the water geometry with its heat-of-formation / dipole bands and the
   methyl-radical geometry.
 
-Usage: python extract_reference_values.py [REFERENCE_ROOT]   (default /root/reference)
+Usage: python extract_reference_values.py REFERENCE_ROOT   (the am1-rs source tree)
 """
 
 from __future__ import annotations
@@ -37,7 +37,9 @@ def parse_xyz_literal(s: str):
 
 
 def main() -> None:
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python extract_reference_values.py REFERENCE_ROOT")
+    root = pathlib.Path(sys.argv[1])
     out: dict = {"source": "ss0832/am1-rs 0.2.3 test files (see extract_reference_values.py)"}
 
     aux = (root / "tests/auxiliary_integral_impact.rs").read_text()

@@ -67,3 +67,38 @@ def test_constants_are_the_reference_dictionary():
     assert c["ev_to_hartree"] == 1.0 / 27.21 and c["angstrom_to_bohr"] == 1.0 / 0.529167 and c["kcal_to_ev"] == 1.0 / 23.061
     assert c["au_dipole_to_debye"] == 2.541746473 and c["ir_intensity_km_per_mol"] == 42.2561
     assert c["e_to_debye_per_angstrom"] == 2.541746473 * (1.0 / 0.529167)
+
+
+def test_parameter_sets_without_a_device():
+    # Am1Parameters (src/params.rs:61-263) through am1gpu_element_params / am1gpu_derive_element,
+    # which need no device: the built-in records equal the oracle's derivation, and a CSV written
+    # from them parses back (Am1Parameters::from_csv) to the same records bit for bit
+    import oracle as O
+
+    from am1gpu import native
+
+    for method in ("am1", "rm1"):
+        ps = native.Am1Parameters.for_method(method)
+        assert 1 in ps.elements and 6 in ps.elements and 8 in ps.elements
+        for z, e in ps.elements.items():
+            o = O.element(z, method)
+            for f in ("u_ss", "u_pp", "zeta_s", "zeta_p", "beta_s", "beta_p", "g_ss", "g_sp", "g_pp", "g_p2", "h_sp",
+                      "alpha", "core_charge", "eheat_ev", "e_isol", "dd", "qq", "rho0", "rho1", "rho2"):
+                assert e[f] == o[f], (method, z, f)
+            assert (e["n"], e["n_orb"], len(e["gauss"])) == (o["n"], o["norb"], o["ngauss"])
+        names = ["N", "U_ss", "U_pp", "zeta_s", "zeta_p", "beta_s", "beta_p", "g_ss", "g_sp", "g_pp", "g_p2", "h_sp",
+                 "alpha"] + [f"Gaussian{k}_{x}" for k in range(1, 5) for x in ("K", "L", "M")]
+        rows = ["# provenance line", ", ".join(n.replace("_s", " _s") if n == "zeta_s" else n for n in names)]
+        for z, e in sorted(ps.elements.items()):
+            g = list(e["gauss"]) + [(0.0, 0.0, 0.0)] * (4 - len(e["gauss"]))
+            vals = [z] + [e[f.lower() if f.startswith("U_") else f] for f in names[1:13]] + [x for t in g for x in t]
+            rows.append(",".join(repr(float(v)) for v in vals))
+        rows.append("99,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,0")  # not parameterized: skipped
+        back = native.Am1Parameters.from_csv("\n".join(rows), method)
+        assert back.elements == ps.elements
+    try:
+        native.Am1Parameters.for_method("am1").element(2)
+    except native.Am1GpuError as err:
+        assert err.code == 2
+    else:
+        raise AssertionError("helium must be refused")

@@ -1,8 +1,8 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle, on a B200.
 
-Tolerances are the north-star bars for the plain FP64 path: heat of formation within 1e-6
-kcal/mol, Mulliken charges within 1e-7 e, density within 1e-8 max-abs; operators (H_core,
-Fock) within 1e-10 eV, eigenvalues within 1e-10 relative.  Eigenvectors are compared through
+Tolerances are the bars for the plain FP64 path: heat of formation within 1e-6 kcal/mol,
+Mulliken charges within 1e-7 e, density within 1e-8 max-abs, dipole within 1e-6 D; operators
+(H_core, Fock) within 1e-10 eV, eigenvalues within 1e-10 relative.  Eigenvectors are compared through
 sign- and rotation-invariant quantities (reconstruction, density), as the reference's own tests do.
 """
 
@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 HOF_TOL = 1e-6      # kcal/mol
 Q_TOL = 1e-7        # e
 P_TOL = 1e-8        # max |dP|
+MU_TOL = 1e-6       # Debye, each Cartesian component of the dipole
 OP_TOL = 1e-10      # eV, operator elements
 
 
@@ -36,6 +37,10 @@ def _compare_scf(g, o, tag):
     assert np.max(np.abs(g["charges"] - o["charges"])) < Q_TOL, tag
     if "density" in g and "density" in o:
         assert np.max(np.abs(g["density"] - o["density"])) < P_TOL, (tag, np.max(np.abs(g["density"] - o["density"])))
+    # point-charge plus s-p hybrid dipole (src/scf.rs:410-427)
+    dmu = np.max(np.abs(np.array(g["dipole_debye"]) - np.array(o["dipole_debye"])))
+    assert dmu < MU_TOL, (tag, dmu)
+    assert abs(g["dipole_magnitude"] - o["dipole_magnitude"]) < MU_TOL, tag
     assert abs(g["iterations"] - o["iterations"]) <= 1, (tag, g["iterations"], o["iterations"])
 
 
@@ -130,6 +135,18 @@ def test_co2_spectrum(gpu, ref_values, method, tag):
     assert abs(g["charges"][0] - ref["charge_carbon"]) < tol["charge"]
 
 
+def test_water_dipole_band(gpu, ref_values):
+    # src/scf.rs:1298-1312: water's AM1 dipole is 1.86 +- 0.15 D, and lies in the molecular plane
+    w = ref_values["scf_water"]
+    z, xyz = atoms_to_arrays(w["atoms"])
+    g = gpu.scf(z, xyz)
+    mu = np.array(g["dipole_debye"])
+    assert abs(g["dipole_magnitude"] - w["dipole_debye"]) < w["dipole_tol"], g["dipole_magnitude"]
+    assert abs(np.linalg.norm(mu) - g["dipole_magnitude"]) < 1e-12
+    normal = np.cross(xyz[1] - xyz[0], xyz[2] - xyz[0])
+    assert abs(np.dot(mu, normal)) < 1e-10 * np.linalg.norm(normal)
+
+
 def test_uhf_radical_and_forced_references(gpu, oracle, ref_values):
     m = ref_values["scf_methyl_radical"]
     z, xyz = atoms_to_arrays(m["atoms"])
@@ -214,6 +231,46 @@ def test_batch_matches_oracle_and_solo(gpu, oracle):
         assert np.array_equal(solo["density"], res[i]["density"])
 
 
+def _largest_config1_molecules():
+    """The largest molecules of the 4096-molecule benchmark's size range: C30H62, C40H82 (242
+    orbitals), water clusters of 43, 50 and 64 monomers (258, 300 and 384 orbitals, past the
+    256-orbital cut-over of the on-chip kernels) and the C40H81 radical (UHF, 241 orbitals)."""
+    from am1gpu import workloads as W, _abi
+
+    rng = np.random.default_rng(31)
+    mols = []
+    for n in (30, 40):
+        a = W.alkane(n, rng)
+        mols.append((f"C{n}H{2 * n + 2}", a.numbers, _abi.angstrom_to_bohr(a.xyz), 1))
+    for k in (43, 50, 64):
+        w = W.water_cluster(k, rng)
+        mols.append((f"(H2O){k}", w.numbers, _abi.angstrom_to_bohr(w.xyz), 1))
+    r = W.alkane(40, rng, radical=True)
+    mols.append(("C40H81 radical", r.numbers, _abi.angstrom_to_bohr(r.xyz), 2))
+    return mols
+
+
+def test_largest_batch_molecules_match_oracle(gpu, oracle):
+    mols = _largest_config1_molecules()
+    for name, z, xyz, mult in mols:
+        g = gpu.scf(z, xyz, 0.0, mult)
+        o = oracle.scf(z, xyz, 0.0, mult)
+        _compare_scf(g, o, name)
+        assert np.max(np.abs(g["mo_energies"] - o["mo_energies"])) < 1e-7, name
+        if mult == 2:
+            assert g["unrestricted"]
+            assert np.max(np.abs(g["spin_density"] - o["spin_density"])) < P_TOL, name
+            assert np.max(np.abs(g["beta_energies"] - o["beta_energies"])) < 1e-7, name
+    # the same molecules in one batch: every result equal to its solo run, bit for bit
+    status, res = gpu.scf_batch([(z, xyz, 0.0, mult) for _, z, xyz, mult in mols], want_matrices=True)
+    assert all(s == 0 for s in status), status
+    for (name, z, xyz, mult), r in zip(mols, res):
+        solo = gpu.scf(z, xyz, 0.0, mult)
+        assert solo["heat_of_formation_kcal"] == r["heat_of_formation_kcal"], name
+        assert np.array_equal(solo["density"], r["density"]), name
+        assert solo["dipole_debye"] == r["dipole_debye"], name
+
+
 def test_orbital_energies_match_oracle(gpu, oracle, ref_values):
     # mo_energies are the eigenvalues of the last extrapolated Fock matrix (src/scf.rs:654-689)
     for name, z, xyz in _golden_molecules(ref_values):
@@ -296,3 +353,65 @@ def test_symmetric_eigen_batch(gpu):
         assert np.max(np.abs(v @ np.diag(w) @ v.T - a)) < 1e-9
         w1, v1 = gpu.eigh(a)
         assert np.array_equal(w1, w) and np.array_equal(v1, v)
+
+
+def test_caller_parameter_set(gpu, oracle, ref_values):
+    # run_am1(molecule, params, options) takes any &Am1Parameters (src/scf.rs:294; the elements map
+    # is public and Am1Parameters::from_csv builds custom sets, src/params.rs:61-70,139): a custom
+    # set must change the GPU result exactly as it changes the oracle's
+    import ctypes
+
+    from am1gpu import native, workloads as W, _abi
+
+    std = native.Am1Parameters.for_method("am1")
+    mols = _golden_molecules(ref_values)
+    a = W.alkane(6, np.random.default_rng(12))
+    mols.append(("hexane", a.numbers, _abi.angstrom_to_bohr(a.xyz)))
+    # the built-in set passed explicitly: the default call, bit for bit
+    for name, z, xyz in mols:
+        d = gpu.scf(z, xyz)
+        e = gpu.scf(z, xyz, params=std)
+        assert d["heat_of_formation_kcal"] == e["heat_of_formation_kcal"], name
+        assert np.array_equal(d["density"], e["density"]), name
+    # carbon U_ss + 0.1 eV, and a derived field (hydrogen rho0 x 1.01), which is used as given
+    mod = std.copy()
+    mod.elements[6]["u_ss"] += 0.1
+    mod.elements[1]["rho0"] *= 1.01
+    for name, z, xyz in mols:
+        g = gpu.scf(z, xyz, params=mod)
+        o = oracle.scf(z, xyz, params=mod)
+        _compare_scf(g, o, name)
+        assert abs(g["heat_of_formation_kcal"] - gpu.scf(z, xyz)["heat_of_formation_kcal"]) > 1e-3, name
+    # the set's method is the calculation's: the built-in RM1 set equals method="rm1"
+    z, xyz = mols[0][1], mols[0][2]
+    r1 = gpu.scf(z, xyz, params=native.Am1Parameters.for_method("rm1"))
+    r2 = gpu.scf(z, xyz, method="rm1")
+    assert r1["heat_of_formation_kcal"] == r2["heat_of_formation_kcal"]
+    # batched and gradient calls take the set too; each batch result equals its solo run
+    batch = [(z, xyz, 0.0, 1) for _, z, xyz in mols]
+    status, res = gpu.scf_batch(batch, want_matrices=True, params=mod)
+    assert all(s == 0 for s in status), status
+    for (name, z, xyz), r in zip(mols, res):
+        solo = gpu.scf(z, xyz, params=mod)
+        assert r["heat_of_formation_kcal"] == solo["heat_of_formation_kcal"], name
+    gst, gres = gpu.gradient_batch(batch, params=mod)
+    gst0, gres0 = gpu.gradient_batch(batch)
+    assert all(s == 0 for s in gst)
+    for r, r0 in zip(gres, gres0):
+        assert np.max(np.abs(r["gradient"].sum(axis=0))) < 1e-8  # translation invariance
+        assert np.max(np.abs(r["gradient"] - r0["gradient"])) > 1e-6  # the set is used
+    # an element the set lacks, and malformed sets
+    no_o = native.Am1Parameters({k: v for k, v in std.elements.items() if k != 8}, "am1")
+    w = gpu.scf(*atoms_to_arrays(ref_values["scf_water"]["atoms"]), params=no_o)
+    assert w["status"] == _abi.ELEMENT_NOT_PARAMETERIZED and "Z=8" in w["error"]
+    mb = _abi.MolBuffers(*atoms_to_arrays(ref_values["scf_water"]["atoms"]))
+    rb = _abi.ResultBuffers(3, 6, False)
+    o = _abi.default_options()
+    twice = (_abi.Element * 2)(_abi.element_from_dict(std.elements[1]), _abi.element_from_dict(std.elements[1]))
+    t = _abi.ParamTable(method=0, count=2, elements=twice)
+    rc = _abi.lib().am1gpu_scf_params(ctypes.byref(mb.mol), ctypes.byref(t), ctypes.byref(o), ctypes.byref(rb.res))
+    assert rc == _abi.INVALID_INPUT and b"twice" in _abi.lib().am1gpu_last_error()
+    bad = std.copy()
+    bad.elements[8]["g_ss"] = float("nan")
+    w = gpu.scf(*atoms_to_arrays(ref_values["scf_water"]["atoms"]), params=bad)
+    assert w["status"] == _abi.INVALID_INPUT

@@ -98,8 +98,9 @@ def stein_prep(d, e, eps):
     return tn, EPS * tn, shift, cl, cl_list
 
 
-def stein_solve(d, e, shift, Z, U, scale, floor_, first, n):
-    """k_stein_solve, every thread k at once."""
+def stein_solve(d, e, shift, Z, U, scale, floor_, first, n, last=False, tn=1.0):
+    """k_stein_solve, every thread k at once.  Returns the growth-test flags of the last solve
+    (True where a vector falls below sqrt(0.1 / n) / (n eps ||T||))."""
     nn = n * n
     k = np.arange(n)
     lam = shift
@@ -140,6 +141,9 @@ def stein_solve(d, e, shift, Z, U, scale, floor_, first, n):
     nrm = np.sqrt(np.sum(Z.a[: nn].reshape(n, n) ** 2, axis=0))
     assert np.all(nrm > 0) and np.all(np.isfinite(nrm))
     scale[:] = 1.0 / nrm
+    if not last:
+        return np.zeros(n, dtype=bool)
+    return nrm * (n * EPS * tn) < np.sqrt(0.1 / n)
 
 
 def stein_orth(Z, Zt, cl, cl_list, scale, n):
@@ -203,8 +207,9 @@ def back_transform_emulated(Wm, d, e):
     Zt = Buf(nn)
     scale = np.ones(n)
     for it in range(4):
-        stein_solve(d, e, shift, Z, Ubuf, scale, floor_, it == 0, n)
+        bad = stein_solve(d, e, shift, Z, Ubuf, scale, floor_, it == 0, n, last=it == 3, tn=tn)
         stein_orth(Z, Zt, cl, cl_list, scale, n)
+    assert not bad.any(), "growth test failed on an accurate spectrum"
     Z.a[:nn] = (Z.a[:nn].reshape(n, n) * scale[None, :]).ravel()
     # back-transformation: Vt | V | Uw share the factor storage
     U = Ubuf
@@ -270,3 +275,23 @@ def test_emulated_path_degenerate_and_split():
     _check(a)
     _check(np.diag(np.arange(70.0)))
     _check(np.zeros((67, 67)))
+
+
+def test_growth_test_flags_a_shift_that_is_no_eigenvalue():
+    # the last solve's growth test (bit 4 of counts[1], LINALG): with the exact eigenvalues every
+    # vector passes; a shift halfway between two eigenvalues gives a growth of about 2 / gap, far
+    # below the threshold, and only that vector is flagged
+    rng = np.random.default_rng(5)
+    n = 90
+    a = rng.standard_normal((n, n))
+    Wf, d, e = reduce_store(a + a.T)
+    eps = np.linalg.eigvalsh(np.diag(d) + np.diag(e[: n - 1], 1) + np.diag(e[: n - 1], -1))
+    tn, floor_, shift, cl, cl_list = stein_prep(d, e, eps)
+    bad_k = 40
+    shift = shift.copy()
+    shift[bad_k] = 0.5 * (eps[bad_k] + eps[bad_k + 1])
+    Z, U, Zt, scale = Buf(n * n), Buf(3 * n * n), Buf(n * n), np.ones(n)
+    for it in range(4):
+        bad = stein_solve(d, e, shift, Z, U, scale, floor_, it == 0, n, last=it == 3, tn=tn)
+        stein_orth(Z, Zt, cl, cl_list, scale, n)
+    assert bad[bad_k] and bad.sum() == 1

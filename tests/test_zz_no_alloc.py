@@ -5,7 +5,8 @@ owns the whole device memory pool, or in a real-time loop, or only hold device b
 them -- so this entry point takes device pointers for its input and outputs and keeps its
 scratch in a fixed array inside the library.  Here its results are checked, through the C ABI,
 against the existing (allocating) am1gpu_symmetric_eigen on the same matrices, on two calls in a
-row (the second call must not see anything left over from the first).  The file is named to be
+row (the second call must not see anything left over from the first), and the device's free
+memory is checked to stay the same across calls.  The file is named to be
 collected last, so a run that stops at its first failure has run every other test before it.
 """
 
@@ -76,3 +77,41 @@ def test_noalloc_eigensolver_refuses_what_it_cannot_hold(gpu):
     b[3, 1] = np.nan
     rc, _, _ = _noalloc(lib, torch, b)
     assert rc == _abi.LINALG
+
+
+def test_noalloc_eigensolver_allocates_no_device_memory(gpu):
+    # the property the entry point exists for: after one warm call (which loads the kernels and
+    # fetches the scratch address), further calls -- here from a host thread the library has not
+    # seen, so no per-thread workspace exists for it -- leave the device's free memory unchanged
+    import threading
+
+    import torch
+
+    from am1gpu import _abi
+
+    lib = _abi.lib()
+    n = 100
+    rng = np.random.default_rng(99)
+    m = rng.standard_normal((n, n))
+    a = m + m.T
+    da = torch.from_numpy(a).to("cuda")
+    dw = torch.empty(n, dtype=torch.float64, device="cuda")
+    dv = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    args = (n, ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(dw.data_ptr()), ctypes.c_void_p(dv.data_ptr()), None)
+    assert lib.am1gpu_symmetric_eigen_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    codes = []
+
+    def worker():
+        for _ in range(3):
+            codes.append(lib.am1gpu_symmetric_eigen_noalloc(*args))
+
+    t = threading.Thread(target=worker)
+    t.start()
+    t.join()
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert codes == [0, 0, 0], lib.am1gpu_last_error().decode()
+    assert free_after == free_before, (free_before, free_after)
+    _check_against_allocating(gpu, dw.cpu().numpy(), dv.cpu().numpy(), a)
