@@ -64,6 +64,27 @@ def sample_order(n, seed=7):
     return np.random.default_rng(seed).permutation(n)
 
 
+CPU_SAMPLE = 64  # molecules per CPU-baseline step
+
+
+def stratified_sample(mols, k=CPU_SAMPLE):
+    """k molecules spread evenly over the batch sorted by orbital count: the middle molecule of each of
+    k equal strata.  The sample's size mix, and so its CPU cost per molecule (which grows with n^3),
+    matches the whole batch's, so the CPU's solves/s on the sample is its rate on the batch."""
+    nao = np.array([int(np.sum(np.where(m[0] == 1, 1, 4))) for m in mols])
+    order = np.argsort(nao, kind="stable")
+    n = len(mols)
+    return [int(order[min(n - 1, int((i + 0.5) * n / k))]) for i in range(k)]
+
+
+def bench_config(nmol):
+    """The workload, as both arms (this library and the reference's CPU path) state it."""
+    return {"workload": WORKLOAD, "molecules": nmol,
+            "cpu_sample": f"{CPU_SAMPLE} molecules per step, one from the middle of each of {CPU_SAMPLE} equal strata of "
+                          "the batch sorted by orbital count (the batch's size mix)",
+            "l2": "device state ~25 GB, larger than L2: no flush needed between steps"}
+
+
 # ---------------------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------------------
@@ -127,20 +148,18 @@ class ClockSampler:
 SP2_DRAM_PER_ALG_BYTE = 0.866
 
 
-def oracle_rate(mols, order, budget_s, threads, chunk=None):
+def oracle_rate(mols, sample, budget_s, threads):
+    """The oracle on `threads` host threads (one molecule per thread at a time) over the stratified
+    sample, repeated until `budget_s` has passed (at least once): (solves/s, solves, seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     O.lib()
-    chunk = chunk or max(threads * 2, 16)
-    done, t0, k = 0, time.perf_counter(), 0
+    step = [mols[i] for i in sample]
+    done, t0 = 0, time.perf_counter()
     while True:
-        idx = order[k: k + chunk]
-        if len(idx) == 0:
-            break
-        st, _ = O.scf_batch([mols[i] for i in idx], nthreads=threads)
-        done += len(idx)
-        k += chunk
+        O.scf_batch(step, nthreads=threads)
+        done += len(step)
         if time.perf_counter() - t0 >= budget_s:
             break
     el = time.perf_counter() - t0
@@ -152,13 +171,12 @@ def run_reference(args):
     if rank != 0:
         return
     mols = workload(args.nmol)
-    order = sample_order(len(mols))
     threads = os.cpu_count() or 1
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     O.lib()
-    step = [mols[i] for i in order[:48]]
+    step = [mols[i] for i in stratified_sample(mols)]
     times = []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -173,10 +191,11 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generators)",
-        "config": {"workload": WORKLOAD, "sample": f"48 molecules of the batch in a fixed random order per step"},
+        "config": bench_config(len(mols)),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": "48 molecules of the 4096-molecule batch (fixed random order), per step; "
-                                   "C++ restatement of am1-rs's SCF (the Rust reference cannot be built here)"},
+                         "sample": f"{len(step)} molecules per step, stratified by orbital count over the "
+                                   f"{len(mols)}-molecule batch; C++ restatement of am1-rs's SCF, one molecule per "
+                                   "host thread (the Rust reference cannot be built here)"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -228,6 +247,50 @@ def config0_block(native, _abi, oracle_mod, reps=5):
             "published_reference_cpu_s": 0.27,
             "published_reference_note": "am1-rs full SCF, 32-water cluster (4.0 A spacing, not this geometry), "
                                         "16 cores (docs/divide-conquer.md:408-412)"}
+
+
+def serving_block(native, _abi, oracle_mod, n_requests=2000, rate=2000.0, cpu_budget_s=20.0):
+    """Per-request latency on a short stream of the serving workload: n_requests open-loop Poisson
+    arrivals at `rate` per second (sizes log-uniform on [3, 600] atoms, RHF:UHF = 9:1, seed 2) through the
+    continuous-batching server (3 workers and a priority lane for requests of at most 448 orbitals, 2
+    workers), after 64 warm-up requests.  Beside it, the oracle's per-request solve time on all host
+    threads, request after request in stream order, until cpu_budget_s has passed (service time only: a
+    CPU server that queued these arrivals would add its waiting time)."""
+    from am1gpu import workloads as W
+    from am1gpu.serve import ScfServer, run_stream
+
+    reqs = W.serving_stream(n_requests, rate, seed=2)
+    with ScfServer(workers=3, small_lane=448, small_workers=2) as srv:
+        warm = [srv.submit(r.mol.numbers, _abi.angstrom_to_bohr(r.mol.xyz), r.mol.charge, r.mol.multiplicity) for r in reqs[:64]]
+        for f in warm:
+            f.result()
+        out, wall = run_stream(reqs, srv)
+        stats = srv.stats
+    lat = np.array([o[2] for o in out]) * 1e3
+    ok = sum(1 for o in out if o[0] == 0)
+    threads = os.cpu_count() or 1
+    oracle_mod.set_threads(threads)
+    cpu_lat = []
+    t_start = time.perf_counter()
+    for r in reqs:
+        t0 = time.perf_counter()
+        oracle_mod.scf(r.mol.numbers, _abi.angstrom_to_bohr(r.mol.xyz), r.mol.charge, r.mol.multiplicity, want_matrices=False)
+        cpu_lat.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > cpu_budget_s:
+            break
+    oracle_mod.set_threads(1)
+    cl = np.array(cpu_lat) * 1e3
+    return {
+        "workload": f"{n_requests} requests of the serving stream (open-loop Poisson arrivals at {rate:g}/s, sizes "
+                    "log-uniform on [3, 600] atoms, RHF:UHF = 9:1, seed 2)",
+        "server": "3 workers + a 448-orbital priority lane of 2 workers, FP64",
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max()),
+                       "per": "request (arrival to result)"},
+        "solves_per_s": len(out) / wall, "offered_per_s": rate, "failed": len(out) - ok, "batches": stats.batches,
+        "cpu_oracle_latency_ms": {"p50": float(np.percentile(cl, 50)), "p99": float(np.percentile(cl, 99)),
+                                  "n": int(cl.size), "threads": threads,
+                                  "per": "request, solve time alone (the first requests of the same stream, in order)"},
+    }
 
 
 def run_ours(args):
@@ -343,9 +406,10 @@ def run_ours(args):
     line = None
     if rank == 0:
         order = sample_order(nmol)
-        # plain path: one molecule at a time through am1gpu_scf
+        strat = stratified_sample(mols)
+        # plain path: one molecule at a time through am1gpu_scf, on the stratified sample (the batch's size mix)
         native.set_timing(False)
-        plain_idx = order[: args.plain_sample]
+        plain_idx = strat[: args.plain_sample]
         t0 = time.perf_counter()
         for i in plain_idx:
             native.scf(*mols[i][:2], want_matrices=False)
@@ -362,9 +426,10 @@ def run_ours(args):
         dhf_m64 = max(abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) for a, b in zip(res, res_m))
         dq_m64 = max(float(np.max(np.abs(a["charges"] - b["charges"]))) for a, b in zip(res, res_m))
         cfg0 = config0_block(native, _abi, O)
-        # CPU baseline: the oracle on the host cores, bounded sample
+        serving = serving_block(native, _abi, O)
+        # CPU baseline: the oracle on the host cores, the stratified sample (as the reference arm times it)
         threads = os.cpu_count() or 1
-        cpu_rate, cpu_done, cpu_s = oracle_rate(mols, order, args.cpu_seconds, threads)
+        cpu_rate, cpu_done, cpu_s = oracle_rate(mols, strat, args.cpu_seconds, threads)
 
         # roofline of the dominant kernel: the purification step (symmetric X.X, FP64 mma.sync)
         ph = {k: sum(s["phase_ms"][k] for s in stats) / args.steps for k in stats[0]["phase_ms"]}
@@ -399,14 +464,17 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded generators; no dataset)",
-            "config": {"workload": WORKLOAD, "molecules": nmol, "aos_total": int(nao.sum()),
-                       "max_aos": int(nao.max()), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (device state ~25 GB), no flush needed",
-                       "converged": conv, "failed": len(bad), "scf_iterations_mean": float(iters.mean()),
-                       "scf_iterations_max": int(iters.max())},
-            "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-                           "per": "batch step (all 4096 molecules)"},
-            "plain": {"value": plain_rate, "unit": "solves/s", "sample": f"{len(plain_idx)} molecules, one am1gpu_scf call each",
+            "config": bench_config(nmol),
+            "run": {"aos_total": int(nao.sum()), "max_aos": int(nao.max()),
+                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                    "converged": conv, "failed": len(bad), "scf_iterations_mean": float(iters.mean()),
+                    "scf_iterations_max": int(iters.max())},
+            "latency_ms": serving["latency_ms"],
+            "serving": serving,
+            "step_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                        "per": "batch step (all molecules)"},
+            "plain": {"value": plain_rate, "unit": "solves/s",
+                      "sample": f"{len(plain_idx)} molecules (the stratified CPU sample), one am1gpu_scf call each",
                       "batched_over_plain": value / world / plain_rate},
             "parity": {"sample": len(par_idx), "max_abs_dHf_kcal_vs_oracle": dhf, "bar": 1e-4},
             "config0": cfg0,
@@ -447,8 +515,8 @@ def run_ours(args):
                               "share_of_step": ph["scf:fock"] / step_dev_ms},
             "phases_ms_per_step": ph,
             "cpu_baseline": {"value": cpu_rate, "unit": "solves/s", "cores": threads, "kind": "port",
-                             "sample": f"{cpu_done} molecules of the batch (fixed random order) in {cpu_s:.1f} s; "
-                                       "C++ restatement of am1-rs's SCF on all host threads"},
+                             "sample": f"{cpu_done} solves of the {len(strat)}-molecule stratified sample in {cpu_s:.1f} s; "
+                                       "C++ restatement of am1-rs's SCF, one molecule per host thread"},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "gpu_launches_note": "FP64 timed region (the mixed and e2e regions are timed separately)",
             "clocks": clk,

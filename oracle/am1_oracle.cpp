@@ -48,8 +48,10 @@ thread_local bool t_serial = false;
 // which threads are not worth starting.
 template <class F>
 void par_for(int n, double work, F&& f) {
-    int nt = g_inner_threads.load();
-    if (nt <= 1 || t_serial || work < 2.0e5 || n < 2 * nt) {
+    // each thread takes at least ~2e5 operations and 16 rows, so that starting it costs little
+    // next to its share (a host with hundreds of threads would otherwise spend its time starting them)
+    int nt = std::min(g_inner_threads.load(), (int)std::min(work / 2.0e5, (double)n / 16.0));
+    if (nt <= 1 || t_serial) {
         f(0, n);
         return;
     }

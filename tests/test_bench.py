@@ -20,6 +20,11 @@ def test_reference_arm_prints_its_line():
                 "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert line["config"] == bench.bench_config(4096)  # the same config our arm prints
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
@@ -46,3 +51,22 @@ def test_workload_and_config0_helper():
     assert gpu.calls == 4 and oracle.calls == 1  # a warm-up call, then the timed ones
     assert r["iterations"] == 10 and abs(r["abs_dHf_kcal_vs_oracle"] - 1e-9) < 1e-12
     assert r["published_reference_cpu_s"] == 0.27 and r["gpu_scf_s"] >= 0.0 and r["oracle_threads"] == 1
+
+
+def test_stratified_cpu_sample_has_the_batch_size_mix():
+    # both arms time the CPU on the same 64 molecules; their orbital counts follow the batch's, so
+    # the CPU's cost per molecule (about n^3) on the sample is its cost on the batch
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+    import numpy as np
+
+    import bench
+
+    mols = bench.workload(4096)
+    nao = np.array([int(np.sum(np.where(m[0] == 1, 1, 4))) for m in mols], dtype=float)
+    idx = bench.stratified_sample(mols)
+    assert len(idx) == bench.CPU_SAMPLE == len(set(idx))
+    s = nao[idx]
+    assert abs(s.mean() / nao.mean() - 1) < 0.02
+    assert abs((s ** 3).mean() / (nao ** 3).mean() - 1) < 0.05
+    assert bench.stratified_sample(mols) == idx  # deterministic
