@@ -170,6 +170,7 @@ class CallStats(ctypes.Structure):
         ("purification_bytes", ctypes.c_double),
         ("lowp_purification_steps", ctypes.c_double),
         ("lowp_purification_flops", ctypes.c_double),
+        ("graph_launches", ctypes.c_int64),
     ]
 
 
@@ -253,6 +254,7 @@ def stats_dict(st: CallStats) -> dict:
         "purification_bytes": float(st.purification_bytes),
         "lowp_purification_steps": float(st.lowp_purification_steps),
         "lowp_purification_flops": float(st.lowp_purification_flops),
+        "graph_launches": int(st.graph_launches),
     }
 
 _lib = None

@@ -258,6 +258,7 @@ struct Mem {
     char* hpin = nullptr;
     size_t hcap = 0;
     std::vector<cudaEvent_t> events;  // timing events, reused across calls
+    cudaStream_t cap_stream = nullptr;  // stream the SCF graph is captured on
 };
 
 // Stream priority asked for by the calling host thread (am1gpu_set_stream_priority).
@@ -294,6 +295,7 @@ void mem_release(Mem& w) {
     if (w.hpin) cudaFreeHost(w.hpin);
     for (auto e : w.events) cudaEventDestroy(e);
     if (w.stream) cudaStreamDestroy(w.stream);
+    if (w.cap_stream) cudaStreamDestroy(w.cap_stream);
     w = Mem();
 }
 
@@ -611,6 +613,11 @@ struct Batch {
     long long arena_doubles = 0;
     const DevElem* d_params = nullptr;  // the call's own parameter table (staged with the inputs), or NULL: the built-in upload
     int* d_big_stall = nullptr;  // per channel job: 1 when a large molecule's purification stalled this iteration
+    GraphLoop* d_loop = nullptr;  // loop counters of the captured solve
+    GraphLoop* h_loop = nullptr;  // their pinned host copy
+    int64_t graph_counts[3] = {0, 0, 0};  // kernels per captured head (+ arm), step (+ condition), tail (+ condition)
+    bool graph_cacheable = false;  // a resident batch keeps its instantiated graph across runs
+    cudaGraphExec_t graph_exec = nullptr;
 };
 
 // Lays out the batch in one device pool and one pinned staging area, copies inputs.
@@ -704,6 +711,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_eps = take(dv, sizeof(double) * std::max<long long>(eps_total, 1));
     const size_t o_grad = take(dv, sizeof(double) * 3 * std::max<long long>(natoms, 1));
     const size_t o_bstall = take(dv, sizeof(int) * std::max<long long>(nch_total, 1));
+    const size_t o_loop = take(dv, sizeof(GraphLoop));
     const size_t dtotal = align256(dv);
     // pinned staging also receives the outputs
     size_t hs = staged;
@@ -713,6 +721,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t h_o_chg = take(hs, sizeof(double) * std::max<long long>(natoms, 1));
     const size_t h_o_eps = take(hs, sizeof(double) * std::max<long long>(eps_total, 1));
     const size_t h_o_grad = take(hs, sizeof(double) * 3 * std::max<long long>(natoms, 1));
+    const size_t h_o_loop = take(hs, sizeof(GraphLoop));
     int rc = mem_ensure(mem, dtotal, align256(hs));
     if (rc) return rc;
     Mem* ws = &mem;
@@ -754,6 +763,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_eps = (double*)dptr(o_eps);
     b.d_grad = (double*)dptr(o_grad);
     b.d_big_stall = (int*)dptr(o_bstall);
+    b.d_loop = (GraphLoop*)dptr(o_loop);
+    b.h_loop = (GraphLoop*)(Hs + h_o_loop);
     b.eps_total = eps_total;
     b.h_active = (int*)(Hs + h_o_active);
     b.h_work = (double*)(Hs + h_o_work);
@@ -1192,13 +1203,14 @@ int launch_big_tridiag(Batch& b, cudaStream_t s, int64_t* launches) {
     return AM1GPU_OK;
 }
 
-int launch_jacobi(Batch& b, Mem* ws, int force, const int* mask = nullptr) {
+// stream: where to launch (NULL: the workspace's own stream)
+int launch_jacobi(Batch& b, Mem* ws, int force, const int* mask = nullptr, cudaStream_t stream = nullptr) {
     for (auto& bk : b.buckets) {
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(bk.count * bk.C, 1, 1);
         cfg.blockDim = dim3(256, 1, 1);
         cfg.dynamicSmemBytes = bk.smem;
-        cfg.stream = ws->stream;
+        cfg.stream = stream ? stream : ws->stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = bk.C;
@@ -1209,6 +1221,266 @@ int launch_jacobi(Batch& b, Mem* ws, int force, const int* mask = nullptr) {
         CK(cudaLaunchKernelEx(&cfg, k_jacobi, (const EigJob*)(b.d_eig + bk.off), (const MolState*)b.d_st, b.d_status, force,
                               mask));
     }
+    return AM1GPU_OK;
+}
+
+// One SCF iteration's launches, shared by the host-driven loop and the captured graph.
+struct IterEnq {
+    Batch& b;
+    Mem* ws;
+    cudaStream_t s;
+    const DevElem* dp;
+    ScfParams prm;
+    int nblk, rowblk, njobs;
+    Run* run;
+    size_t ph;  // start event of the phase being timed
+};
+
+// Fock build, commutator and history, extrapolation, and (purification path) the spectral bounds
+// and the start of the purification.
+int enq_head(IterEnq& e, bool lowp_left) {
+    (void)lowp_left;
+    Batch& b = e.b;
+    const cudaStream_t s = e.s;
+    Run& run = *e.run;
+    int rc;
+    CK(cudaMemsetAsync(b.d_active, 0, 4 * sizeof(int), s));
+    if ((rc = run.begin(&e.ph))) return rc;
+    k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, e.dp, b.d_atom_z, b.d_wstore, b.d_arena, b.d_st, 0);
+    run.launched(AM1GPU_PHASE_FOCK);
+    if ((rc = run.end(AM1GPU_PHASE_FOCK, e.ph)) || (rc = run.begin(&e.ph))) return rc;
+    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+        if (pairs) k_commutator16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+        else k_commutator8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+    });
+    k_post_fock<<<dim3(e.nblk, e.njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, e.nblk, 0, 0);
+    run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
+    if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, e.ph)) || (rc = run.begin(&e.ph))) return rc;
+    k_diis_solve<<<cdiv(b.nmol, 64), 64, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, e.nblk, e.prm);
+    k_combine<<<dim3(e.rowblk, e.njobs), 256, 0, s>>>(b.d_jobs, b.d_st, 0);
+    run.launched(AM1GPU_PHASE_ACCEL, 2);
+    if ((rc = run.end(AM1GPU_PHASE_ACCEL, e.ph)) || (rc = run.begin(&e.ph))) return rc;
+    if (density_mode() == 0) {
+        // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
+        k_sp2_bounds<<<e.njobs, 512, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
+        if ((rc = launch_big_bounds(b, s))) return rc;
+        k_sp2_init<<<dim3(b.sp2_nblk, e.njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
+        k_sp2_start<<<cdiv(e.njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, e.njobs, b.sp2_nblk);
+        CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
+        run.launched(AM1GPU_PHASE_EIGEN,
+                     3 + big_launches(big_split((int)b.sp2_big.size(), [&](int i) { return b.jobs[b.sp2_big[i]].n; }),
+                                      (int)b.sp2_big.size()));
+    }
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+// One purification step of every channel still purifying: the FP64 products (and the TF32 ones
+// while any molecule may be in its TF32 phase), then the trace bookkeeping.  zero_count: clear the
+// count of channels still purifying first (the captured loop's condition kernel clears it instead).
+int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
+    Batch& b = e.b;
+    const cudaStream_t s = e.s;
+    Run& run = *e.run;
+    int rc;
+    size_t pc;
+    if ((rc = run.begin(&pc))) return rc;
+    int nl = 0;
+    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
+        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+        ++nl;
+    });
+    if (lowp_left) {
+        launch_tiles(b, s, [&](const GemmTile* t, int nt, bool) {
+            k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+            ++nl;
+        });
+    }
+    run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
+    if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
+    if (zero_count) CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
+    k_sp2_update<<<cdiv(e.njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, e.njobs, sp2_max, b.d_sp2_active, b.d_work);
+    run.launched(AM1GPU_PHASE_EIGEN);
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+// The density of the iteration (the purified X, or the eigensolver for stalled and Jacobi-path
+// molecules), the density change and the convergence test.
+int enq_tail(IterEnq& e) {
+    Batch& b = e.b;
+    const cudaStream_t s = e.s;
+    Run& run = *e.run;
+    int rc;
+    if (density_mode() == 0) {
+        const unsigned fin_blocks = std::max(8u, std::min(256u, cdiv((long long)b.maxn * b.maxn, 65536)));
+        k_sp2_finish<<<dim3(fin_blocks, e.njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_work,
+                                                               b.d_big_stall, b.d_active + 3);
+        run.launched(AM1GPU_PHASE_EIGEN);
+        if (!b.sp2_big.empty() && (rc = big_fallback(b, e.ws))) return rc;
+        // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
+        k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
+        if ((rc = launch_jacobi(b, e.ws, 0, b.d_need_eigen, e.s))) return rc;
+        run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
+        if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
+        k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
+        run.launched(AM1GPU_PHASE_EIGEN, 3);
+        if ((rc = run.end(AM1GPU_PHASE_EIGEN, e.ph)) || (rc = run.begin(&e.ph))) return rc;
+    } else {
+        k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, nullptr);
+        CK(cudaGetLastError());
+        size_t pj;
+        if ((rc = run.begin(&pj))) return rc;
+        if ((rc = launch_jacobi(b, e.ws, 0, nullptr, e.s))) return rc;
+        run.launched(AM1GPU_PHASE_DENSITY_CORE, (int)b.buckets.size());
+        if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pj))) return rc;
+        if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
+        run.launched(AM1GPU_PHASE_EIGEN, 2);
+        if ((rc = run.end(AM1GPU_PHASE_EIGEN, e.ph)) || (rc = run.begin(&e.ph))) return rc;
+        k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, nullptr);
+        run.launched(AM1GPU_PHASE_DENSITY);
+    }
+    k_density_post<<<dim3(e.nblk, e.njobs), 256, 0, s>>>(b.d_jobs, b.d_st, e.nblk);
+    k_converge<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, e.nblk, e.prm,
+                                                 b.d_active);
+    run.launched(AM1GPU_PHASE_DENSITY, 2);
+    if ((rc = run.end(AM1GPU_PHASE_DENSITY, e.ph))) return rc;
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+// The captured solve (AM1GPU_GRAPH, default on): the SCF loop runs as one graph launch whose loops
+// are decided on the device, so the host reads nothing until the solve ends.  Not for batches
+// with molecules above 448 orbitals (their purification bounds and reductions take cooperative
+// launches, and their fallback reads flags on the host), the mixed path (whose TF32 launches the
+// host drops once no molecule is in its TF32 phase), the Jacobi density path, or when phase timing
+// is on (the phase events sit between launches).
+bool graph_ok(const Batch& b, const am1gpu_options& o, bool timed) {
+    static const int env = [] {
+        const char* v = std::getenv("AM1GPU_GRAPH");
+        return v ? std::atoi(v) : 1;
+    }();
+    return env != 0 && !timed && density_mode() == 0 && o.precision != AM1GPU_PRECISION_MIXED && b.sp2_big.empty() &&
+           b.tri_big.empty() && b.nmol > 0 && o.max_scf > 0;
+}
+
+// Adds the work `fn` enqueues on stream cs to graph g after `deps` (capture into the graph), and
+// returns the single node the captured sequence ends on.
+template <class F>
+int capture_into(cudaStream_t cs, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphNode_t* last, F&& fn) {
+    CK(cudaStreamBeginCaptureToGraph(cs, g, deps, nullptr, ndeps, cudaStreamCaptureModeRelaxed));
+    int rc = fn();
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* tail = nullptr;
+    size_t ntail = 0;
+    cudaError_t e1 = cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &tail, &ntail);
+    cudaGraphNode_t last_node = (e1 == cudaSuccess && ntail == 1) ? tail[0] : nullptr;
+    cudaGraph_t out = g;
+    cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+    if (rc) return rc;
+    if (e1 != cudaSuccess) return fail(AM1GPU_DEVICE_ERROR, std::string("capture info: ") + cudaGetErrorString(e1));
+    if (e2 != cudaSuccess) return fail(AM1GPU_DEVICE_ERROR, std::string("end capture: ") + cudaGetErrorString(e2));
+    if (!last_node) return fail(AM1GPU_DEVICE_ERROR, "captured sequence does not end on one node");
+    *last = last_node;
+    return AM1GPU_OK;
+}
+
+// A WHILE node after `dep` in g, with handle h; its body graph in *body.
+int add_while(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    CK(cudaGraphAddNode(node, g, &dep, 1, &np));
+    *body = np.conditional.phGraph_out[0];
+    return AM1GPU_OK;
+}
+
+// The SCF loop of run_device as one graph launch:
+//   k_scf_arm -> WHILE(scf) { head -> k_sp2_arm -> WHILE(sp2) { step -> k_sp2_cond } -> tail -> k_scf_cond }
+// The kernels are the eager loop's, in the same order; only the loop decisions moved to the device
+// (k_graph.cu), so the results are the same bit for bit.  The purification loop stops as soon as no
+// channel purifies (the eager loop looks every six steps from the twelfth on); the extra eager
+// steps change nothing, because finished channels skip their products.
+// *launched: the graph was launched (an error before that leaves the stream untouched).
+int scf_loop_graph(IterEnq& e, const am1gpu_options& o, bool* launched) {
+    Batch& b = e.b;
+    Mem& m = *e.ws;
+    const int sp2_max = sp2_max_steps();
+    if (!m.cap_stream) CK(cudaStreamCreateWithFlags(&m.cap_stream, cudaStreamNonBlocking));
+    const cudaStream_t cs = m.cap_stream;
+    if (b.graph_cacheable && b.graph_exec) {  // a resident batch's graph, captured on its first run
+        *launched = true;
+        CK(cudaGraphLaunch(b.graph_exec, e.s));
+        CK(cudaMemcpyAsync(b.h_loop, b.d_loop, sizeof(GraphLoop), cudaMemcpyDeviceToHost, e.s));
+        return AM1GPU_OK;
+    }
+    am1gpu_call_stats cnt{};  // launches per captured sequence
+    Run crun{e.ws, &cnt, false};
+    IterEnq ce = e;
+    ce.s = cs;
+    ce.run = &crun;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    struct GraphGuard {
+        cudaGraph_t g;
+        ~GraphGuard() {
+            if (g) cudaGraphDestroy(g);
+        }
+    } guard{g};
+    cudaGraphConditionalHandle h_scf, h_sp2;
+    CK(cudaGraphConditionalHandleCreate(&h_scf, g, 0, 0));
+    int rc;
+    cudaGraphNode_t arm, w_scf, head, w_sp2, step, tail;
+    if ((rc = capture_into(cs, g, nullptr, 0, &arm, [&]() -> int {
+             k_scf_arm<<<1, 32, 0, cs>>>(h_scf, b.d_loop, o.max_scf);
+             return AM1GPU_OK;
+         })))
+        return rc;
+    cudaGraph_t body = nullptr, body2 = nullptr;
+    if ((rc = add_while(g, arm, h_scf, &w_scf, &body))) return rc;
+    CK(cudaGraphConditionalHandleCreate(&h_sp2, body, 0, 0));
+    const int64_t head0 = cnt.kernel_launches;
+    if ((rc = capture_into(cs, body, nullptr, 0, &head, [&]() -> int {
+             int r = enq_head(ce, false);
+             if (r) return r;
+             k_sp2_arm<<<1, 32, 0, cs>>>(h_sp2, b.d_loop, b.d_sp2_active);
+             return AM1GPU_OK;
+         })))
+        return rc;
+    const int64_t per_head = cnt.kernel_launches - head0 + 1;
+    if ((rc = add_while(body, head, h_sp2, &w_sp2, &body2))) return rc;
+    const int64_t step0 = cnt.kernel_launches;
+    if ((rc = capture_into(cs, body2, nullptr, 0, &step, [&]() -> int {
+             int r = enq_step(ce, sp2_max, false, false);
+             if (r) return r;
+             k_sp2_cond<<<1, 32, 0, cs>>>(h_sp2, b.d_loop, b.d_sp2_active, sp2_max);
+             return AM1GPU_OK;
+         })))
+        return rc;
+    const int64_t per_step = cnt.kernel_launches - step0 + 1;
+    const int64_t tail0 = cnt.kernel_launches;
+    if ((rc = capture_into(cs, body, &w_sp2, 1, &tail, [&]() -> int {
+             int r = enq_tail(ce);
+             if (r) return r;
+             k_scf_cond<<<1, 32, 0, cs>>>(h_scf, b.d_loop, b.d_active, o.max_scf);
+             return AM1GPU_OK;
+         })))
+        return rc;
+    const int64_t per_tail = cnt.kernel_launches - tail0 + 1;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaGraphInstantiate(&ge, g, 0));
+    *launched = true;
+    const cudaError_t le = cudaGraphLaunch(ge, e.s);
+    if (b.graph_cacheable && le == cudaSuccess) b.graph_exec = ge;
+    else cudaGraphExecDestroy(ge);  // an executable graph still running is freed once it completes
+    CK(le);
+    CK(cudaMemcpyAsync(b.h_loop, b.d_loop, sizeof(GraphLoop), cudaMemcpyDeviceToHost, e.s));
+    b.graph_counts[0] = per_head;
+    b.graph_counts[1] = per_step;
+    b.graph_counts[2] = per_tail;
     return AM1GPU_OK;
 }
 
@@ -1243,110 +1515,45 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     CK(cudaGetLastError());
     if ((rc = run.end(AM1GPU_PHASE_CORE, ph))) return rc;
     ScfParams prm{o.max_scf, o.use_diis, o.accelerator, o.e_tol, o.p_tol, o.adiis_switch, lowp_switch(), lowp_max_iter()};
-    const int nblk = b.nblk;
-    const int rowblk = std::max(1, std::min(64, (b.maxn + 7) / 8));
+    IterEnq e{b, ws, s, dp, prm, b.nblk, std::max(1, std::min(64, (b.maxn + 7) / 8)), njobs, &run, 0};
     int done = 0;
-    const int check = b.nmol > 64 ? 4 : 1;
-    while (done < o.max_scf) {
-        for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
-            CK(cudaMemsetAsync(b.d_active, 0, 4 * sizeof(int), s));
-            if ((rc = run.begin(&ph))) return rc;
-            k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena,
-                                                      b.d_st, 0);
-            run.launched(AM1GPU_PHASE_FOCK);
-            if ((rc = run.end(AM1GPU_PHASE_FOCK, ph)) || (rc = run.begin(&ph))) return rc;
-            launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-                if (pairs) k_commutator16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
-                else k_commutator8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
-            });
-            k_post_fock<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, nblk, 0, 0);
-            run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
-            if ((rc = run.end(AM1GPU_PHASE_COMMUTATOR, ph)) || (rc = run.begin(&ph))) return rc;
-            k_diis_solve<<<cdiv(b.nmol, 64), 64, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm);
-            k_combine<<<dim3(rowblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, 0);
-            run.launched(AM1GPU_PHASE_ACCEL, 2);
-            if ((rc = run.end(AM1GPU_PHASE_ACCEL, ph)) || (rc = run.begin(&ph))) return rc;
-            if (density_mode() == 0) {
-                // purification: P from F* by SP2, eigensolver only for molecules whose purification stalls
-                k_sp2_bounds<<<njobs, 512, 3 * sizeof(double) * b.maxn, s>>>(b.d_sp2, b.d_st);
-                if ((rc = launch_big_bounds(b, s))) return rc;
-                k_sp2_init<<<dim3(b.sp2_nblk, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.sp2_nblk);
-                k_sp2_start<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, njobs, b.sp2_nblk);
-                CK(cudaMemsetAsync(b.d_need_eigen, 0, sizeof(int) * b.nmol, s));
-                run.launched(AM1GPU_PHASE_EIGEN,
-                             3 + big_launches(big_split((int)b.sp2_big.size(), [&](int i) { return b.jobs[b.sp2_big[i]].n; }),
-                                              (int)b.sp2_big.size()));
-                const int sp2_max = sp2_max_steps();
-                for (int step = 0; step < sp2_max; ++step) {
-                    size_t pc;
-                    if ((rc = run.begin(&pc))) return rc;
-                    // FP64 steps (jobs in a TF32 run skip them), then the TF32 steps while any
-                    // molecule may be in its TF32 phase
-                    int nl = 0;
-                    launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-                        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                        ++nl;
-                    });
-                    if (lowp_left) {
-                        launch_tiles(b, s, [&](const GemmTile* t, int nt, bool) {
-                            k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-                            ++nl;
-                        });
-                    }
-                    run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
-                    if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
-                    CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
-                    k_sp2_update<<<cdiv(njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, njobs, sp2_max, b.d_sp2_active,
-                                                                  b.d_work);
-                    run.launched(AM1GPU_PHASE_EIGEN);
-                    if (step >= 12 && (step % 6) == 5) {
-                        CK(cudaMemcpyAsync(b.h_active + 1, b.d_sp2_active, sizeof(int), cudaMemcpyDeviceToHost, s));
-                        CK(cudaStreamSynchronize(s));
-                        if (b.h_active[1] == 0) break;
+    bool graph = graph_ok(b, o, run.timed);
+    if (graph) {
+        bool launched = false;
+        rc = scf_loop_graph(e, o, &launched);
+        if (rc && launched) return rc;
+        if (rc) {  // the graph could not be built here: the host-driven loop runs the same kernels
+            graph = false;
+            cudaGetLastError();
+        }
+    }
+    if (!graph) {
+        const int check = b.nmol > 64 ? 4 : 1;
+        while (done < o.max_scf) {
+            for (int k = 0; k < check && done < o.max_scf; ++k, ++done) {
+                if ((rc = enq_head(e, lowp_left))) return rc;
+                if (density_mode() == 0) {
+                    const int sp2_max = sp2_max_steps();
+                    for (int step = 0; step < sp2_max; ++step) {
+                        if ((rc = enq_step(e, sp2_max, lowp_left, true))) return rc;
+                        if (step >= 12 && (step % 6) == 5) {
+                            CK(cudaMemcpyAsync(b.h_active + 1, b.d_sp2_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+                            CK(cudaStreamSynchronize(s));
+                            if (b.h_active[1] == 0) break;
+                        }
                     }
                 }
-                const unsigned fin_blocks = std::max(8u, std::min(256u, cdiv((long long)b.maxn * b.maxn, 65536)));
-                k_sp2_finish<<<dim3(fin_blocks, njobs), 256, 0, s>>>(b.d_sp2, b.d_sp2_state, b.d_st, b.d_need_eigen, b.d_work,
-                                                                     b.d_big_stall, b.d_active + 3);
-                run.launched(AM1GPU_PHASE_EIGEN);
-                if (!b.sp2_big.empty() && (rc = big_fallback(b, ws))) return rc;
-                // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
-                k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
-                if ((rc = launch_jacobi(b, ws, 0, b.d_need_eigen))) return rc;
-                run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
-                if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
-                k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
-                run.launched(AM1GPU_PHASE_EIGEN, 3);
-                if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
-            } else {
-                k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, nullptr);
-                CK(cudaGetLastError());
-                size_t pj;
-                if ((rc = run.begin(&pj))) return rc;
-                if ((rc = launch_jacobi(b, ws, 0))) return rc;
-                run.launched(AM1GPU_PHASE_DENSITY_CORE, (int)b.buckets.size());
-                if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pj))) return rc;
-                if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, nullptr);
-                run.launched(AM1GPU_PHASE_EIGEN, 2);
-                if ((rc = run.end(AM1GPU_PHASE_EIGEN, ph)) || (rc = run.begin(&ph))) return rc;
-                k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, nullptr);
-                run.launched(AM1GPU_PHASE_DENSITY);
+                if ((rc = enq_tail(e))) return rc;
             }
-            k_density_post<<<dim3(nblk, njobs), 256, 0, s>>>(b.d_jobs, b.d_st, nblk);
-            k_converge<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, nblk, prm,
-                                                         b.d_active);
-            run.launched(AM1GPU_PHASE_DENSITY, 2);
-            if ((rc = run.end(AM1GPU_PHASE_DENSITY, ph))) return rc;
-            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(b.h_active, b.d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+            if (lowp_left) CK(cudaMemcpyAsync(b.h_active + 2, b.d_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (*b.h_active == 0) break;
+            if (lowp_left && b.h_active[2] == 0) lowp_left = false;  // no molecule returns to TF32
         }
-        CK(cudaMemcpyAsync(b.h_active, b.d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
-        if (lowp_left) CK(cudaMemcpyAsync(b.h_active + 2, b.d_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        if (*b.h_active == 0) break;
-        if (lowp_left && b.h_active[2] == 0) lowp_left = false;  // no molecule returns to TF32
     }
     stats->scf_cycles = done;
+    const int nblk = b.nblk;
     // final energy at the final density (src/scf.rs:698-701, 835-839) and the result records
     if ((rc = run.begin(&ph))) return rc;
     k_fock<<<cdiv(b.natoms, 8), 256, 0, s>>>(b.d_mols, b.d_atom_mol, b.natoms, dp, b.d_atom_z, b.d_wstore, b.d_arena, b.d_st, 1);
@@ -1372,6 +1579,13 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     stats->eigen_fallbacks += (int32_t)b.h_work[2];
     stats->lowp_purification_steps += b.h_work[4];
     stats->lowp_purification_flops += b.h_work[5];
+    if (graph) {  // what the captured loops launched
+        const GraphLoop lp = *b.h_loop;
+        stats->scf_cycles = lp.scf_iter;
+        stats->kernel_launches += 1 + (int64_t)lp.scf_iter * (b.graph_counts[0] + b.graph_counts[2]) +
+                                  (int64_t)lp.sp2_total * b.graph_counts[1];
+        stats->graph_launches += 1;
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, mem.events[t0], mem.events[t1]));
     stats->device_ms += ms;
@@ -2435,6 +2649,7 @@ int am1gpu_batch_create(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_
     }
     if (!plans.empty()) {
         rc = build_batch(mols, *opts, std::move(plans), h->b, h->mem, &h->stats);
+        h->b.graph_cacheable = true;
         if (!rc && cudaStreamSynchronize(h->mem.stream) != cudaSuccess) rc = fail(AM1GPU_DEVICE_ERROR, "upload failed");
         if (rc) {
             mem_release(h->mem);
@@ -2483,6 +2698,10 @@ int am1gpu_batch_results(am1gpu_batch* h, am1gpu_result* results, int32_t* statu
 
 void am1gpu_batch_destroy(am1gpu_batch* h) {
     if (!h) return;
+    if (h->b.graph_exec) {
+        cudaStreamSynchronize(h->mem.stream);
+        cudaGraphExecDestroy(h->b.graph_exec);
+    }
     am1::mem_release(h->mem);
     delete h;
 }

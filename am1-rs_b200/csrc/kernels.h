@@ -1,6 +1,8 @@
 // Kernel interfaces of libam1gpu (device side), shared with the host driver.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 
 #include "am1gpu_internal.h"
@@ -97,6 +99,18 @@ struct TriJob {
     double* eps;       // ascending eigenvalues, n
     int n, mol;
 };
+
+// Loop counters of the captured solve (k_graph.cu), in device memory.
+struct GraphLoop {
+    int scf_iter;   // SCF iterations done in this launch
+    int sp2_step;   // purification steps of the current iteration
+    int sp2_total;  // purification steps of this launch
+    int pad;
+};
+__global__ void k_scf_arm(cudaGraphConditionalHandle h, GraphLoop* loop, int max_scf);
+__global__ void k_sp2_arm(cudaGraphConditionalHandle h, GraphLoop* loop, int* active_count);
+__global__ void k_sp2_cond(cudaGraphConditionalHandle h, GraphLoop* loop, int* active_count, int max_steps);
+__global__ void k_scf_cond(cudaGraphConditionalHandle h, GraphLoop* loop, const int* active, int max_scf);
 
 struct ScfParams {
     int max_scf, use_diis, accelerator;

@@ -325,6 +325,7 @@ typedef struct {
     double purification_bytes;   /* their algorithmic HBM traffic: 16 n^2 per product (read X, write X^2) */
     double lowp_purification_steps;  /* products X.X of the mixed path's reduced-precision (TF32) iterations */
     double lowp_purification_flops;  /* their algorithmic work, n^3 each (not in purification_flops) */
+    int64_t graph_launches;      /* 1 when the SCF loop ran as one CUDA graph launch with device-side loops, 0 when the host drove it */
 } am1gpu_call_stats;
 
 /* Per-phase CUDA-event timing on (1) or off (0); the default follows AM1_TIMING. */

@@ -57,7 +57,11 @@ def test_largest_clusters_match_recorded_oracle(gpu, name):
     g = gpu.scf(m.numbers, xyz, want_matrices=False)
     assert g["status"] == 0 and g["converged"], g.get("error")
     assert g["nao"] == rec["nao"]
-    assert abs(g["heat_of_formation_kcal"] - rec["heat_of_formation_kcal"]) < 1e-6
+    # the heat of formation within 1e-11 of the total energy's magnitude (4e-5 kcal/mol for 512
+    # waters): an energy of 1.8e5 eV summed over 9.4 million matrix elements in a different order
+    # (blocks of a GPU reduction against the reference's eight-lane sums) differs by a few 1e-12 of it
+    tol = max(1e-6, 1e-11 * abs(rec["energy_ev"]) * 23.061)
+    assert abs(g["heat_of_formation_kcal"] - rec["heat_of_formation_kcal"]) < tol
     assert np.max(np.abs(g["charges"] - np.array(rec["charges"]))) < 1e-7
     assert np.max(np.abs(np.array(g["dipole_debye"]) - np.array(rec["dipole_debye"]))) < 1e-6
     assert abs(g["homo_ev"] - rec["homo_ev"]) < 1e-7 and abs(g["lumo_ev"] - rec["lumo_ev"]) < 1e-7

@@ -415,3 +415,48 @@ def test_caller_parameter_set(gpu, oracle, ref_values):
     bad.elements[8]["g_ss"] = float("nan")
     w = gpu.scf(*atoms_to_arrays(ref_values["scf_water"]["atoms"]), params=bad)
     assert w["status"] == _abi.INVALID_INPUT
+
+
+def test_captured_solve_equals_host_driven_loop(gpu):
+    # The SCF loop as one CUDA graph launch (device-side WHILE loops) must give the host-driven
+    # loop's results bit for bit: phase timing forces the host-driven loop, so the same calls are
+    # made with timing on and off.  A resident batch reuses its graph across runs.
+    from am1gpu import workloads as W, _abi
+
+    rng = np.random.default_rng(77)
+    mols = []
+    for n in (1, 4, 13, 30):
+        a = W.alkane(n, rng)
+        mols.append((a.numbers, _abi.angstrom_to_bohr(a.xyz), 0.0, 1))
+    for k in (2, 11, 40):
+        w = W.water_cluster(k, rng)
+        mols.append((w.numbers, _abi.angstrom_to_bohr(w.xyz), 0.0, 1))
+    r = W.alkane(7, rng, radical=True)
+    mols.append((r.numbers, _abi.angstrom_to_bohr(r.xyz), 0.0, 2))
+    try:
+        gpu.set_timing(True)
+        st_e, res_e = gpu.scf_batch(mols, want_matrices=True)
+        assert gpu.last_call_stats()["graph_launches"] == 0
+        solo_e = gpu.scf(*mols[3][:2])
+        gpu.set_timing(False)
+        st_g, res_g = gpu.scf_batch(mols, want_matrices=True)
+        stats = gpu.last_call_stats()
+        assert stats["graph_launches"] == 1 and stats["scf_cycles"] == max(x["iterations"] for x in res_g)
+        solo_g = gpu.scf(*mols[3][:2])
+        assert gpu.last_call_stats()["graph_launches"] == 1
+    finally:
+        gpu.set_timing(False)
+    assert st_e == st_g and all(s == 0 for s in st_g)
+    for a, b in zip(res_e, res_g):
+        assert a["heat_of_formation_kcal"] == b["heat_of_formation_kcal"] and a["iterations"] == b["iterations"]
+        assert np.array_equal(a["density"], b["density"]) and np.array_equal(a["charges"], b["charges"])
+    assert solo_e["heat_of_formation_kcal"] == solo_g["heat_of_formation_kcal"]
+    rb = gpu.ResidentBatch(mols)
+    try:
+        for _ in range(2):
+            rb.run()
+            assert rb.stats()["graph_launches"] == 1
+            st, res = rb.results()
+            assert [x["heat_of_formation_kcal"] for x in res] == [x["heat_of_formation_kcal"] for x in res_g]
+    finally:
+        rb.close()
