@@ -220,6 +220,8 @@ SIGNATURES = {
     "am1gpu_g_matrix_batch": (ctypes.c_int, [ctypes.POINTER(Molecule), ctypes.c_int32, ctypes.c_int32, _dp, _dp]),
     "am1gpu_symmetric_eigen": (ctypes.c_int, [ctypes.c_int32, _dp, _dp, _dp]),
     "am1gpu_symmetric_eigenvalues": (ctypes.c_int, [ctypes.c_int32, _dp, _dp]),
+    "am1gpu_lowp_tuning": (ctypes.c_int, [_ip, ctypes.POINTER(ctypes.c_float)]),
+    "am1gpu_density_purify": (ctypes.c_int, [ctypes.c_int32, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _dp, _ip]),
     "am1gpu_set_stream_priority": (ctypes.c_int, [ctypes.c_int32]),
     "am1gpu_symmetric_eigen_batch": (
         ctypes.c_int,

@@ -362,6 +362,32 @@ def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
     return g
 
 
+PURIFY_PRECISION = {"fp64": 0, "fp32_tcgen05": 1, "tf32": 2}
+
+
+def density_purify(f, n_occ, weight=2.0, precision="fp64"):
+    """P = weight * projector onto the n_occ lowest eigenvectors of symmetric f (n <= 448), by
+    purification at one of the batched path's product precisions (``am1gpu_density_purify``).
+    Returns (P, number of products)."""
+    a = np.ascontiguousarray(f, dtype=np.float64)
+    p = np.zeros_like(a)
+    steps = ctypes.c_int32()
+    _check(_abi.lib().am1gpu_density_purify(a.shape[0], a.ctypes.data_as(_dp), float(n_occ), float(weight),
+                                            PURIFY_PRECISION[precision], p.ctypes.data_as(_dp), ctypes.byref(steps)))
+    return p, steps.value
+
+
+def lowp_tuning() -> dict:
+    """The autotuner's choice of reduced-precision purification kernel per size class on this device
+    (``am1gpu_lowp_tuning``): {class: {"kernel": "tcgen05" | "mma.sync tf32" | None, "ms": (mma.sync, tcgen05)}}."""
+    choice = (ctypes.c_int32 * 4)()
+    ms = (ctypes.c_float * 8)()
+    _check(_abi.lib().am1gpu_lowp_tuning(choice, ms))
+    names = ["n<=128", "n<=256", "n<=384", "n>384"]
+    kern = {1: "tcgen05", 0: "mma.sync tf32", -1: None}
+    return {names[c]: {"kernel": kern[choice[c]], "ms": (ms[2 * c], ms[2 * c + 1])} for c in range(4)}
+
+
 def eigvalsh(a):
     """Ascending eigenvalues of a symmetric matrix (up to 8192 rows), ``am1gpu_symmetric_eigenvalues``."""
     a = np.ascontiguousarray(a, dtype=np.float64)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cstdlib>
 #include <cmath>
@@ -224,6 +225,8 @@ int device_ctx(DeviceCtx** out) {
         if ((err = cudaFuncSetAttribute(k_sp2_step_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf32_smem_bytes())) !=
             cudaSuccess)
             return bad("tf32 tile kernel smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_sp2_step_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes())) != cudaSuccess)
+            return bad("tcgen05 tile kernel smem attribute", err);
         for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8, (const void*)k_dgemm16,
                               (const void*)k_dgemm8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
@@ -364,6 +367,37 @@ int sp2_max_steps() {
         return k < 1 ? kSp2MaxSteps : std::min(k, kSp2MaxSteps);
     }();
     return v;
+}
+
+// Which molecules' reduced-precision purification products run on tcgen05 (k_sp2_step_tc, FP32
+// accuracy from 3xTF32) rather than mma.sync TF32 (k_sp2_step_tf32).  AM1GPU_LOWP_TC=1 or 0 forces
+// one kernel; otherwise the autotuner's choice for the molecule's size class (tune_lowp_kernels,
+// run once per device and class before the first mixed batch that holds such a molecule).
+constexpr int kTuneClasses = 4;
+inline int tune_class(int n) { return n <= 128 ? 0 : n <= 256 ? 1 : n <= 384 ? 2 : 3; }
+constexpr int kTuneSize[kTuneClasses] = {96, 192, 320, 448};  // the matrix each class is timed on
+struct LowpTune {
+    std::mutex mu;
+    int choice[kTuneClasses] = {-1, -1, -1, -1};  // -1 untuned, 1 tcgen05, 0 mma.sync TF32
+    float ms[kTuneClasses][2] = {};                // time of one purification (mma.sync, tcgen05)
+};
+LowpTune g_lowp_tune[64];
+
+int lowp_tc_env() {
+    static const int v = [] {
+        const char* e = std::getenv("AM1GPU_LOWP_TC");
+        return e ? std::atoi(e) : -1;
+    }();
+    return v;
+}
+
+bool lowp_tc_for(int n) {
+    const int env = lowp_tc_env();
+    if (env >= 0) return env != 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    const int c = g_lowp_tune[dev].choice[tune_class(n)];
+    return c != 0;  // untuned classes (the tuner could not run) take tcgen05
 }
 
 int density_mode() {
@@ -587,6 +621,8 @@ struct Batch {
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
+    GemmTile* d_tc_tiles = nullptr;  // 128 x 128 upper-triangle tiles of the tcgen05 reduced-precision step
+    int nt_tc = 0;
     Sp2State* d_sp2_state;
     TriJob* d_tri;
     int* d_need_eigen;
@@ -648,11 +684,14 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.nblk = std::max(1, std::min(32, (maxn + 15) / 16));
     const int nblk = b.nblk;
     // GEMM tile counts
-    int tiles_nn = 0, tiles_up = 0;
+    int tiles_nn = 0, tiles_up = 0, tiles_tc = 0;
+    const bool mixed = o.precision == AM1GPU_PRECISION_MIXED;
     for (auto& p : b.plans) {
         const int tn = (p.nao + 63) / 64;
         tiles_nn += p.nch * tn * tn;
         tiles_up += p.nch * tn * (tn + 1) / 2;
+        const int tc = (p.nao + 127) / 128;
+        if (mixed && lowp_tc_for(p.nao)) tiles_tc += p.nch * tc * (tc + 1) / 2;
     }
     const int sp2_nblk = std::max(1, std::min(32, (maxn + 7) / 8));
     // ---- staged (host -> device) region layout
@@ -677,6 +716,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_eig = take(st, sizeof(EigJob) * nch_total);
     const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
     const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
+    const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
     const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
@@ -742,6 +782,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_eig = (EigJob*)dptr(o_eig);
     b.d_sp2 = (Sp2Job*)dptr(o_sp2);
     b.d_sp2_tiles = (GemmTile*)dptr(o_sp2t);
+    b.d_tc_tiles = (GemmTile*)dptr(o_tct);
+    GemmTile* htct = (GemmTile*)(Hs + o_tct);
+    int ntc = 0;
     b.d_tri = (TriJob*)dptr(o_tri);
     b.d_sp2_big = (int*)dptr(o_sp2big);
     b.d_need_eigen = (int*)dptr(o_need);
@@ -909,6 +952,14 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.ldf = (int)((n + 3) & ~3LL);  // FP32 iterates of the mixed path: in the VS slot, 16-byte aligned
             sj.Xf0 = (float*)(((uintptr_t)(base + SLOT_VS * nn) + 15) & ~(uintptr_t)15);
             sj.Xf1 = sj.Xf0 + n * sj.ldf;
+            sj.lowp_tc = (mixed && lowp_tc_for((int)n)) ? 1 : 0;
+            sj.tc_tile0 = ntc;
+            if (sj.lowp_tc) {
+                const int tc = (int)((n + 127) / 128);
+                for (int x = 0; x < tc; ++x)
+                    for (int y = x; y < tc; ++y) htct[ntc++] = GemmTile{job, x, y};
+            }
+            sj.tc_ntiles = ntc - sj.tc_tile0;
             if (!sj.fallback) b.sp2_big.push_back(job);
             sj.tile0 = (int)tl.size();  // tile index inside its own launch
             for (int x = 0; x < (int)tn_; ++x)
@@ -967,6 +1018,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     for (size_t i = 0; i < tiles_pairs.size(); ++i) hsp2t[i] = tiles_pairs[i];
     for (size_t i = 0; i < tiles_other.size(); ++i) hsp2t[tiles_pairs.size() + i] = tiles_other[i];
     b.nt_sp2_pairs = (int)tiles_pairs.size();
+    b.nt_tc = ntc;
     b.nt_sp2 = (int)(tiles_pairs.size() + tiles_other.size());
     // eigen jobs grouped by cluster size, largest first inside a group
     std::vector<int> idx(eig_all.size());
@@ -1296,6 +1348,10 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
             k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
             ++nl;
         });
+        if (b.nt_tc > 0) {
+            k_sp2_step_tc<<<b.nt_tc, 128, tc_smem_bytes(), s>>>(b.d_sp2, b.d_tc_tiles, b.nt_tc, b.d_sp2_state, b.d_sp2_active + 2);
+            ++nl;
+        }
     }
     run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
@@ -1497,6 +1553,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.begin(&ph))) return rc;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, s));
     CK(cudaMemsetAsync(b.d_work, 0, sizeof(double) * kWorkN, s));
+    CK(cudaMemsetAsync(b.d_sp2_active, 0, 4 * sizeof(int), s));  // [2]: error word of the tcgen05 step
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * b.arena_doubles, s));
     // mixed precision: every molecule starts with TF32 purification (k_converge ends that phase)
     const bool mixed = o.precision == AM1GPU_PRECISION_MIXED && density_mode() == 0;
@@ -1572,7 +1629,9 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     size_t t1;
     if ((rc = run.event(&t1))) return rc;
     CK(cudaMemcpyAsync(b.h_work, b.d_work, sizeof(double) * kWorkN, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(b.h_active + 2, b.d_sp2_active + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (b.h_active[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
     stats->purification_steps += b.h_work[0];
     stats->purification_flops += b.h_work[1];
     stats->purification_bytes += b.h_work[3];
@@ -1727,6 +1786,55 @@ void fill_empty(am1gpu_result* r) {
 }  // namespace
 
 // grads (optional): one caller buffer of 3 * natoms doubles per molecule for the nuclear gradient
+int density_purify_one(int n, const double* F, double nocc, double weight, int precision, double* P, int* steps_out,
+                       Mem* mem_override);
+
+// The autotuner of the reduced-precision purification kernel: for each size class not yet tuned on
+// this device, one AM1-like matrix of the class's size (spectrum in [-40, -12] eV occupied and
+// [1, 10] eV virtual, the same matrix for both) is purified with each kernel after a warm-up, and
+// the faster one is kept for the process (both reach the same FP32-level density; the tcgen05 one
+// is the more accurate).  Runs in its own device pool, before the batch is laid out.
+int tune_lowp_kernels(const std::vector<MolPlan>& plans) {
+    if (lowp_tc_env() >= 0) return AM1GPU_OK;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return AM1GPU_OK;
+    LowpTune& t = g_lowp_tune[dev];
+    bool need[kTuneClasses] = {false, false, false, false};
+    for (const auto& p : plans) need[tune_class(p.nao)] = true;
+    std::lock_guard<std::mutex> lock(t.mu);
+    const std::string saved = g_err;
+    for (int c = 0; c < kTuneClasses; ++c) {
+        if (!need[c] || t.choice[c] >= 0) continue;
+        const int n = kTuneSize[c], nocc = (2 * n) / 3;
+        std::vector<double> f((size_t)n * n, 0.0), p((size_t)n * n);
+        // F = diag(spectrum) + a small symmetric coupling: a gapped, dense matrix
+        for (int i = 0; i < n; ++i) {
+            f[(size_t)i * n + i] = i < nocc ? -40.0 + 28.0 * i / std::max(1, nocc - 1) : 1.0 + 9.0 * (i - nocc) / std::max(1, n - nocc - 1);
+            for (int j = 0; j < i; ++j) {
+                const double v = 0.05 * std::sin(0.37 * i + 0.91 * j);
+                f[(size_t)i * n + j] = f[(size_t)j * n + i] = v;
+            }
+        }
+        float best[2] = {0.f, 0.f};
+        bool ok = true;
+        for (int prec : {2, 1}) {  // 2: mma.sync TF32, 1: tcgen05
+            for (int rep = 0; rep < 3 && ok; ++rep) {
+                const auto t0 = std::chrono::steady_clock::now();
+                int steps = 0;
+                if (density_purify_one(n, f.data(), nocc, 2.0, prec, p.data(), &steps, &tl_mem_eig)) ok = false;
+                const float ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                if (rep > 0) best[prec == 1] = rep == 1 ? ms : std::min(best[prec == 1], ms);
+            }
+        }
+        t.ms[c][0] = best[0];
+        t.ms[c][1] = best[1];
+        t.choice[c] = ok ? (best[1] <= best[0] ? 1 : 0) : 1;
+    }
+    g_err = saved;
+    return AM1GPU_OK;
+}
+
 // params (optional): the caller's parameter set, whose method replaces opts->method
 int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts_in, am1gpu_result* res, int* status,
               double* const* grads = nullptr, const am1gpu_param_table* params = nullptr) {
@@ -1796,6 +1904,7 @@ int scf_batch(int nmol, const am1gpu_molecule* mols, const am1gpu_options* opts_
         Batch b;
         Workspace* ws;
         rc = workspace(&ws, 0, 0);
+        if (!rc && opts->precision == AM1GPU_PRECISION_MIXED) rc = tune_lowp_kernels(plans);
         if (!rc) rc = build_batch(mols, *opts, std::move(plans), b, *ws, &tl_stats, -1.0, tab_all);
         const DevElem* dp = b.d_params ? b.d_params : ctx->d_params;
         if (!rc) rc = run_device(b, *ws, dp, *opts, &tl_stats);
@@ -2172,6 +2281,149 @@ int big_fallback(Batch& b, Mem* ws) {
     }
     CK(cudaMemsetAsync(b.d_active + 3, 0, sizeof(int), s));
     CK(cudaStreamSynchronize(s));
+    return AM1GPU_OK;
+}
+
+// Density of one symmetric matrix F by purification, P = w * (projector onto its nocc lowest
+// eigenvectors): the step an SCF iteration takes after the extrapolation (the reference's
+// symmetric_eigen + density_from_coeff, src/scf.rs:654-661, 503-524), alone, at the precision of
+// the batched path's products: 0 FP64 tensor cores (k_sp2_step16/8), 1 FP32-accurate products on
+// tcgen05 (k_sp2_step_tc, 3xTF32), 2 TF32 mma.sync (k_sp2_step_tf32).  The reduced-precision runs
+// stop at their own rounding floor and are rescaled to the exact trace, as in the mixed SCF.
+int density_purify_one(int n, const double* F, double nocc, double weight, int precision, double* P, int* steps_out,
+                       Mem* mem_override = nullptr) {
+    g_err.clear();
+    if (n < 1 || n > 448 || !F || !P) return fail(AM1GPU_INVALID_INPUT, "n must be 1..448 and the pointers non-null");
+    if (precision < 0 || precision > 2) return fail(AM1GPU_INVALID_INPUT, "precision must be 0, 1 or 2");
+    if (!(nocc >= 0.0 && nocc <= n)) return fail(AM1GPU_INVALID_INPUT, "nocc outside 0..n");
+    for (long long i = 0; i < (long long)n * n; ++i)
+        if (!std::isfinite(F[i])) return fail(AM1GPU_LINALG, "the matrix is not finite");
+    DeviceCtx* ctx;
+    int rc = device_ctx(&ctx);
+    if (rc) return rc;
+    const long long nn = (long long)n * n;
+    const int ldf = (n + 3) & ~3;
+    const int t64 = (n + 63) / 64, t128 = (n + 127) / 128;
+    const int nt64 = t64 * (t64 + 1) / 2, nt128 = t128 * (t128 + 1) / 2;
+    const int nblk = sp2_init_blocks(n);
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+        off = align256(off);
+        const size_t o = off;
+        off += bytes;
+        return o;
+    };
+    const size_t o_job = take(sizeof(Sp2Job)), o_t64 = take(sizeof(GemmTile) * nt64), o_t128 = take(sizeof(GemmTile) * nt128),
+                 o_ms = take(sizeof(MolState)), o_f = take(8 * nn), o_rmin = take(8 * (size_t)n), o_rmax = take(8 * (size_t)n);
+    const size_t staged = align256(off);
+    const size_t o_sst = take(sizeof(Sp2State)), o_bnd = take(16), o_x0 = take(8 * nn), o_x1 = take(8 * nn), o_p = take(8 * nn),
+                 o_part = take(16 * (size_t)std::max(32, nt64)), o_xf = take(8 * (size_t)n * ldf + 64), o_need = take(16),
+                 o_work = take(8 * kWorkN), o_act = take(16), o_stall = take(16);
+    Workspace* ws;
+    if (mem_override) {
+        if ((rc = mem_ensure(*mem_override, align256(off), staged + align256(sizeof(Sp2State)) + 256))) return rc;
+        ws = mem_override;
+    } else if ((rc = workspace(&ws, align256(off), staged + align256(sizeof(Sp2State)) + 256))) {
+        return rc;
+    }
+    char* D = ws->dpool;
+    char* H = ws->hpin;
+    const cudaStream_t s = ws->stream;
+    Sp2Job jb{};
+    jb.F = (const double*)(D + o_f);
+    jb.rowmin = (const double*)(D + o_rmin);
+    jb.rowmax = (const double*)(D + o_rmax);
+    jb.X0 = (double*)(D + o_x0);
+    jb.X1 = (double*)(D + o_x1);
+    jb.P = (double*)(D + o_p);
+    jb.part = (double*)(D + o_part);
+    jb.bounds = (double*)(D + o_bnd);
+    jb.nocc = nocc;
+    jb.weight = weight;
+    jb.n = n;
+    jb.mol = 0;
+    jb.tile0 = 0;
+    jb.ntiles = nt64;
+    jb.fallback = 1;
+    jb.ldf = ldf;
+    jb.Xf0 = (float*)(((uintptr_t)(D + o_xf) + 15) & ~(uintptr_t)15);
+    jb.Xf1 = jb.Xf0 + (size_t)n * ldf;
+    jb.lowp_tc = precision == 1 ? 1 : 0;
+    jb.tc_tile0 = 0;
+    jb.tc_ntiles = precision == 1 ? nt128 : 0;
+    std::memcpy(H + o_job, &jb, sizeof jb);
+    GemmTile* h64 = (GemmTile*)(H + o_t64);
+    GemmTile* h128 = (GemmTile*)(H + o_t128);
+    int k = 0;
+    for (int x = 0; x < t64; ++x)
+        for (int y = x; y < t64; ++y) h64[k++] = GemmTile{0, x, y};
+    k = 0;
+    for (int x = 0; x < t128; ++x)
+        for (int y = x; y < t128; ++y) h128[k++] = GemmTile{0, x, y};
+    MolState ms{};
+    ms.active = 1;
+    ms.lowp = precision != 0 ? 1 : 0;
+    std::memcpy(H + o_ms, &ms, sizeof ms);
+    double* hf = (double*)(H + o_f);
+    double* hmin = (double*)(H + o_rmin);
+    double* hmax = (double*)(H + o_rmax);
+    for (int r = 0; r < n; ++r) {  // the lower triangle, mirrored (Side::Lower), and its Gershgorin row bounds
+        double bound = 0.0;
+        for (int c = 0; c < n; ++c) {
+            const double v = r >= c ? F[(size_t)r * n + c] : F[(size_t)c * n + r];
+            hf[(size_t)r * n + c] = v;
+            if (c != r) bound += std::fabs(v);
+        }
+        hmin[r] = hf[(size_t)r * n + r] - bound;
+        hmax[r] = hf[(size_t)r * n + r] + bound;
+    }
+    CK(cudaMemcpyAsync(D, H, staged, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(D + o_work, 0, 8 * kWorkN, s));
+    CK(cudaMemsetAsync(D + o_need, 0, 16, s));
+    CK(cudaMemsetAsync(D + o_act, 0, 16, s));
+    CK(cudaMemsetAsync(D + o_stall, 0, 16, s));
+    const Sp2Job* dj = (const Sp2Job*)(D + o_job);
+    Sp2State* dsst = (Sp2State*)(D + o_sst);
+    const MolState* dms = (const MolState*)(D + o_ms);
+    const GemmTile* d64 = (const GemmTile*)(D + o_t64);
+    const GemmTile* d128 = (const GemmTile*)(D + o_t128);
+    int* dact = (int*)(D + o_act);
+    k_sp2_bounds<<<1, 512, 3 * sizeof(double) * n, s>>>(dj, dms);
+    k_sp2_init<<<dim3(nblk, 1), 256, 0, s>>>(dj, dsst, dms, nblk);
+    k_sp2_start<<<1, 128, 0, s>>>(dj, dsst, dms, 1, nblk);
+    CK(cudaGetLastError());
+    const bool pairs = n % 2 == 0;  // every slot here starts on 256 bytes
+    int* hact = (int*)(H + staged);
+    for (int step = 0; step < kSp2MaxSteps; ++step) {
+        if (precision == 0) {
+            if (pairs) k_sp2_step16<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+            else k_sp2_step8<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+        } else if (precision == 2) {
+            k_sp2_step_tf32<<<nt64, 128, tf32_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+        } else {
+            k_sp2_step_tc<<<nt128, 128, tc_smem_bytes(), s>>>(dj, d128, nt128, dsst, dact + 2);
+        }
+        CK(cudaMemsetAsync(dact, 0, sizeof(int), s));
+        k_sp2_update<<<1, 128, 0, s>>>(dj, dsst, 1, kSp2MaxSteps, dact, (double*)(D + o_work));
+        CK(cudaGetLastError());
+        if (step >= 12 && (step % 6) == 5) {
+            CK(cudaMemcpyAsync(hact, dact, 16, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (hact[0] == 0) break;
+        }
+    }
+    k_sp2_finish<<<dim3(std::max(8u, std::min(256u, cdiv(nn, 65536))), 1), 256, 0, s>>>(dj, dsst, dms, (int*)(D + o_need),
+                                                                                       (double*)(D + o_work), (int*)(D + o_stall),
+                                                                                       dact + 3);
+    CK(cudaGetLastError());
+    Sp2State* hs = (Sp2State*)(H + staged + 256);
+    CK(cudaMemcpyAsync(hs, dsst, sizeof(Sp2State), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hact, dact, 16, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(P, D + o_p, 8 * nn, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (steps_out) *steps_out = hs->steps;
+    if (hact[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
+    if (!hs->converged) return fail(AM1GPU_LINALG, "the purification did not reach idempotency (gap too small)");
     return AM1GPU_OK;
 }
 
@@ -2617,6 +2869,28 @@ int am1gpu_symmetric_eigen_batch(int32_t count, const int32_t* n, const double* 
 
 int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w) { return am1::symmetric_eigenvalues_one(n, a, w); }
 
+int am1gpu_lowp_tuning(int32_t* choice, float* ms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return am1::fail(AM1GPU_DEVICE_ERROR, "no CUDA device");
+    am1::LowpTune& t = am1::g_lowp_tune[dev];
+    std::lock_guard<std::mutex> lock(t.mu);
+    for (int c = 0; c < am1::kTuneClasses; ++c) {
+        if (choice) choice[c] = t.choice[c];
+        if (ms) {
+            ms[2 * c] = t.ms[c][0];
+            ms[2 * c + 1] = t.ms[c][1];
+        }
+    }
+    return AM1GPU_OK;
+}
+
+int am1gpu_density_purify(int32_t n, const double* f, double n_occ, double weight, int32_t precision, double* p, int32_t* steps) {
+    int st = 0;
+    const int rc = am1::density_purify_one(n, f, n_occ, weight, precision, p, &st);
+    if (steps) *steps = st;
+    return rc;
+}
+
 int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v) {
     return am1::symmetric_eigen_one(n, a, w, v);
 }
@@ -2648,7 +2922,8 @@ int am1gpu_batch_create(int32_t nmol, const am1gpu_molecule* mols, const am1gpu_
         }
     }
     if (!plans.empty()) {
-        rc = build_batch(mols, *opts, std::move(plans), h->b, h->mem, &h->stats);
+        if (opts->precision == AM1GPU_PRECISION_MIXED) rc = tune_lowp_kernels(plans);
+        if (!rc) rc = build_batch(mols, *opts, std::move(plans), h->b, h->mem, &h->stats);
         h->b.graph_cacheable = true;
         if (!rc && cudaStreamSynchronize(h->mem.stream) != cudaSuccess) rc = fail(AM1GPU_DEVICE_ERROR, "upload failed");
         if (rc) {

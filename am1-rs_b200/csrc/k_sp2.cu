@@ -387,7 +387,8 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
         if (lowp) {  // FP32 iterate (rows of ldf floats, pad columns zero in both buffers)
             float* Xr = jb.Xf0 + (long long)r * jb.ldf;
             for (int c = lane; c < jb.ldf; c += 32) {
-                const float x = c < n ? tf32_round((float)(((c == r ? emax : 0.0) - Fr[c]) * inv)) : 0.0f;
+                const float xf = c < n ? (float)(((c == r ? emax : 0.0) - Fr[c]) * inv) : 0.0f;
+                const float x = jb.lowp_tc ? xf : tf32_round(xf);
                 Xr[c] = x;
                 if (c >= n) jb.Xf1[(long long)r * jb.ldf + c] = 0.0f;
                 fr += (double)x * x;
@@ -533,7 +534,8 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
         atomicAdd(&work[3], 16.0 * jb.n * jb.n);  // read X, write X^2 (both triangles), FP64
     }
     double tr = 0.0, fr = 0.0;
-    for (int t = 0; t < jb.ntiles; ++t) {
+    const int nparts = (s.lowp && jb.lowp_tc) ? jb.tc_ntiles : jb.ntiles;  // 128-tiles of the tcgen05 step
+    for (int t = 0; t < nparts; ++t) {
         tr += jb.part[2 * t];
         fr += jb.part[2 * t + 1];
     }

@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(TF_THREADS, 4) k_sp2_step_tf32(const Sp2Job* _
     if (t >= ntiles) return;
     const GemmTile tl = tiles[t];
     const Sp2State* sp = sst + tl.job;
-    if (!sp->active || !sp->lowp) return;  // FP64 runs: k_sp2_step16 / k_sp2_step8
     const Sp2Job* jp = jobs + tl.job;
+    if (!sp->active || !sp->lowp || jp->lowp_tc) return;  // FP64 runs: k_sp2_step16 / k_sp2_step8; tcgen05: k_sp2_step_tc
     const int n = jp->n, ldf = jp->ldf;
     const int cur = sp->cur;
     const float* X = cur ? jp->Xf1 : jp->Xf0;

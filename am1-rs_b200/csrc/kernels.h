@@ -80,6 +80,10 @@ struct Sp2Job {
     float* Xf0;
     float* Xf1;
     int ldf;
+    // 1: the reduced-precision products run on tcgen05 at FP32 accuracy (k_sp2_step_tc, 128 x 128
+    // tiles tc_tile0 .. tc_tile0 + tc_ntiles - 1 of their launch, FP32 iterates); 0: mma.sync TF32
+    // (k_sp2_step_tf32, TF32-rounded iterates)
+    int lowp_tc, tc_tile0, tc_ntiles;
 };
 
 struct Sp2State {
@@ -166,6 +170,8 @@ __global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int n
 __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
+size_t tc_smem_bytes();
+__global__ void k_sp2_step_tc(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
                              int* big_stall, int* big_count);
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each

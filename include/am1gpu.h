@@ -250,6 +250,29 @@ int am1gpu_symmetric_eigen(int32_t n, const double* a, double* w, double* v);
 int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
 
 /*
+ * Density of one symmetric matrix f (n <= 448 rows, its lower triangle read):
+ * p = weight * (projector onto its n_occ lowest eigenvectors), by trace-correcting purification
+ * -- the step an SCF iteration takes after the extrapolation, symmetric_eigen + density_from_coeff
+ * (src/scf.rs:654-661, 503-524), alone.  precision: 0 FP64 tensor cores (the products of the FP64
+ * SCF), 1 FP32-accurate products on the fifth-generation tensor cores (tcgen05, TF32 operands split
+ * in two, as the mixed path's early iterations use), 2 TF32 products on mma.sync.  The reduced-
+ * precision runs stop at their own rounding floor and are rescaled to trace n_occ.  *steps (may be
+ * NULL) receives the number of products.  A matrix whose gap is too small to purify in 100 steps
+ * returns AM1GPU_LINALG.
+ */
+int am1gpu_density_purify(int32_t n, const double* f, double n_occ, double weight, int32_t precision, double* p,
+                          int32_t* steps);
+
+/*
+ * The autotuner's table for the current device: which kernel the mixed path's reduced-precision
+ * purification products use per size class (n <= 128, <= 256, <= 384, larger): choice[c] = 1
+ * tcgen05 (FP32-accurate), 0 mma.sync TF32, -1 not tuned yet; ms[2c], ms[2c+1] the time of one
+ * purification of the class's test matrix with each (mma.sync, tcgen05).  Either pointer may be
+ * NULL.  No counterpart in the reference.
+ */
+int am1gpu_lowp_tuning(int32_t* choice, float* ms);
+
+/*
  * count independent symmetric eigendecompositions in one call (each as am1gpu_symmetric_eigen:
  * those of n[i] <= 448 in one set of launches, larger ones after them, one at a time): replaces the per-subsystem symmetric_eigen calls of the divide-and-conquer SCF
  * (solve_subsystems, src/divide_conquer.rs:587-617).  a[i], w[i], v[i] as above for matrix i;
