@@ -6,8 +6,9 @@
 //     lane-parallel, a partner per lane, 32 at a time, in registers, and reduced over the warp once
 //     per atom;
 //   * the exchange blocks K_AB = -s sum P^s_ab (mu nu | lambda sigma) (src/fock.rs:449-466) of a
-//     heavy A with heavy B > A: one pair at a time, the 100-integral block staged through shared
-//     memory with coalesced loads, lanes 0..15 on the 16 outputs, written to F_AB and F_BA;
+//     heavy A with heavy B > A: two pairs at a time, their adjacent 100-integral blocks staged
+//     through shared memory with coalesced loads, a half-warp per pair and a lane per output,
+//     written to F_AB and F_BA;
 //   * the exchange of every other pair (a hydrogen on either side: blocks of 10 or 1 integrals)
 //     lane-parallel, the lane of the partner writing F_AB and F_BA when A is the pair's first atom.
 // The one-centre terms (oc_two_electron, src/fock.rs:27-65 and 321-344) finish the diagonal.
@@ -45,9 +46,9 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __re
                                                          int natoms_total, const DevElem* __restrict__ params,
                                                          const int* __restrict__ atom_z, const double* __restrict__ wstore,
                                                          double* __restrict__ arena, const MolState* __restrict__ st, int force) {
-    __shared__ double s_w[FOCK_WARPS][100];
+    __shared__ double s_w[FOCK_WARPS][200];
     __shared__ double s_q[FOCK_WARPS][10];
-    __shared__ double s_pab[FOCK_WARPS][2][16];
+    __shared__ double s_pab[FOCK_WARPS][2][2][16];
     __shared__ double s_j[FOCK_WARPS][10];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int a = blockIdx.x * FOCK_WARPS + warp;
@@ -108,29 +109,36 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __re
                 }
             }
         }
-        // exchange blocks with the heavier-indexed heavy partners (A is the pair's first atom)
-        for (int B = A + 1; B < h; ++B) {
+        // exchange blocks with the heavier-indexed heavy partners (A is the pair's first atom), two
+        // partners at a time: lanes 0..15 take B0, lanes 16..31 take B0 + 1, a lane per output
+        // element of the 4 x 4 block (the same sum, in the same order, as one partner at a time)
+        const int half = lane >> 4, l16 = lane & 15;
+        for (int B0 = A + 1; B0 < h; B0 += 2) {
+            const int nb = min(2, h - B0);  // partners in this round
+            const double* blk0 = w + 100LL * ((long long)A * h - (long long)A * (A + 1) / 2 + (B0 - A - 1));
+            for (int l = lane; l < 100 * nb; l += 32) wb[l] = blk0[l];  // the blocks of (A, B0), (A, B0 + 1) are adjacent
+            const int B = B0 + half;
+            const bool mine = half < nb;
             const int oB = 4 * B;
-            const double* blk = w + 100LL * ((long long)A * h - (long long)A * (A + 1) / 2 + (B - A - 1));
-            for (int l = lane; l < 100; l += 32) wb[l] = blk[l];
-            if (lane < 16) {
-                const long long idx = (long long)(oA + (lane >> 2)) * n + oB + (lane & 3);
-                s_pab[warp][0][lane] = P0[idx];
-                if (P1) s_pab[warp][1][lane] = P1[idx];
+            if (mine) {
+                const long long idx = (long long)(oA + (l16 >> 2)) * n + oB + (l16 & 3);
+                s_pab[warp][half][0][l16] = P0[idx];
+                if (P1) s_pab[warp][half][1][l16] = P1[idx];
             }
             __syncwarp();
-            if (lane < 16) {
-                const int mu = lane >> 2, la = lane & 3;
+            if (mine) {
+                const int mu = l16 >> 2, la = l16 & 3;
                 const long long ab = (long long)(oA + mu) * n + oB + la;
                 const long long ba = (long long)(oB + la) * n + oA + mu;
                 const double hab = H0[ab];
+                const double* wbh = wb + 100 * half;
                 for (int c = 0; c < md.nch; ++c) {
                     double acc = 0.0;
 #pragma unroll
                     for (int nu = 0; nu < 4; ++nu) {
-                        const double* row = wb + pack2(mu, nu) * 10;
+                        const double* row = wbh + pack2(mu, nu) * 10;
 #pragma unroll
-                        for (int sg = 0; sg < 4; ++sg) acc += s_pab[warp][c][nu * 4 + sg] * row[pack2(la, sg)];
+                        for (int sg = 0; sg < 4; ++sg) acc += s_pab[warp][half][c][nu * 4 + sg] * row[pack2(la, sg)];
                     }
                     const double v = hab - acc * sc;
                     double* F = c == 0 ? F0 : F1;
