@@ -362,7 +362,7 @@ def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
     return g
 
 
-PURIFY_PRECISION = {"fp64": 0, "fp32_tcgen05": 1, "tf32": 2}
+PURIFY_PRECISION = {"fp64": 0, "fp32_tcgen05": 1, "tf32": 2, "fp64_digits": 3}
 
 
 def density_purify(f, n_occ, weight=2.0, precision="fp64"):

@@ -227,6 +227,8 @@ int device_ctx(DeviceCtx** out) {
             return bad("tf32 tile kernel smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_sp2_step_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes())) != cudaSuccess)
             return bad("tcgen05 tile kernel smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_sp2_step_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oz_smem_bytes())) != cudaSuccess)
+            return bad("digit-plane tile kernel smem attribute", err);
         for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8, (const void*)k_dgemm16,
                               (const void*)k_dgemm8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
@@ -382,6 +384,26 @@ struct LowpTune {
     float ms[kTuneClasses][2] = {};                // time of one purification (mma.sync, tcgen05)
 };
 LowpTune g_lowp_tune[64];
+
+// Which molecules' FP64 purification products run on tcgen05's integer path from digit planes
+// (k_sp2_step_oz) rather than on the FP64 tensor cores (k_sp2_step16/8): AM1GPU_FP64_DIGITS=1 all,
+// 0 none (the default).
+bool fp64_oz_for(int n) {
+    static const int v = [] {
+        const char* e = std::getenv("AM1GPU_FP64_DIGITS");
+        return e ? std::atoi(e) : 0;
+    }();
+    (void)n;
+    return v != 0;
+}
+inline int oz_ldq(int n) { return (n + 15) & ~15; }
+inline int oz_tiles_of(int n) {  // 128 x 48 tiles with an element on or above the diagonal
+    int k = 0;
+    for (int tm = 0; tm < (n + 127) / 128; ++tm)
+        for (int tn = 0; tn < (n + 47) / 48; ++tn)
+            if (48 * tn + 47 >= 128 * tm) ++k;
+    return k;
+}
 
 int lowp_tc_env() {
     static const int v = [] {
@@ -623,6 +645,8 @@ struct Batch {
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
     GemmTile* d_tc_tiles = nullptr;  // 128 x 128 upper-triangle tiles of the tcgen05 reduced-precision step
     int nt_tc = 0;
+    GemmTile* d_oz_tiles = nullptr;  // 128 x 48 tiles of the digit-plane FP64 step
+    int nt_oz = 0;
     Sp2State* d_sp2_state;
     TriJob* d_tri;
     int* d_need_eigen;
@@ -684,7 +708,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.nblk = std::max(1, std::min(32, (maxn + 15) / 16));
     const int nblk = b.nblk;
     // GEMM tile counts
-    int tiles_nn = 0, tiles_up = 0, tiles_tc = 0;
+    int tiles_nn = 0, tiles_up = 0, tiles_tc = 0, tiles_oz = 0;
+    long long dq_bytes = 0;
     const bool mixed = o.precision == AM1GPU_PRECISION_MIXED;
     for (auto& p : b.plans) {
         const int tn = (p.nao + 63) / 64;
@@ -692,6 +717,10 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         tiles_up += p.nch * tn * (tn + 1) / 2;
         const int tc = (p.nao + 127) / 128;
         if (mixed && lowp_tc_for(p.nao)) tiles_tc += p.nch * tc * (tc + 1) / 2;
+        if (fp64_oz_for(p.nao)) {
+            tiles_oz += p.nch * oz_tiles_of(p.nao);
+            dq_bytes += p.nch * (2LL * kOzPlanes * p.nao * oz_ldq(p.nao) + 256);
+        }
     }
     const int sp2_nblk = std::max(1, std::min(32, (maxn + 7) / 8));
     // ---- staged (host -> device) region layout
@@ -717,6 +746,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
     const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
     const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
+    const size_t o_ozt = take(st, sizeof(GemmTile) * std::max(tiles_oz, 1));
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
     const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
@@ -752,6 +782,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_grad = take(dv, sizeof(double) * 3 * std::max<long long>(natoms, 1));
     const size_t o_bstall = take(dv, sizeof(int) * std::max<long long>(nch_total, 1));
     const size_t o_loop = take(dv, sizeof(GraphLoop));
+    const size_t o_dq = take(dv, (size_t)std::max<long long>(dq_bytes, 16));
     const size_t dtotal = align256(dv);
     // pinned staging also receives the outputs
     size_t hs = staged;
@@ -785,6 +816,10 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_tc_tiles = (GemmTile*)dptr(o_tct);
     GemmTile* htct = (GemmTile*)(Hs + o_tct);
     int ntc = 0;
+    b.d_oz_tiles = (GemmTile*)dptr(o_ozt);
+    GemmTile* hozt = (GemmTile*)(Hs + o_ozt);
+    int noz = 0;
+    long long dq_off = 0;
     b.d_tri = (TriJob*)dptr(o_tri);
     b.d_sp2_big = (int*)dptr(o_sp2big);
     b.d_need_eigen = (int*)dptr(o_need);
@@ -960,6 +995,20 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
                     for (int y = x; y < tc; ++y) htct[ntc++] = GemmTile{job, x, y};
             }
             sj.tc_ntiles = ntc - sj.tc_tile0;
+            sj.oz = fp64_oz_for((int)n) ? 1 : 0;
+            sj.oz_tile0 = noz;
+            sj.ldq = oz_ldq((int)n);
+            sj.Dq0 = sj.Dq1 = nullptr;
+            if (sj.oz) {
+                for (int tm = 0; tm < (int)((n + 127) / 128); ++tm)
+                    for (int tn = 0; tn < (int)((n + 47) / 48); ++tn)
+                        if (48 * tn + 47 >= 128 * tm) hozt[noz++] = GemmTile{job, tm, tn};
+                const long long pl = (long long)kOzPlanes * n * sj.ldq;
+                sj.Dq0 = (int8_t*)dptr(o_dq) + dq_off;
+                sj.Dq1 = sj.Dq0 + pl;
+                dq_off += 2 * pl + 256;
+            }
+            sj.oz_ntiles = noz - sj.oz_tile0;
             if (!sj.fallback) b.sp2_big.push_back(job);
             sj.tile0 = (int)tl.size();  // tile index inside its own launch
             for (int x = 0; x < (int)tn_; ++x)
@@ -1019,6 +1068,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     for (size_t i = 0; i < tiles_other.size(); ++i) hsp2t[tiles_pairs.size() + i] = tiles_other[i];
     b.nt_sp2_pairs = (int)tiles_pairs.size();
     b.nt_tc = ntc;
+    b.nt_oz = noz;
     b.nt_sp2 = (int)(tiles_pairs.size() + tiles_other.size());
     // eigen jobs grouped by cluster size, largest first inside a group
     std::vector<int> idx(eig_all.size());
@@ -1343,6 +1393,10 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
         else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
         ++nl;
     });
+    if (b.nt_oz > 0) {
+        k_sp2_step_oz<<<b.nt_oz, 128, oz_smem_bytes(), s>>>(b.d_sp2, b.d_oz_tiles, b.nt_oz, b.d_sp2_state, b.d_sp2_active + 2);
+        ++nl;
+    }
     if (lowp_left) {
         launch_tiles(b, s, [&](const GemmTile* t, int nt, bool) {
             k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
@@ -1631,6 +1685,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     CK(cudaMemcpyAsync(b.h_work, b.d_work, sizeof(double) * kWorkN, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(b.h_active + 2, b.d_sp2_active + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (b.h_active[2] & (1 << 10)) return fail(AM1GPU_LINALG, "a purification iterate left the range of its digit planes (|x| >= 2)");
     if (b.h_active[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
     stats->purification_steps += b.h_work[0];
     stats->purification_flops += b.h_work[1];
@@ -2294,7 +2349,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
                        Mem* mem_override = nullptr) {
     g_err.clear();
     if (n < 1 || n > 448 || !F || !P) return fail(AM1GPU_INVALID_INPUT, "n must be 1..448 and the pointers non-null");
-    if (precision < 0 || precision > 2) return fail(AM1GPU_INVALID_INPUT, "precision must be 0, 1 or 2");
+    if (precision < 0 || precision > 3) return fail(AM1GPU_INVALID_INPUT, "precision must be 0, 1, 2 or 3");
     if (!(nocc >= 0.0 && nocc <= n)) return fail(AM1GPU_INVALID_INPUT, "nocc outside 0..n");
     for (long long i = 0; i < (long long)n * n; ++i)
         if (!std::isfinite(F[i])) return fail(AM1GPU_LINALG, "the matrix is not finite");
@@ -2304,7 +2359,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     const long long nn = (long long)n * n;
     const int ldf = (n + 3) & ~3;
     const int t64 = (n + 63) / 64, t128 = (n + 127) / 128;
-    const int nt64 = t64 * (t64 + 1) / 2, nt128 = t128 * (t128 + 1) / 2;
+    const int nt64 = t64 * (t64 + 1) / 2, nt128 = t128 * (t128 + 1) / 2, ntoz = oz_tiles_of(n);
+    const int ldq = oz_ldq(n);
     const int nblk = sp2_init_blocks(n);
     size_t off = 0;
     auto take = [&off](size_t bytes) {
@@ -2314,11 +2370,13 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         return o;
     };
     const size_t o_job = take(sizeof(Sp2Job)), o_t64 = take(sizeof(GemmTile) * nt64), o_t128 = take(sizeof(GemmTile) * nt128),
+                 o_toz = take(sizeof(GemmTile) * ntoz),
                  o_ms = take(sizeof(MolState)), o_f = take(8 * nn), o_rmin = take(8 * (size_t)n), o_rmax = take(8 * (size_t)n);
     const size_t staged = align256(off);
     const size_t o_sst = take(sizeof(Sp2State)), o_bnd = take(16), o_x0 = take(8 * nn), o_x1 = take(8 * nn), o_p = take(8 * nn),
                  o_part = take(16 * (size_t)std::max(32, nt64)), o_xf = take(8 * (size_t)n * ldf + 64), o_need = take(16),
-                 o_work = take(8 * kWorkN), o_act = take(16), o_stall = take(16);
+                 o_work = take(8 * kWorkN), o_act = take(16), o_stall = take(16),
+                 o_dq = take(2 * (size_t)kOzPlanes * n * ldq);
     Workspace* ws;
     if (mem_override) {
         if ((rc = mem_ensure(*mem_override, align256(off), staged + align256(sizeof(Sp2State)) + 256))) return rc;
@@ -2351,7 +2409,18 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     jb.lowp_tc = precision == 1 ? 1 : 0;
     jb.tc_tile0 = 0;
     jb.tc_ntiles = precision == 1 ? nt128 : 0;
+    jb.oz = precision == 3 ? 1 : 0;
+    jb.oz_tile0 = 0;
+    jb.oz_ntiles = precision == 3 ? ntoz : 0;
+    jb.ldq = ldq;
+    jb.Dq0 = (int8_t*)(D + o_dq);
+    jb.Dq1 = jb.Dq0 + (size_t)kOzPlanes * n * ldq;
     std::memcpy(H + o_job, &jb, sizeof jb);
+    GemmTile* hoz = (GemmTile*)(H + o_toz);
+    int koz = 0;
+    for (int tm = 0; tm < t128; ++tm)
+        for (int tn = 0; tn < (n + 47) / 48; ++tn)
+            if (48 * tn + 47 >= 128 * tm) hoz[koz++] = GemmTile{0, tm, tn};
     GemmTile* h64 = (GemmTile*)(H + o_t64);
     GemmTile* h128 = (GemmTile*)(H + o_t128);
     int k = 0;
@@ -2362,7 +2431,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         for (int y = x; y < t128; ++y) h128[k++] = GemmTile{0, x, y};
     MolState ms{};
     ms.active = 1;
-    ms.lowp = precision != 0 ? 1 : 0;
+    ms.lowp = (precision == 1 || precision == 2) ? 1 : 0;
     std::memcpy(H + o_ms, &ms, sizeof ms);
     double* hf = (double*)(H + o_f);
     double* hmin = (double*)(H + o_rmin);
@@ -2398,6 +2467,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         if (precision == 0) {
             if (pairs) k_sp2_step16<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
             else k_sp2_step8<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+        } else if (precision == 3) {
+            k_sp2_step_oz<<<ntoz, 128, oz_smem_bytes(), s>>>(dj, (const GemmTile*)(D + o_toz), ntoz, dsst, dact + 2);
         } else if (precision == 2) {
             k_sp2_step_tf32<<<nt64, 128, tf32_smem_bytes(), s>>>(dj, d64, nt64, dsst);
         } else {
@@ -2422,6 +2493,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     CK(cudaMemcpyAsync(P, D + o_p, 8 * nn, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (steps_out) *steps_out = hs->steps;
+    if (hact[2] & (1 << 10)) return fail(AM1GPU_LINALG, "a purification iterate left the range of its digit planes (|x| >= 2)");
     if (hact[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
     if (!hs->converged) return fail(AM1GPU_LINALG, "the purification did not reach idempotency (gap too small)");
     return AM1GPU_OK;

@@ -403,6 +403,17 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
             fr += x * x;
             if (c == r) tr += x;
         }
+        if (jb.oz) {  // the digit planes of X0, and zero pad columns in both digit buffers
+            const long long plane = (long long)n * jb.ldq;
+            for (int c = lane; c < jb.ldq; c += 32) {
+                const long long o = (long long)r * jb.ldq + c;
+                if (c < n) {
+                    oz_digits_of(Xr[c], jb.Dq0, plane, o);
+                } else {
+                    for (int i = 0; i < kOzPlanes; ++i) jb.Dq0[i * plane + o] = jb.Dq1[i * plane + o] = 0;
+                }
+            }
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         tr += __shfl_xor_sync(0xffffffffu, tr, o);
@@ -462,8 +473,8 @@ __device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, c
     if (t >= ntiles) return;
     const GemmTile tl = tiles[t];
     const Sp2State* sp = sst + tl.job;
-    if (!sp->active || sp->lowp) return;  // TF32 runs: k_sp2_step_tf32
     const Sp2Job* jp = jobs + tl.job;
+    if (!sp->active || sp->lowp || jp->oz) return;  // TF32 runs: k_sp2_step_tf32 / _tc; digit products: k_sp2_step_oz
     const int n = jp->n;
     const int cur = sp->cur;
     const double* X = cur ? jp->X1 : jp->X0;
@@ -534,7 +545,8 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
         atomicAdd(&work[3], 16.0 * jb.n * jb.n);  // read X, write X^2 (both triangles), FP64
     }
     double tr = 0.0, fr = 0.0;
-    const int nparts = (s.lowp && jb.lowp_tc) ? jb.tc_ntiles : jb.ntiles;  // 128-tiles of the tcgen05 step
+    // the partial sums come from the tiles of the kernel that took the product
+    const int nparts = s.lowp ? (jb.lowp_tc ? jb.tc_ntiles : jb.ntiles) : (jb.oz ? jb.oz_ntiles : jb.ntiles);
     for (int t = 0; t < nparts; ++t) {
         tr += jb.part[2 * t];
         fr += jb.part[2 * t + 1];

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 
 #include "am1gpu_internal.h"
 
@@ -84,7 +85,15 @@ struct Sp2Job {
     // tiles tc_tile0 .. tc_tile0 + tc_ntiles - 1 of their launch, FP32 iterates); 0: mma.sync TF32
     // (k_sp2_step_tf32, TF32-rounded iterates)
     int lowp_tc, tc_tile0, tc_ntiles;
+    // 1: the FP64 products run on tcgen05's integer path from the iterate's 7-bit digit planes
+    // (k_sp2_step_oz, 128 x 48 tiles oz_tile0 .. oz_tile0 + oz_ntiles - 1 of their launch); the digits of
+    // X0 / X1 are kOzPlanes int8 planes of n rows of ldq bytes each (pad columns zero)
+    int oz, oz_tile0, oz_ntiles, ldq;
+    int8_t* Dq0;
+    int8_t* Dq1;
 };
+constexpr int kOzPlanes = 8;  // 7-bit digits of an iterate: 2^-5 .. 2^-54
+constexpr int kOzGroups = 9;  // digit-plane products kept: i + j <= 8
 
 struct Sp2State {
     int active, steps, cur, square, converged;
@@ -171,6 +180,18 @@ __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int nt
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 size_t tc_smem_bytes();
+size_t oz_smem_bytes();
+__global__ void k_sp2_step_oz(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
+__device__ __forceinline__ void oz_digits_of(double y, int8_t* __restrict__ D, long long plane, long long o) {
+    double r = y;
+#pragma unroll
+    for (int i = 0; i < kOzPlanes; ++i) {
+        const double sc = ldexp(1.0, 5 + 7 * i);
+        const double d = rint(r * sc);
+        r -= d / sc;
+        D[i * plane + o] = (int8_t)d;
+    }
+}
 __global__ void k_sp2_step_tc(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
                              int* big_stall, int* big_count);

@@ -255,7 +255,8 @@ int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
  * -- the step an SCF iteration takes after the extrapolation, symmetric_eigen + density_from_coeff
  * (src/scf.rs:654-661, 503-524), alone.  precision: 0 FP64 tensor cores (the products of the FP64
  * SCF), 1 FP32-accurate products on the fifth-generation tensor cores (tcgen05, TF32 operands split
- * in two, as the mixed path's early iterations use), 2 TF32 products on mma.sync.  The reduced-
+ * in two, as the mixed path's early iterations use), 2 TF32 products on mma.sync, 3 FP64 products on
+ * tcgen05's integer path from 7-bit digit planes of the iterate (AM1GPU_FP64_DIGITS).  The reduced-
  * precision runs stop at their own rounding floor and are rescaled to trace n_occ.  *steps (may be
  * NULL) receives the number of products.  A matrix whose gap is too small to purify in 100 steps
  * returns AM1GPU_LINALG.
