@@ -169,18 +169,22 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_sp2_step_oz(const Sp2Job* __r
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (tid == 0) {
             const uint32_t a0 = sbase + st * OZ_STAGE, b0 = a0 + kOzPlanes * OZ_A_PLANE;
-#pragma unroll 1
+            // a plane or k offset moves only the start-address field (address >> 4, 14 bits; shared-memory
+            // addresses stay below 2^18, so the sum never carries out of the field)
+            const uint64_t da0 = oz_desc(a0), db0 = oz_desc(b0);
+#pragma unroll
             for (int g = 0; g < kOzGroups; ++g) {
                 const uint32_t acc_col = tmem + (uint32_t)(g * OZ_N);
-                const int ilo = g - (kOzPlanes - 1) > 0 ? g - (kOzPlanes - 1) : 0;
-                const int ihi = g < kOzPlanes - 1 ? g : kOzPlanes - 1;
-                for (int i = ilo; i <= ihi; ++i) {
+#pragma unroll
+                for (int i = 0; i < kOzPlanes; ++i) {
                     const int j = g - i;
+                    if (j < 0 || j >= kOzPlanes) continue;
+                    const int ilo = g - (kOzPlanes - 1) > 0 ? g - (kOzPlanes - 1) : 0;
 #pragma unroll
                     for (int kk = 0; kk < OZ_BK / 32; ++kk) {  // K = 32 per MMA: 32 bytes along the swizzled row
-                        const uint32_t o = 32u * kk;
-                        oz_mma(acc_col, oz_desc(a0 + i * OZ_A_PLANE + o), oz_desc(b0 + j * OZ_B_PLANE + o),
-                               (kt > 0 || i > ilo || kk > 0) ? 1u : 0u);
+                        const uint64_t da = da0 + (uint64_t)((i * OZ_A_PLANE + 32 * kk) >> 4);
+                        const uint64_t db = db0 + (uint64_t)((j * OZ_B_PLANE + 32 * kk) >> 4);
+                        oz_mma(acc_col, da, db, (kt > 0 || i > ilo || kk > 0) ? 1u : 0u);
                     }
                 }
             }
@@ -243,6 +247,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_sp2_step_oz(const Sp2Job* __r
         return;
     }
     // Y = X^2 or 2X - X^2 for the tile's elements with row <= column, mirrored, in FP64, and its digits
+    // (computed once per element: the mirrored pass reads them back from shared memory)
+    unsigned long long* dig = reinterpret_cast<unsigned long long*>(base + OZ_M * OZ_OUT_LD * sizeof(double));
     const int square = sp->square;
     double tr = 0.0, fr = 0.0;
     int bad = 0;
@@ -253,8 +259,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_sp2_step_oz(const Sp2Job* __r
         const double x2 = out[i * OZ_OUT_LD + j];
         const double y = square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
         if (!(fabs(y) < 2.0)) bad = 1;
+        const unsigned long long dp = oz_digits_packed(y);
+        out[i * OZ_OUT_LD + j] = y;
+        dig[i * OZ_N + j] = dp;
         Y[(long long)r * n + c] = y;
-        oz_digits_of(y, Dy, plane, (long long)r * ldq + c);
+        oz_store_digits(dp, Dy, plane, (long long)r * ldq + c);
         if (r == c) {
             tr += y;
             fr += y * y;
@@ -268,10 +277,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_sp2_step_oz(const Sp2Job* __r
         const int j = idx / OZ_M, i = idx % OZ_M;  // consecutive threads: consecutive tile rows = mirrored columns
         const int r = m0 + i, c = n0 + j;
         if (r >= n || c >= n || r >= c) continue;
-        const double x2 = out[i * OZ_OUT_LD + j];
-        const double y = square ? x2 : 2.0 * X[(long long)r * n + c] - x2;
-        Y[(long long)c * n + r] = y;
-        oz_digits_of(y, Dy, plane, (long long)c * ldq + r);
+        Y[(long long)c * n + r] = out[i * OZ_OUT_LD + j];
+        oz_store_digits(dig[i * OZ_N + j], Dy, plane, (long long)c * ldq + r);
     }
     if (bad) atomicOr(err, 1 << 10);
     for (int o = 16; o > 0; o >>= 1) {

@@ -182,15 +182,27 @@ __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int m
 size_t tc_smem_bytes();
 size_t oz_smem_bytes();
 __global__ void k_sp2_step_oz(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
-__device__ __forceinline__ void oz_digits_of(double y, int8_t* __restrict__ D, long long plane, long long o) {
+// The eight 7-bit digits of y (|y| < 2) packed one per byte, digit i in byte i: d_i = rint(r_i 2^(5+7i)),
+// r_{i+1} = r_i - d_i 2^-(5+7i), every step exact (powers of two, no division).
+__device__ __forceinline__ unsigned long long oz_digits_packed(double y) {
     double r = y;
+    unsigned long long packed = 0;
 #pragma unroll
     for (int i = 0; i < kOzPlanes; ++i) {
-        const double sc = ldexp(1.0, 5 + 7 * i);
+        const double sc = __longlong_as_double((long long)(1023 + 5 + 7 * i) << 52);    // 2^(5+7i)
+        const double isc = __longlong_as_double((long long)(1023 - 5 - 7 * i) << 52);   // 2^-(5+7i)
         const double d = rint(r * sc);
-        r -= d / sc;
-        D[i * plane + o] = (int8_t)d;
+        r = fma(-d, isc, r);
+        packed |= (unsigned long long)(unsigned char)(signed char)(int)d << (8 * i);
     }
+    return packed;
+}
+__device__ __forceinline__ void oz_store_digits(unsigned long long packed, int8_t* __restrict__ D, long long plane, long long o) {
+#pragma unroll
+    for (int i = 0; i < kOzPlanes; ++i) D[i * plane + o] = (int8_t)(packed >> (8 * i));
+}
+__device__ __forceinline__ void oz_digits_of(double y, int8_t* __restrict__ D, long long plane, long long o) {
+    oz_store_digits(oz_digits_packed(y), D, plane, o);
 }
 __global__ void k_sp2_step_tc(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
