@@ -13,6 +13,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 namespace am1 {
 
 constexpr int DG_TILE = 64;
@@ -244,6 +246,187 @@ __device__ __forceinline__ void dg_mainloop_diff(double* smem, const double* __r
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// TMA-fed main loop for products of symmetric matrices.  Both operands of a 64x64 output tile are
+// 64-row blocks read along k: A = Ma[m0:m0+64, :], and B[:, n0:n0+64] = Mb[n0:n0+64, :]^T (Mb
+// symmetric).  Each k-tile of an operand is one 2D box of 16 doubles (128 bytes) x 64 rows copied by
+// the tensor memory accelerator (cp.async.bulk.tensor) from a tensor map of the n x n row-major
+// matrix; rows and columns past n read as zero.  The map uses the 128-byte swizzle: 16-byte chunk c
+// of box row r lands at r * 128 + (c ^ (r % 8)) * 16.
+//
+// Thread 0 issues the copies.  Each stage has a "full" mbarrier (the copies' byte count) and an
+// "empty" one (one arrival per warp when it has read the stage).  After its own k-tile g, thread 0
+// refills the stage that k-tile g - 1 used with k-tile g - 1 + DT_STAGES, so a warp may run up to two
+// k-tiles ahead of the others: no CTA barrier inside the k-loop.  The MMAs, their fragments and
+// their order are those of dg_mainloop (acc bit-identical for symmetric operands).
+//
+// Every wait is bounded (DT_WAIT_LIMIT polls).  A wait that runs out stops the loop in every warp,
+// thread 0 waits (bounded) for the copies it issued, and the function returns false on all threads:
+// the caller writes nothing for the tile and reports the error.
+constexpr int DT_STAGES = 3;
+constexpr int DT_OP_BYTES = DG_TILE * DG_BK * 8;  // one operand box: 64 rows x 128 bytes
+constexpr int DT_STAGE_BYTES = 2 * DT_OP_BYTES;
+constexpr size_t DT_SMEM = DT_STAGES * DT_STAGE_BYTES + 1024;  // + room to align the stages to 1024 bytes
+constexpr long long DT_WAIT_LIMIT = 1LL << 22;
+
+struct DtBars {
+    unsigned long long full[DT_STAGES], empty[DT_STAGES];
+};
+
+__device__ __forceinline__ uint32_t dt_saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// the stages: the dynamic shared memory rounded up to 1024 bytes (the swizzle atom)
+__device__ __forceinline__ unsigned char* dt_stages(unsigned char* dyn) {
+    const uint32_t a = dt_saddr(dyn);
+    return dyn + (((a + 1023u) & ~1023u) - a);
+}
+
+// true once the phase with this parity has completed; false after DT_WAIT_LIMIT polls
+__device__ __forceinline__ bool dt_wait(uint32_t bar, uint32_t parity) {
+    for (long long it = 0; it < DT_WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\n"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            "selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// one 16 x 64 box (x = first k, y = first row) of the matrix behind `map` into shared memory at
+// `dst`, counted on mbarrier `bar`
+__device__ __forceinline__ void dt_copy(uint32_t dst, const void* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// acc = Ma1[m0:, :].Mb1[n0:, :]^T (map_a2 == nullptr), or that minus Ma2[m0:, :].Mb2[n0:, :]^T as
+// one pipeline over 2K k-tiles (the accumulator is negated between the two products, as in
+// dg_mainloop_diff).  same_ab: Ma1 == Mb1 and m0 == n0 (a diagonal tile of X.X): one box per k-tile.
+// K: the matrices' order.  Same fragment layout and `compute` rule as dg_mainloop.
+__device__ __forceinline__ bool dg_mainloop_tma(unsigned char* stages, DtBars& bars, const void* map_a1, const void* map_b1,
+                                                const void* map_a2, const void* map_b2, bool same_ab, int K, int m0, int n0,
+                                                double acc[2][4][4], bool compute) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+    const int KT = (K + DG_BK - 1) / DG_BK;  // k-tiles per product
+    const int NT = map_a2 ? 2 * KT : KT;
+    const uint32_t sbase = dt_saddr(stages);
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < DT_STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(dt_saddr(&bars.full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(dt_saddr(&bars.empty[s])), "r"(DG_THREADS / 32));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    int issued = 0, landed = 0;  // thread 0: k-tiles issued; warp 0: k-tiles seen landed
+    auto issue = [&](int kt) {
+        const int s = kt % DT_STAGES;
+        const uint32_t fb = dt_saddr(&bars.full[s]);
+        const uint32_t a = sbase + s * DT_STAGE_BYTES;
+        const bool second = kt >= KT;
+        const int x = (second ? kt - KT : kt) * DG_BK;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                     "r"(same_ab ? DT_OP_BYTES : DT_STAGE_BYTES)
+                     : "memory");
+        dt_copy(a, second ? map_a2 : map_a1, x, m0, fb);
+        if (!same_ab) dt_copy(a + DT_OP_BYTES, second ? map_b2 : map_b1, x, n0, fb);
+    };
+    if (tid == 0)
+        for (; issued < DT_STAGES && issued < NT; ++issued) issue(issued);
+    // lane-constant part of the swizzled fragment addresses: row g of each 8-row group, chunk
+    // (k / 2) ^ g with k = kk + tq (a0, a1, b0) or kk + tq + 4 (a2, a3, b1)
+    const int lo8 = (tq & 1) * 8;
+    const int ra = (wr + g) * 128 + lo8, rb = (wc + g) * 128 + lo8;
+    const int c0 = (tq >> 1) ^ g;
+    bool ok = true;
+    for (int kt = 0; kt < NT; ++kt) {
+        const int s = kt % DT_STAGES;
+        ok = __all_sync(0xffffffffu, dt_wait(dt_saddr(&bars.full[s]), (kt / DT_STAGES) & 1));
+        if (!ok) break;
+        if (warp == 0) landed = kt + 1;
+        const unsigned char* As = stages + s * DT_STAGE_BYTES;
+        const unsigned char* Bs = same_ab ? As : As + DT_OP_BYTES;
+        if (compute) {
+            if (kt == KT) {  // first product done: acc = -A1.B1, then accumulate A2.B2
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
+            }
+            const int kbase = (kt < KT ? kt : kt - KT) * DG_BK;
+#pragma unroll
+            for (int kk = 0; kk < DG_BK; kk += 8) {
+                if (kk > 0 && kbase + kk >= K) break;
+                const int x0 = (c0 ^ (kk >> 1)) << 4, x1 = (c0 ^ ((kk >> 1) | 2)) << 4;
+                double a[2][4], b[4][2];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const unsigned char* p = As + ra + i * 16 * 128;
+                    a[i][0] = *reinterpret_cast<const double*>(p + x0);
+                    a[i][1] = *reinterpret_cast<const double*>(p + 8 * 128 + x0);
+                    a[i][2] = *reinterpret_cast<const double*>(p + x1);
+                    a[i][3] = *reinterpret_cast<const double*>(p + 8 * 128 + x1);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const unsigned char* p = Bs + rb + j * 8 * 128;
+                    b[j][0] = *reinterpret_cast<const double*>(p + x0);
+                    b[j][1] = *reinterpret_cast<const double*>(p + x1);
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dg_mma(acc[i][j], a[i], b[j]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(dt_saddr(&bars.empty[s])) : "memory");
+        if (warp == 0) {
+            // the stage k-tile kt - 1 used takes k-tile kt - 1 + DT_STAGES
+            int pok = 1;
+            if (lane == 0 && kt >= 1 && issued < NT) {
+                const int kp = kt - 1;
+                if (dt_wait(dt_saddr(&bars.empty[kp % DT_STAGES]), (kp / DT_STAGES) & 1))
+                    issue(issued++);
+                else
+                    pok = 0;
+            }
+            ok = __shfl_sync(0xffffffffu, pok, 0) != 0;
+            if (!ok) break;
+        }
+    }
+    if (tid == 0 && !ok)
+        for (int k = landed; k < issued; ++k) dt_wait(dt_saddr(&bars.full[k % DT_STAGES]), (k / DT_STAGES) & 1);
+    if (!__syncthreads_and(ok)) return false;
+    if (map_a2 && compute) {  // acc = A2.B2 - A1.B1: flip to A1.B1 - A2.B2
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
+    }
+    return true;
 }
 
 }  // namespace am1

@@ -6,6 +6,8 @@
 // convergence test and retires in place (MolState::active), so a molecule's result does not
 // depend on what else is in the batch.  The host only reads one integer (molecules still
 // active) every few iterations.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -222,6 +224,9 @@ int device_ctx(DeviceCtx** out) {
                               (const void*)k_commutator8})
             if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_smem_bytes())) != cudaSuccess)
                 return bad("tile kernel smem attribute", err);
+        for (const void* f : {(const void*)k_sp2_step_tma, (const void*)k_commutator_tma})
+            if ((err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dgemm_tma_smem_bytes())) != cudaSuccess)
+                return bad("tensor-map tile kernel smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_sp2_step_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tf32_smem_bytes())) !=
             cudaSuccess)
             return bad("tf32 tile kernel smem attribute", err);
@@ -396,6 +401,39 @@ bool fp64_oz_for(int n) {
     (void)n;
     return v != 0;
 }
+// The FP64 purification products of even-order matrices copy their operands with the tensor memory
+// accelerator (k_sp2_step_tma) unless AM1GPU_SP2_TMA=0 (k_sp2_step16, cp.async) or the driver has no
+// tensor-map encoder.  cuTensorMapEncodeTiled is looked up once through the runtime, so the library
+// does not link the driver library itself.
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        const char* e = std::getenv("AM1GPU_SP2_TMA");
+        if (e && std::atoi(e) == 0) return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        return (PFN_cuTensorMapEncodeTiled_v12000)f;
+    }();
+    return fn;
+}
+static_assert(sizeof(CUtensorMap) == sizeof(TmaDesc), "TmaDesc mirrors CUtensorMap");
+
+// The tensor map k_sp2_step_tma reads an n x n row-major FP64 matrix through: boxes of 16 columns
+// (128 bytes) x 64 rows, 128-byte swizzle, zero fill past the edges.  Needs n even and a 16-byte
+// aligned base (row pitch a multiple of 16 bytes); false otherwise or when encoding fails.
+bool encode_square_map(TmaDesc* out, const double* base, int n) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+    if (!enc || n < 1 || n % 2 != 0 || !aligned16(base)) return false;
+    const cuuint64_t dim[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t pitch[1] = {(cuuint64_t)n * sizeof(double)};
+    const cuuint32_t box[2] = {16, 64}, es[2] = {1, 1};
+    return enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dim, pitch, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 inline int oz_ldq(int n) { return (n + 15) & ~15; }
 inline int oz_tiles_of(int n) {  // 128 x 48 tiles with an element on or above the diagonal
     int k = 0;
@@ -642,6 +680,8 @@ struct Batch {
     int* d_sp2_big;
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
+    TmaDesc* d_sp2_maps;    // tensor maps of every pair-copy job's X0, X1, F, P (4 per job)
+    bool sp2_tma = false;   // the pair-copy tiles run k_sp2_step_tma and k_commutator_tma (every map encoded)
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
     GemmTile* d_tc_tiles = nullptr;  // 128 x 128 upper-triangle tiles of the tcgen05 reduced-precision step
     int nt_tc = 0;
@@ -745,6 +785,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_eig = take(st, sizeof(EigJob) * nch_total);
     const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
     const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
+    const size_t o_maps = take(st, sizeof(TmaDesc) * 4 * std::max<long long>(nch_total, 1));
     const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
     const size_t o_ozt = take(st, sizeof(GemmTile) * std::max(tiles_oz, 1));
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
@@ -813,6 +854,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_eig = (EigJob*)dptr(o_eig);
     b.d_sp2 = (Sp2Job*)dptr(o_sp2);
     b.d_sp2_tiles = (GemmTile*)dptr(o_sp2t);
+    b.d_sp2_maps = (TmaDesc*)dptr(o_maps);
+    TmaDesc* hmaps = (TmaDesc*)(Hs + o_maps);
+    b.sp2_tma = tma_encoder() != nullptr;
     b.d_tc_tiles = (GemmTile*)dptr(o_tct);
     GemmTile* htct = (GemmTile*)(Hs + o_tct);
     int ntc = 0;
@@ -983,6 +1027,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             // F and P starts on 16 bytes: even n (slot bases are then 16-byte aligned too)
             const bool pairs = n % 2 == 0 && aligned16(sj.X0) && aligned16(sj.X1) && aligned16(cj.F) && aligned16(cj.P);
             std::vector<GemmTile>& tl = pairs ? tiles_pairs : tiles_other;
+            if (pairs && b.sp2_tma)
+                b.sp2_tma = encode_square_map(&hmaps[4 * job], sj.X0, (int)n) && encode_square_map(&hmaps[4 * job + 1], sj.X1, (int)n) &&
+                            encode_square_map(&hmaps[4 * job + 2], cj.F, (int)n) && encode_square_map(&hmaps[4 * job + 3], cj.P, (int)n);
             sj.fallback = p.cluster > 0;
             sj.ldf = (int)((n + 3) & ~3LL);  // FP32 iterates of the mixed path: in the VS slot, 16-byte aligned
             sj.Xf0 = (float*)(((uintptr_t)(base + SLOT_VS * nn) + 15) & ~(uintptr_t)15);
@@ -1352,8 +1399,12 @@ int enq_head(IterEnq& e, bool lowp_left) {
     run.launched(AM1GPU_PHASE_FOCK);
     if ((rc = run.end(AM1GPU_PHASE_FOCK, e.ph)) || (rc = run.begin(&e.ph))) return rc;
     launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-        if (pairs) k_commutator16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
-        else k_commutator8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+        if (pairs && b.sp2_tma)
+            k_commutator_tma<<<nt, 128, dgemm_tma_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st, b.d_sp2_maps, b.d_sp2_active + 2);
+        else if (pairs)
+            k_commutator16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
+        else
+            k_commutator8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_jobs, t, nt, b.d_st);
     });
     k_post_fock<<<dim3(e.nblk, e.njobs), 256, 0, s>>>(b.d_jobs, b.d_mols, b.d_st, e.nblk, 0, 0);
     run.launched(AM1GPU_PHASE_COMMUTATOR, 2);
@@ -1389,8 +1440,12 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
     if ((rc = run.begin(&pc))) return rc;
     int nl = 0;
     launch_tiles(b, s, [&](const GemmTile* t, int nt, bool pairs) {
-        if (pairs) k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
-        else k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+        if (pairs && b.sp2_tma)
+            k_sp2_step_tma<<<nt, 128, dgemm_tma_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state, b.d_sp2_maps, b.d_sp2_active + 2);
+        else if (pairs)
+            k_sp2_step16<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
+        else
+            k_sp2_step8<<<nt, 128, dgemm_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
         ++nl;
     });
     if (b.nt_oz > 0) {
@@ -1607,7 +1662,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = run.begin(&ph))) return rc;
     CK(cudaMemsetAsync(b.d_status, 0, sizeof(int) * b.nmol, s));
     CK(cudaMemsetAsync(b.d_work, 0, sizeof(double) * kWorkN, s));
-    CK(cudaMemsetAsync(b.d_sp2_active, 0, 4 * sizeof(int), s));  // [2]: error word of the tcgen05 step
+    CK(cudaMemsetAsync(b.d_sp2_active, 0, 4 * sizeof(int), s));  // [2]: error word of the tensor-core steps
     CK(cudaMemsetAsync(b.d_arena, 0, sizeof(double) * b.arena_doubles, s));
     // mixed precision: every molecule starts with TF32 purification (k_converge ends that phase)
     const bool mixed = o.precision == AM1GPU_PRECISION_MIXED && density_mode() == 0;
@@ -1686,7 +1741,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     CK(cudaMemcpyAsync(b.h_active + 2, b.d_sp2_active + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (b.h_active[2] & (1 << 10)) return fail(AM1GPU_LINALG, "a purification iterate left the range of its digit planes (|x| >= 2)");
-    if (b.h_active[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
+    if (b.h_active[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core step gave up waiting for its MMAs or operand copies");
     stats->purification_steps += b.h_work[0];
     stats->purification_flops += b.h_work[1];
     stats->purification_bytes += b.h_work[3];
@@ -2369,7 +2424,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         off += bytes;
         return o;
     };
-    const size_t o_job = take(sizeof(Sp2Job)), o_t64 = take(sizeof(GemmTile) * nt64), o_t128 = take(sizeof(GemmTile) * nt128),
+    const size_t o_job = take(sizeof(Sp2Job)), o_maps = take(4 * sizeof(TmaDesc)), o_t64 = take(sizeof(GemmTile) * nt64),
+                 o_t128 = take(sizeof(GemmTile) * nt128),
                  o_toz = take(sizeof(GemmTile) * ntoz),
                  o_ms = take(sizeof(MolState)), o_f = take(8 * nn), o_rmin = take(8 * (size_t)n), o_rmax = take(8 * (size_t)n);
     const size_t staged = align256(off);
@@ -2416,6 +2472,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     jb.Dq0 = (int8_t*)(D + o_dq);
     jb.Dq1 = jb.Dq0 + (size_t)kOzPlanes * n * ldq;
     std::memcpy(H + o_job, &jb, sizeof jb);
+    TmaDesc* hmaps = (TmaDesc*)(H + o_maps);
+    const bool tma = encode_square_map(&hmaps[0], jb.X0, n) && encode_square_map(&hmaps[1], jb.X1, n);
     GemmTile* hoz = (GemmTile*)(H + o_toz);
     int koz = 0;
     for (int tm = 0; tm < t128; ++tm)
@@ -2465,8 +2523,12 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     int* hact = (int*)(H + staged);
     for (int step = 0; step < kSp2MaxSteps; ++step) {
         if (precision == 0) {
-            if (pairs) k_sp2_step16<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
-            else k_sp2_step8<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+            if (tma)
+                k_sp2_step_tma<<<nt64, 128, dgemm_tma_smem_bytes(), s>>>(dj, d64, nt64, dsst, (const TmaDesc*)(D + o_maps), dact + 2);
+            else if (pairs)
+                k_sp2_step16<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+            else
+                k_sp2_step8<<<nt64, 128, dgemm_smem_bytes(), s>>>(dj, d64, nt64, dsst);
         } else if (precision == 3) {
             k_sp2_step_oz<<<ntoz, 128, oz_smem_bytes(), s>>>(dj, (const GemmTile*)(D + o_toz), ntoz, dsst, dact + 2);
         } else if (precision == 2) {
@@ -2494,7 +2556,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     CK(cudaStreamSynchronize(s));
     if (steps_out) *steps_out = hs->steps;
     if (hact[2] & (1 << 10)) return fail(AM1GPU_LINALG, "a purification iterate left the range of its digit planes (|x| >= 2)");
-    if (hact[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core purification step gave up waiting for its MMAs");
+    if (hact[2]) return fail(AM1GPU_DEVICE_ERROR, "a tensor-core step gave up waiting for its MMAs or operand copies");
     if (!hs->converged) return fail(AM1GPU_LINALG, "the purification did not reach idempotency (gap too small)");
     return AM1GPU_OK;
 }

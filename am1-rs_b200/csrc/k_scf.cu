@@ -153,10 +153,13 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
 // upper-triangle tiles are computed.  The epilogue takes the strict upper triangle: it stores e in
 // the packed history slot of this iteration and forms this tile's share of |e|_F^2 and of
 // <e, e_slot> for every live slot (the new CDIIS Gram row).
-template <bool PAIRS>
+//
+// COPY: how the operands reach shared memory: 0 8-byte cp.async, 1 16-byte cp.async (even n, 16-byte
+// aligned rows), 2 tensor-memory-accelerator boxes from the job's tensor maps of F and P
+// (maps[4 job + 2], maps[4 job + 3]; a copy wait that runs out sets bit 11 of *err).
+template <int COPY>
 __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
-                                                const MolState* __restrict__ st) {
-    extern __shared__ __align__(16) double dsm[];
+                                                const MolState* __restrict__ st, const TmaDesc* __restrict__ maps, int* __restrict__ err) {
     __shared__ double red[CP_N][4];
     const int t = blockIdx.x;
     if (t >= ntiles) return;
@@ -174,7 +177,18 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
     // e is antisymmetric: a warp whose quarter is padding or lies below the diagonal issues no MMAs
     const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
     double acc[2][4][4];
-    dg_mainloop_diff<PAIRS>(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
+    if constexpr (COPY == 2) {
+        extern __shared__ __align__(1024) unsigned char ctsm[];
+        __shared__ DtBars bars;
+        const TmaDesc* mp = maps + 4 * tl.job;  // F and P are symmetric: B = F or P read by rows
+        if (!dg_mainloop_tma(dt_stages(ctsm), bars, mp + 2, mp + 3, mp + 3, mp + 2, false, n, m0, n0, acc, compute)) {
+            if (threadIdx.x == 0) atomicOr(err, 1 << 11);
+            return;
+        }
+    } else {
+        extern __shared__ __align__(16) double dsm[];
+        dg_mainloop_diff<COPY == 1>(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
+    }
     double v[CP_N];
 #pragma unroll
     for (int k = 0; k < CP_N; ++k) v[k] = 0.0;
@@ -217,11 +231,16 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
 
 __global__ void __launch_bounds__(DG_THREADS, 4) k_commutator16(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
                                                                 int ntiles, const MolState* __restrict__ st) {
-    commutator_body<true>(jobs, tiles, ntiles, st);
+    commutator_body<1>(jobs, tiles, ntiles, st, nullptr, nullptr);
 }
 __global__ void __launch_bounds__(DG_THREADS, 4) k_commutator8(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
                                                                int ntiles, const MolState* __restrict__ st) {
-    commutator_body<false>(jobs, tiles, ntiles, st);
+    commutator_body<0>(jobs, tiles, ntiles, st, nullptr, nullptr);
+}
+__global__ void __launch_bounds__(DG_THREADS, 4) k_commutator_tma(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                                  int ntiles, const MolState* __restrict__ st,
+                                                                  const TmaDesc* __restrict__ maps, int* __restrict__ err) {
+    commutator_body<2>(jobs, tiles, ntiles, st, maps, err);
 }
 
 // Gaussian elimination with partial pivoting; false when a pivot is below 1e-12.

@@ -463,30 +463,14 @@ __global__ void k_sp2_start(const Sp2Job* __restrict__ jobs, Sp2State* __restric
     s.square = fabs(fr - jb.nocc) < fabs(2.0 * tr - fr - jb.nocc) ? 1 : 0;
 }
 
-// One SP2 step over all upper-triangle 64x64 tiles of every active channel.
-template <bool PAIRS>
-__device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
-                                              const Sp2State* __restrict__ sst) {
-    extern __shared__ __align__(16) double dsm[];
-    __shared__ double red[2][4];
-    const int t = blockIdx.x;
-    if (t >= ntiles) return;
-    const GemmTile tl = tiles[t];
-    const Sp2State* sp = sst + tl.job;
-    const Sp2Job* jp = jobs + tl.job;
-    if (!sp->active || sp->lowp || jp->oz) return;  // TF32 runs: k_sp2_step_tf32 / _tc; digit products: k_sp2_step_oz
-    const int n = jp->n;
+// Epilogue of one purification-step tile: Y = X^2 or 2X - X^2 for r <= c, mirrored; the tile's
+// partial trace and Frobenius sums into the job's partials (the job fields it needs are read only
+// now, so they hold no registers during the k-loop).
+__device__ __forceinline__ void sp2_step_epilogue(const Sp2Job* __restrict__ jp, const Sp2State* __restrict__ sp, int t, int n,
+                                                  int m0, int n0, const double acc[2][4][4], bool compute, double red[2][4]) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cur = sp->cur;
     const double* X = cur ? jp->X1 : jp->X0;
-    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // only the upper triangle of X^2 is computed: a warp whose quarter is padding or lies below
-    // the diagonal of a diagonal tile issues no MMAs
-    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
-    double acc[2][4][4];
-    dg_mainloop<PAIRS>(dsm, X, n, X, n, n, n, n, m0, n0, acc, compute);  // X symmetric: X[rows m0..] . X[:, n0..]
-    // epilogue: Y = X^2 or 2X - X^2 for r <= c, mirrored; partial trace / Frobenius sums (the job
-    // fields it needs are read only now, so they hold no registers during the k-loop)
     double* Y = cur ? jp->X0 : jp->X1;
     const int square = sp->square;
     double tr = 0.0, fr = 0.0;
@@ -525,6 +509,58 @@ __device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, c
         p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
         p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
     }
+}
+
+// One SP2 step over all upper-triangle 64x64 tiles of every active channel (operands copied by
+// cp.async: k_sp2_step8 for odd n, and k_sp2_step16 where the tensor-map kernel is not used).
+template <bool PAIRS>
+__device__ __forceinline__ void sp2_step_body(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
+                                              const Sp2State* __restrict__ sst) {
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ double red[2][4];
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const Sp2State* sp = sst + tl.job;
+    const Sp2Job* jp = jobs + tl.job;
+    if (!sp->active || sp->lowp || jp->oz) return;  // TF32 runs: k_sp2_step_tf32 / _tc; digit products: k_sp2_step_oz
+    const int n = jp->n;
+    const double* X = sp->cur ? jp->X1 : jp->X0;
+    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
+    // only the upper triangle of X^2 is computed: a warp whose quarter is padding or lies below
+    // the diagonal of a diagonal tile issues no MMAs
+    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
+    double acc[2][4][4];
+    dg_mainloop<PAIRS>(dsm, X, n, X, n, n, n, n, m0, n0, acc, compute);  // X symmetric: X[rows m0..] . X[:, n0..]
+    sp2_step_epilogue(jp, sp, t, n, m0, n0, acc, compute, red);
+}
+
+// The same step for even n with the operands copied by the tensor memory accelerator from the
+// job's tensor maps (maps[4 job + cur] describes the current iterate), through the mbarrier
+// pipeline of dg_mainloop_tma: bit-identical to k_sp2_step16.  A copy wait that runs out sets bit
+// 11 of *err and the tile is left unwritten.
+__global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step_tma(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                               int ntiles, const Sp2State* __restrict__ sst,
+                                                               const TmaDesc* __restrict__ maps, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char dtsm[];
+    __shared__ DtBars bars;
+    __shared__ double red[2][4];
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const Sp2State* sp = sst + tl.job;
+    const Sp2Job* jp = jobs + tl.job;
+    if (!sp->active || sp->lowp || jp->oz) return;
+    const int n = jp->n;
+    const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
+    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
+    const TmaDesc* map = maps + 4 * tl.job + sp->cur;
+    double acc[2][4][4];
+    if (!dg_mainloop_tma(dt_stages(dtsm), bars, map, map, nullptr, nullptr, tl.tm == tl.tn, n, m0, n0, acc, compute)) {
+        if (threadIdx.x == 0) atomicOr(err, 1 << 11);
+        return;
+    }
+    sp2_step_epilogue(jp, sp, t, n, m0, n0, acc, compute, red);
 }
 
 // After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
@@ -615,6 +651,7 @@ __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __
 }
 
 size_t dgemm_smem_bytes() { return DG_SMEM; }
+size_t dgemm_tma_smem_bytes() { return DT_SMEM; }
 
 __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step16(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
                                                               int ntiles, const Sp2State* __restrict__ sst) {

@@ -24,6 +24,12 @@ struct GemmTile {
     int tm, tn;
 };
 
+// A tensor map (the driver's opaque 128-byte CUtensorMap, 64-byte aligned) as the kernels receive
+// it: the device only passes its address to cp.async.bulk.tensor.
+struct __align__(64) TmaDesc {
+    unsigned long long w[16];
+};
+
 // One eigenproblem (a channel of a molecule).
 struct EigJob {
     const double* Gt;      // C0^T F (rows = columns of F C0), n x n
@@ -170,6 +176,13 @@ __global__ void k_sp2_start(const Sp2Job* jobs, Sp2State* sst, const MolState* s
 // *8: any matrix (8-byte copies)
 __global__ void k_sp2_step16(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
 __global__ void k_sp2_step8(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
+// the *16 tiles with the operands copied by the tensor memory accelerator: maps[4 job + i] is the
+// tensor map of job's X_i, maps[4 job + 2] and [4 job + 3] those of the channel's F and P (n x n
+// FP64, box 16 x 64, 128-byte swizzle); dgemm_tma_smem_bytes() of dynamic shared memory; a copy
+// wait that runs out sets bit 11 of *err
+__global__ void k_sp2_step_tma(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, const TmaDesc* maps,
+                               int* err);
+size_t dgemm_tma_smem_bytes();
 // the TF32 step of the mixed path's reduced-precision iterations (jobs with Sp2State::lowp);
 // tf32_smem_bytes() of dynamic shared memory, same tile lists
 __global__ void k_sp2_step_tf32(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst);
@@ -177,6 +190,9 @@ size_t tf32_smem_bytes();
 // E = F.P - P.F over the upper-triangle tiles: history push of E and its CDIIS Gram row
 __global__ void k_commutator16(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
 __global__ void k_commutator8(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st);
+// the *16 tiles from the tensor maps of F and P (maps[4 job + 2], [4 job + 3]); dgemm_tma_smem_bytes()
+__global__ void k_commutator_tma(const ChanJob* jobs, const GemmTile* tiles, int ntiles, const MolState* st, const TmaDesc* maps,
+                                 int* err);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 size_t tc_smem_bytes();
