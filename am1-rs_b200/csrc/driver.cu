@@ -1111,6 +1111,25 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     }
     hpp[b.nmol] = a_off;
     b.nt_gt = b.nt_dn = ntile;
+    // each launch takes its jobs' tiles largest matrix first (a job's tiles stay contiguous, in the
+    // same order, so its partial sums are unchanged): the long k-loops start in the first waves and
+    // the last wave holds short ones
+    auto largest_first = [&](std::vector<GemmTile>& v) {
+        std::vector<std::pair<int, int>> blocks;  // (first tile, job), one per job
+        for (size_t i = 0; i < v.size(); ++i)
+            if (i == 0 || v[i].job != v[i - 1].job) blocks.push_back({(int)i, v[i].job});
+        std::stable_sort(blocks.begin(), blocks.end(),
+                         [&](const std::pair<int, int>& x, const std::pair<int, int>& y) { return hsp2[x.second].n > hsp2[y.second].n; });
+        std::vector<GemmTile> out;
+        out.reserve(v.size());
+        for (auto& bk : blocks) {
+            hsp2[bk.second].tile0 = (int)out.size();
+            for (int i = bk.first; i < bk.first + hsp2[bk.second].ntiles; ++i) out.push_back(v[i]);
+        }
+        v.swap(out);
+    };
+    largest_first(tiles_pairs);
+    largest_first(tiles_other);
     for (size_t i = 0; i < tiles_pairs.size(); ++i) hsp2t[i] = tiles_pairs[i];
     for (size_t i = 0; i < tiles_other.size(); ++i) hsp2t[tiles_pairs.size() + i] = tiles_other[i];
     b.nt_sp2_pairs = (int)tiles_pairs.size();
