@@ -516,7 +516,8 @@ def run_ours(args):
                          "scf_device_ms": grad_stats["device_ms"]},
             "e2e": {"value": world * nmol * args.steps / e2e_s, "unit": "solves/s",
                     "h2d_bytes_per_step": e2e_stats["h2d_bytes"], "d2h_bytes_per_step": e2e_stats["d2h_bytes"]},
-            "roofline": {"kernel": "k_sp2_step (density purification: symmetric FP64 X.X on mma.sync m16n8k8 f64)",
+            "roofline": {"kernel": "k_sp2_step_tma (density purification: symmetric FP64 X.X on mma.sync m16n8k8 f64, "
+                                   "operands copied by TMA through an mbarrier pipeline)",
                          "bound": "tensor", "achieved": achieved_tf, "peak": peak_fp64, "unit": "TFLOP/s",
                          "frac": achieved_tf / peak_fp64 if peak_fp64 else None,
                          "traffic": SP2_DRAM_PER_ALG_BYTE * sp2_bytes / max(pl["eigen:inner"], 1),
