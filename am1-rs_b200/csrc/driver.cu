@@ -715,7 +715,9 @@ struct Batch {
     int* d_big_stall = nullptr;  // per channel job: 1 when a large molecule's purification stalled this iteration
     GraphLoop* d_loop = nullptr;  // loop counters of the captured solve
     GraphLoop* h_loop = nullptr;  // their pinned host copy
-    int64_t graph_counts[3] = {0, 0, 0};  // kernels per captured head (+ arm), step (+ condition), tail (+ condition)
+    // kernels per captured head (+ arm), step (+ condition), tail (+ its two control kernels), and
+    // stalled-purification eigensolver (run in GraphLoop::eig_runs iterations)
+    int64_t graph_counts[4] = {0, 0, 0, 0};
     bool graph_cacheable = false;  // a resident batch keeps its instantiated graph across runs
     cudaGraphExec_t graph_exec = nullptr;
 };
@@ -1491,8 +1493,12 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
 }
 
 // The density of the iteration (the purified X, or the eigensolver for stalled and Jacobi-path
-// molecules), the density change and the convergence test.
-int enq_tail(IterEnq& e) {
+// molecules), the density change and the convergence test, in three parts: the purified density
+// (enq_tail_finish), the eigensolver for the molecules whose purification stalled (enq_tail_stall:
+// its kernels skip every other molecule, and the captured solve runs it only in iterations where
+// some purification stalled), and the rest (enq_tail_rest).  The Jacobi density path (density_mode
+// != 0) is all in enq_tail_finish.
+int enq_tail_finish(IterEnq& e) {
     Batch& b = e.b;
     const cudaStream_t s = e.s;
     Run& run = *e.run;
@@ -1503,14 +1509,6 @@ int enq_tail(IterEnq& e) {
                                                                b.d_big_stall, b.d_active + 3);
         run.launched(AM1GPU_PHASE_EIGEN);
         if (!b.sp2_big.empty() && (rc = big_fallback(b, e.ws))) return rc;
-        // stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
-        k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
-        if ((rc = launch_jacobi(b, e.ws, 0, b.d_need_eigen, e.s))) return rc;
-        run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
-        if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
-        k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
-        run.launched(AM1GPU_PHASE_EIGEN, 3);
-        if ((rc = run.end(AM1GPU_PHASE_EIGEN, e.ph)) || (rc = run.begin(&e.ph))) return rc;
     } else {
         k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, nullptr);
         CK(cudaGetLastError());
@@ -1525,12 +1523,46 @@ int enq_tail(IterEnq& e) {
         k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, nullptr);
         run.launched(AM1GPU_PHASE_DENSITY);
     }
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+// Stalled purifications: warm-started Jacobi + C_occ C_occ^T for those molecules only
+// (need_eigen); nothing on the Jacobi density path.
+int enq_tail_stall(IterEnq& e) {
+    Batch& b = e.b;
+    const cudaStream_t s = e.s;
+    Run& run = *e.run;
+    int rc;
+    if (density_mode() != 0) return AM1GPU_OK;
+    k_gemm_nn<<<b.nt_gt, 256, 0, s>>>(b.d_gj_gt, b.d_gt_gt, b.nt_gt, b.d_st, 0, b.d_need_eigen);
+    if ((rc = launch_jacobi(b, e.ws, 0, b.d_need_eigen, e.s))) return rc;
+    run.launched(AM1GPU_PHASE_EIGEN, (int)b.buckets.size());
+    if (b.neig > 0) k_eig_sort<<<b.neig, 512, 0, s>>>(b.d_eig, b.d_st, 0, b.d_need_eigen);
+    k_gemm_tn<<<b.nt_dn, 256, 0, s>>>(b.d_gj_dn, b.d_gt_dn, b.nt_dn, b.d_st, 0, b.d_need_eigen);
+    run.launched(AM1GPU_PHASE_EIGEN, 3);
+    CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+int enq_tail_rest(IterEnq& e) {
+    Batch& b = e.b;
+    const cudaStream_t s = e.s;
+    Run& run = *e.run;
+    int rc;
+    if (density_mode() == 0 && ((rc = run.end(AM1GPU_PHASE_EIGEN, e.ph)) || (rc = run.begin(&e.ph)))) return rc;
     k_density_post<<<dim3(e.nblk, e.njobs), 256, 0, s>>>(b.d_jobs, b.d_st, e.nblk);
     k_converge<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, e.nblk, e.prm,
                                                  b.d_active);
     run.launched(AM1GPU_PHASE_DENSITY, 2);
     if ((rc = run.end(AM1GPU_PHASE_DENSITY, e.ph))) return rc;
     CK(cudaGetLastError());
+    return AM1GPU_OK;
+}
+
+int enq_tail(IterEnq& e) {
+    int rc;
+    if ((rc = enq_tail_finish(e)) || (rc = enq_tail_stall(e)) || (rc = enq_tail_rest(e))) return rc;
     return AM1GPU_OK;
 }
 
@@ -1582,10 +1614,26 @@ int add_while(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, 
     return AM1GPU_OK;
 }
 
+// An IF node after `dep` in g, with handle h; its body graph in *body.
+int add_if(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    CK(cudaGraphAddNode(node, g, &dep, 1, &np));
+    *body = np.conditional.phGraph_out[0];
+    return AM1GPU_OK;
+}
+
 // The SCF loop of run_device as one graph launch:
 //   k_scf_arm -> WHILE(scf) { head -> k_sp2_arm -> WHILE(sp2) { step -> k_sp2_cond } -> tail -> k_scf_cond }
+// and, in a graph kept for a resident batch's later runs, the tail split as
+//   finish -> k_stall_arm -> IF(stall) { stalled-purification eigensolver } -> rest -> k_scf_cond.
 // The kernels are the eager loop's, in the same order; only the loop decisions moved to the device
-// (k_graph.cu), so the results are the same bit for bit.  The purification loop stops as soon as no
+// (k_graph.cu), and the eigensolver kernels for stalled purifications, which change nothing in an
+// iteration where no purification stalled, run only in iterations where one did.  So the results
+// are the same bit for bit.  The purification loop stops as soon as no
 // channel purifies (the eager loop looks every six steps from the twelfth on); the extra eager
 // steps change nothing, because finished channels skip their products.
 // *launched: the graph was launched (an error before that leaves the stream untouched).
@@ -1646,14 +1694,43 @@ int scf_loop_graph(IterEnq& e, const am1gpu_options& o, bool* launched) {
         return rc;
     const int64_t per_step = cnt.kernel_launches - step0 + 1;
     const int64_t tail0 = cnt.kernel_launches;
-    if ((rc = capture_into(cs, body, &w_sp2, 1, &tail, [&]() -> int {
-             int r = enq_tail(ce);
-             if (r) return r;
-             k_scf_cond<<<1, 32, 0, cs>>>(h_scf, b.d_loop, b.d_active, o.max_scf);
-             return AM1GPU_OK;
-         })))
-        return rc;
-    const int64_t per_tail = cnt.kernel_launches - tail0 + 1;
+    int64_t per_stall = 0, per_tail = 0;
+    if (b.graph_cacheable) {
+        // a graph kept for the batch's later runs: the stalled-purification eigensolver behind an IF
+        // node (its extra capture and instantiation cost more than they save in a one-off graph)
+        cudaGraphConditionalHandle h_stall;
+        CK(cudaGraphConditionalHandleCreate(&h_stall, body, 0, 0));
+        cudaGraphNode_t fin, w_stall, stall_last;
+        if ((rc = capture_into(cs, body, &w_sp2, 1, &fin, [&]() -> int {
+                 int r = enq_tail_finish(ce);
+                 if (r) return r;
+                 k_stall_arm<<<1, 256, 0, cs>>>(h_stall, b.d_loop, b.d_need_eigen, b.nmol);
+                 return AM1GPU_OK;
+             })))
+            return rc;
+        const int64_t stall0 = cnt.kernel_launches;
+        cudaGraph_t body3 = nullptr;
+        if ((rc = add_if(body, fin, h_stall, &w_stall, &body3))) return rc;
+        if ((rc = capture_into(cs, body3, nullptr, 0, &stall_last, [&]() -> int { return enq_tail_stall(ce); }))) return rc;
+        per_stall = cnt.kernel_launches - stall0;
+        if ((rc = capture_into(cs, body, &w_stall, 1, &tail, [&]() -> int {
+                 int r = enq_tail_rest(ce);
+                 if (r) return r;
+                 k_scf_cond<<<1, 32, 0, cs>>>(h_scf, b.d_loop, b.d_active, o.max_scf);
+                 return AM1GPU_OK;
+             })))
+            return rc;
+        per_tail = cnt.kernel_launches - tail0 + 2 - per_stall;
+    } else {
+        if ((rc = capture_into(cs, body, &w_sp2, 1, &tail, [&]() -> int {
+                 int r = enq_tail(ce);
+                 if (r) return r;
+                 k_scf_cond<<<1, 32, 0, cs>>>(h_scf, b.d_loop, b.d_active, o.max_scf);
+                 return AM1GPU_OK;
+             })))
+            return rc;
+        per_tail = cnt.kernel_launches - tail0 + 1;
+    }
     cudaGraphExec_t ge = nullptr;
     CK(cudaGraphInstantiate(&ge, g, 0));
     *launched = true;
@@ -1665,6 +1742,7 @@ int scf_loop_graph(IterEnq& e, const am1gpu_options& o, bool* launched) {
     b.graph_counts[0] = per_head;
     b.graph_counts[1] = per_step;
     b.graph_counts[2] = per_tail;
+    b.graph_counts[3] = per_stall;
     return AM1GPU_OK;
 }
 
@@ -1771,7 +1849,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
         const GraphLoop lp = *b.h_loop;
         stats->scf_cycles = lp.scf_iter;
         stats->kernel_launches += 1 + (int64_t)lp.scf_iter * (b.graph_counts[0] + b.graph_counts[2]) +
-                                  (int64_t)lp.sp2_total * b.graph_counts[1];
+                                  (int64_t)lp.sp2_total * b.graph_counts[1] + (int64_t)lp.eig_runs * b.graph_counts[3];
         stats->graph_launches += 1;
     }
     float ms = 0.f;

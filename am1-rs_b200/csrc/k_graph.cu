@@ -19,6 +19,7 @@ __global__ void k_scf_arm(cudaGraphConditionalHandle h, GraphLoop* loop, int max
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     loop->scf_iter = 0;
     loop->sp2_total = 0;
+    loop->eig_runs = 0;
     cudaGraphSetConditional(h, max_scf > 0 ? 1u : 0u);
 }
 
@@ -40,6 +41,18 @@ __global__ void k_sp2_cond(cudaGraphConditionalHandle h, GraphLoop* loop, int* a
     const int more = *active_count > 0 && step < max_steps;
     *active_count = 0;
     cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// After the purified densities of an iteration: the stalled-purification eigensolver runs only if
+// some molecule's purification stalled (need_eigen set by k_sp2_finish).  One CTA.
+__global__ void k_stall_arm(cudaGraphConditionalHandle h, GraphLoop* loop, const int* need_eigen, int nmol) {
+    int any = 0;
+    for (int i = threadIdx.x; i < nmol; i += blockDim.x) any |= need_eigen[i] != 0;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        if (any) loop->eig_runs += 1;
+        cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
 }
 
 // After each SCF iteration (k_converge has counted the molecules still iterating in active[0]):

@@ -124,11 +124,12 @@ struct GraphLoop {
     int scf_iter;   // SCF iterations done in this launch
     int sp2_step;   // purification steps of the current iteration
     int sp2_total;  // purification steps of this launch
-    int pad;
+    int eig_runs;   // iterations of this launch in which the stalled-purification eigensolver ran
 };
 __global__ void k_scf_arm(cudaGraphConditionalHandle h, GraphLoop* loop, int max_scf);
 __global__ void k_sp2_arm(cudaGraphConditionalHandle h, GraphLoop* loop, int* active_count);
 __global__ void k_sp2_cond(cudaGraphConditionalHandle h, GraphLoop* loop, int* active_count, int max_steps);
+__global__ void k_stall_arm(cudaGraphConditionalHandle h, GraphLoop* loop, const int* need_eigen, int nmol);
 __global__ void k_scf_cond(cudaGraphConditionalHandle h, GraphLoop* loop, const int* active, int max_scf);
 
 struct ScfParams {

@@ -260,11 +260,35 @@ def test_stalled_purification_falls_back_above_448_orbitals(tmp_path):
             assert np.max(np.abs(g["charges"] - o["charges"])) < 1e-7
             assert abs(g["iterations"] - o["iterations"]) <= 1
             assert st["eigen_fallbacks"] >= g["iterations"], (st["eigen_fallbacks"], g["iterations"])
+            # the host-driven loop (phase timing on) against the captured solve, whose eigensolver for
+            # stalled purifications sits behind a device-decided IF node (up to 448 orbitals)
+            native.set_timing(True)
+            ge = native.scf(m.numbers, xyz, 0.0, mult, want_matrices=False)
+            native.set_timing(False)
+            assert ge["heat_of_formation_kcal"] == g["heat_of_formation_kcal"] and ge["iterations"] == g["iterations"]
             print(g["nao"], g["iterations"], st["eigen_fallbacks"])
         status, res = native.scf_batch(batch)
         assert all(s == 0 for s in status), status
         for (z, xyz, q, mult), r in zip(batch, res):
             assert r["heat_of_formation_kcal"] == native.scf(z, xyz, q, mult, want_matrices=False)["heat_of_formation_kcal"]
+        # a resident batch of small molecules: its kept graph runs the eigensolver for stalled
+        # purifications behind a device-decided IF node; against the host-driven loop, bit for bit
+        small = [batch[2]] + [(w.numbers, _abi.angstrom_to_bohr(w.xyz), 0.0, 1) for w in (W.water_cluster(9, rng), W.water_cluster(3, rng))]
+        native.set_timing(True)
+        st_e, res_e = native.scf_batch(small, want_matrices=True)
+        native.set_timing(False)
+        rb = native.ResidentBatch(small)
+        try:
+            for _ in range(2):
+                rb.run()
+                stats = rb.stats()
+                assert stats["graph_launches"] == 1 and stats["eigen_fallbacks"] > 0, stats
+                st_g, res_g = rb.results()
+                assert st_g == st_e and all(x == 0 for x in st_g)
+                for a, b in zip(res_e, res_g):
+                    assert a["heat_of_formation_kcal"] == b["heat_of_formation_kcal"] and a["iterations"] == b["iterations"]
+        finally:
+            rb.close()
         print("ok")
     """)
     f = tmp_path / "stall.py"
