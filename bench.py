@@ -141,9 +141,9 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # CPU baseline / reference arm: the oracle (C++ restatement of am1-rs's SCF) on host cores
 # ---------------------------------------------------------------------------------------
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_sp2_step launch over the whole 512-molecule
-# batch (every molecule active), divided by that launch's algorithmic bytes 16 sum(n^2): 257.3 MB /
-# 297.0 MB, from one ncu capture of that launch.  Traffic grows with the molecules a launch
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_sp2_step_tma launch over the whole 512-molecule
+# batch (every molecule active), divided by that launch's algorithmic bytes 16 sum(n^2): 256.4 and
+# 258.3 MB / 297.0 MB in two captured launches (the cp.async kernel moved 257.3 MB).  Traffic grows with the molecules a launch
 # processes, so the per-launch traffic of this run is its algorithmic bytes times this ratio.
 SP2_DRAM_PER_ALG_BYTE = 0.866
 
