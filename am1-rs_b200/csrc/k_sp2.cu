@@ -143,17 +143,32 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
     for (int i = tid; i < n; i += SP2_BOUND_THREADS) q[i] *= inq;
     __syncthreads();
     const int K = min(SP2_LANCZOS, n);
+    const bool pairs = (n & 1) == 0 && (reinterpret_cast<uintptr_t>(jb.F) & 15) == 0;
     int m = 0;
     double bprev = 0.0;
     for (int j = 0; j < K; ++j) {
-        // w = F q: eight lanes per row, so every warp has four rows' loads in flight
+        // w = F q: eight lanes per row, so every warp has four rows' loads in flight; rows of even
+        // length on 16-byte boundaries are read as pairs (16-byte loads, two partial sums per lane)
         const int sub = lane >> 3, sl = lane & 7;
         for (int r0 = 4 * warp; r0 < n; r0 += 4 * NW) {
             const int r = r0 + sub;
             double acc = 0.0;
             if (r < n) {
                 const double* Fr = jb.F + (long long)r * n;
-                for (int c = sl; c < n; c += 8) acc = fma(Fr[c], q[c], acc);
+                if (pairs) {
+                    const double2* F2 = reinterpret_cast<const double2*>(Fr);
+                    const double2* q2 = reinterpret_cast<const double2*>(q);
+                    double acc1 = 0.0;
+#pragma unroll 4
+                    for (int c = sl; c < n / 2; c += 8) {
+                        const double2 f = F2[c], x = q2[c];
+                        acc = fma(f.x, x.x, acc);
+                        acc1 = fma(f.y, x.y, acc1);
+                    }
+                    acc += acc1;
+                } else {
+                    for (int c = sl; c < n; c += 8) acc = fma(Fr[c], q[c], acc);
+                }
             }
             for (int o = 4; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (sl == 0 && r < n) w[r] = acc;
