@@ -362,7 +362,7 @@ def g_matrix_batch(numbers, xyz_bohr, densities, method="am1"):
     return g
 
 
-PURIFY_PRECISION = {"fp64": 0, "fp32_tcgen05": 1, "tf32": 2, "fp64_digits": 3}
+PURIFY_PRECISION = {"fp64": 0, "fp32_tcgen05": 1, "tf32": 2, "fp64_digits": 3, "tf32_tcgen05": 4}
 
 
 def density_purify(f, n_occ, weight=2.0, precision="fp64"):
@@ -377,15 +377,18 @@ def density_purify(f, n_occ, weight=2.0, precision="fp64"):
     return p, steps.value
 
 
+LOWP_KERNELS = ("mma.sync tf32", "tcgen05 3xtf32", "tcgen05 tf32")
+
+
 def lowp_tuning() -> dict:
     """The autotuner's choice of reduced-precision purification kernel per size class on this device
-    (``am1gpu_lowp_tuning``): {class: {"kernel": "tcgen05" | "mma.sync tf32" | None, "ms": (mma.sync, tcgen05)}}."""
+    (``am1gpu_lowp_tuning``): {class: {"kernel": one of LOWP_KERNELS or None, "ms": {kernel: ms}}}."""
     choice = (ctypes.c_int32 * 4)()
-    ms = (ctypes.c_float * 8)()
+    ms = (ctypes.c_float * 12)()
     _check(_abi.lib().am1gpu_lowp_tuning(choice, ms))
     names = ["n<=128", "n<=256", "n<=384", "n>384"]
-    kern = {1: "tcgen05", 0: "mma.sync tf32", -1: None}
-    return {names[c]: {"kernel": kern[choice[c]], "ms": (ms[2 * c], ms[2 * c + 1])} for c in range(4)}
+    return {names[c]: {"kernel": LOWP_KERNELS[choice[c]] if choice[c] >= 0 else None,
+                       "ms": {k: ms[3 * c + i] for i, k in enumerate(LOWP_KERNELS)}} for c in range(4)}
 
 
 def eigvalsh(a):

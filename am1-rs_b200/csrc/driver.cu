@@ -232,6 +232,9 @@ int device_ctx(DeviceCtx** out) {
             return bad("tf32 tile kernel smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_sp2_step_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes())) != cudaSuccess)
             return bad("tcgen05 tile kernel smem attribute", err);
+        if ((err = cudaFuncSetAttribute(k_sp2_step_tc1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc1_smem_bytes())) !=
+            cudaSuccess)
+            return bad("single-pass tcgen05 tile kernel smem attribute", err);
         if ((err = cudaFuncSetAttribute(k_sp2_step_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oz_smem_bytes())) != cudaSuccess)
             return bad("digit-plane tile kernel smem attribute", err);
         for (const void* f : {(const void*)k_tridiag_syr2k16, (const void*)k_tridiag_syr2k8, (const void*)k_dgemm16,
@@ -376,17 +379,18 @@ int sp2_max_steps() {
     return v;
 }
 
-// Which molecules' reduced-precision purification products run on tcgen05 (k_sp2_step_tc, FP32
-// accuracy from 3xTF32) rather than mma.sync TF32 (k_sp2_step_tf32).  AM1GPU_LOWP_TC=1 or 0 forces
-// one kernel; otherwise the autotuner's choice for the molecule's size class (tune_lowp_kernels,
-// run once per device and class before the first mixed batch that holds such a molecule).
+// Which kernel takes a molecule's reduced-precision purification products: 0 mma.sync TF32
+// (k_sp2_step_tf32), 1 tcgen05 at FP32 accuracy from 3xTF32 (k_sp2_step_tc), 2 tcgen05 in one TF32
+// pass (k_sp2_step_tc1).  AM1GPU_LOWP_TC=0, 1 or 2 forces one kernel; otherwise the autotuner's
+// choice for the molecule's size class (tune_lowp_kernels, run once per device and class before the
+// first mixed batch that holds such a molecule).
 constexpr int kTuneClasses = 4;
 inline int tune_class(int n) { return n <= 128 ? 0 : n <= 256 ? 1 : n <= 384 ? 2 : 3; }
 constexpr int kTuneSize[kTuneClasses] = {96, 192, 320, 448};  // the matrix each class is timed on
 struct LowpTune {
     std::mutex mu;
-    int choice[kTuneClasses] = {-1, -1, -1, -1};  // -1 untuned, 1 tcgen05, 0 mma.sync TF32
-    float ms[kTuneClasses][2] = {};                // time of one purification (mma.sync, tcgen05)
+    int choice[kTuneClasses] = {-1, -1, -1, -1};  // -1 untuned, else the lowp_tc_for kind
+    float ms[kTuneClasses][3] = {};                // time of one purification with kind 0, 1, 2
 };
 LowpTune g_lowp_tune[64];
 
@@ -451,13 +455,13 @@ int lowp_tc_env() {
     return v;
 }
 
-bool lowp_tc_for(int n) {
+int lowp_tc_for(int n) {
     const int env = lowp_tc_env();
-    if (env >= 0) return env != 0;
+    if (env >= 0) return env <= 2 ? env : 1;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
     const int c = g_lowp_tune[dev].choice[tune_class(n)];
-    return c != 0;  // untuned classes (the tuner could not run) take tcgen05
+    return c >= 0 ? c : 1;  // untuned classes (the tuner could not run) take the FP32-accurate tcgen05 kernel
 }
 
 int density_mode() {
@@ -682,6 +686,7 @@ struct Batch {
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
     TmaDesc* d_sp2_maps;    // tensor maps of every pair-copy job's X0, X1, F, P (4 per job)
     bool sp2_tma = false;   // the pair-copy tiles run k_sp2_step_tma and k_commutator_tma (every map encoded)
+    bool has_tc3 = false, has_tc1 = false;  // some job's reduced-precision products run k_sp2_step_tc / _tc1
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
     GemmTile* d_tc_tiles = nullptr;  // 128 x 128 upper-triangle tiles of the tcgen05 reduced-precision step
     int nt_tc = 0;
@@ -758,7 +763,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         tiles_nn += p.nch * tn * tn;
         tiles_up += p.nch * tn * (tn + 1) / 2;
         const int tc = (p.nao + 127) / 128;
-        if (mixed && lowp_tc_for(p.nao)) tiles_tc += p.nch * tc * (tc + 1) / 2;
+        if (mixed && lowp_tc_for(p.nao) != 0) tiles_tc += p.nch * tc * (tc + 1) / 2;
         if (fp64_oz_for(p.nao)) {
             tiles_oz += p.nch * oz_tiles_of(p.nao);
             dq_bytes += p.nch * (2LL * kOzPlanes * p.nao * oz_ldq(p.nao) + 256);
@@ -1036,7 +1041,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.ldf = (int)((n + 3) & ~3LL);  // FP32 iterates of the mixed path: in the VS slot, 16-byte aligned
             sj.Xf0 = (float*)(((uintptr_t)(base + SLOT_VS * nn) + 15) & ~(uintptr_t)15);
             sj.Xf1 = sj.Xf0 + n * sj.ldf;
-            sj.lowp_tc = (mixed && lowp_tc_for((int)n)) ? 1 : 0;
+            sj.lowp_tc = mixed ? lowp_tc_for((int)n) : 0;
+            if (sj.lowp_tc == 1) b.has_tc3 = true;
+            if (sj.lowp_tc == 2) b.has_tc1 = true;
             sj.tc_tile0 = ntc;
             if (sj.lowp_tc) {
                 const int tc = (int)((n + 127) / 128);
@@ -1478,8 +1485,12 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
             k_sp2_step_tf32<<<nt, 128, tf32_smem_bytes(), s>>>(b.d_sp2, t, nt, b.d_sp2_state);
             ++nl;
         });
-        if (b.nt_tc > 0) {
+        if (b.nt_tc > 0 && b.has_tc3) {
             k_sp2_step_tc<<<b.nt_tc, 128, tc_smem_bytes(), s>>>(b.d_sp2, b.d_tc_tiles, b.nt_tc, b.d_sp2_state, b.d_sp2_active + 2);
+            ++nl;
+        }
+        if (b.nt_tc > 0 && b.has_tc1) {
+            k_sp2_step_tc1<<<b.nt_tc, 128, tc1_smem_bytes(), s>>>(b.d_sp2, b.d_tc_tiles, b.nt_tc, b.d_sp2_state, b.d_sp2_active + 2);
             ++nl;
         }
     }
@@ -1998,9 +2009,11 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
 
 // The autotuner of the reduced-precision purification kernel: for each size class not yet tuned on
 // this device, one AM1-like matrix of the class's size (spectrum in [-40, -12] eV occupied and
-// [1, 10] eV virtual, the same matrix for both) is purified with each kernel after a warm-up, and
-// the faster one is kept for the process (both reach the same FP32-level density; the tcgen05 one
-// is the more accurate).  Runs in its own device pool, before the batch is laid out.
+// [1, 10] eV virtual, the same matrix for all) is purified with each of the three kernels after a
+// warm-up, and the fastest is kept for the process.  The mma.sync and single-pass tcgen05 kernels
+// work at TF32 precision, the 3xTF32 one at FP32 accuracy; every one of them only starts the FP64
+// iterations, which take the SCF to convergence.  Runs in its own device pool, before the batch is
+// laid out.
 int tune_lowp_kernels(const std::vector<MolPlan>& plans) {
     if (lowp_tc_env() >= 0) return AM1GPU_OK;
     int dev = 0;
@@ -2023,20 +2036,24 @@ int tune_lowp_kernels(const std::vector<MolPlan>& plans) {
                 f[(size_t)i * n + j] = f[(size_t)j * n + i] = v;
             }
         }
-        float best[2] = {0.f, 0.f};
+        float best[3] = {0.f, 0.f, 0.f};
         bool ok = true;
-        for (int prec : {2, 1}) {  // 2: mma.sync TF32, 1: tcgen05
+        // kind 0: mma.sync TF32 (precision 2), 1: tcgen05 3xTF32 (precision 1), 2: tcgen05 TF32 (precision 4)
+        const int prec_of[3] = {2, 1, 4};
+        for (int kind = 0; kind < 3; ++kind) {
             for (int rep = 0; rep < 3 && ok; ++rep) {
                 const auto t0 = std::chrono::steady_clock::now();
                 int steps = 0;
-                if (density_purify_one(n, f.data(), nocc, 2.0, prec, p.data(), &steps, &tl_mem_eig)) ok = false;
+                if (density_purify_one(n, f.data(), nocc, 2.0, prec_of[kind], p.data(), &steps, &tl_mem_eig)) ok = false;
                 const float ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
-                if (rep > 0) best[prec == 1] = rep == 1 ? ms : std::min(best[prec == 1], ms);
+                if (rep > 0) best[kind] = rep == 1 ? ms : std::min(best[kind], ms);
             }
         }
-        t.ms[c][0] = best[0];
-        t.ms[c][1] = best[1];
-        t.choice[c] = ok ? (best[1] <= best[0] ? 1 : 0) : 1;
+        int pick = 0;
+        for (int kind = 1; kind < 3; ++kind)
+            if (best[kind] < best[pick]) pick = kind;
+        for (int kind = 0; kind < 3; ++kind) t.ms[c][kind] = best[kind];
+        t.choice[c] = ok ? pick : 1;
     }
     g_err = saved;
     return AM1GPU_OK;
@@ -2494,14 +2511,15 @@ int big_fallback(Batch& b, Mem* ws) {
 // Density of one symmetric matrix F by purification, P = w * (projector onto its nocc lowest
 // eigenvectors): the step an SCF iteration takes after the extrapolation (the reference's
 // symmetric_eigen + density_from_coeff, src/scf.rs:654-661, 503-524), alone, at the precision of
-// the batched path's products: 0 FP64 tensor cores (k_sp2_step16/8), 1 FP32-accurate products on
-// tcgen05 (k_sp2_step_tc, 3xTF32), 2 TF32 mma.sync (k_sp2_step_tf32).  The reduced-precision runs
+// the batched path's products: 0 FP64 tensor cores (k_sp2_step_tma/16/8), 1 FP32-accurate products on
+// tcgen05 (k_sp2_step_tc, 3xTF32), 2 TF32 mma.sync (k_sp2_step_tf32), 3 FP64 from digit planes
+// (k_sp2_step_oz), 4 TF32 on tcgen05 in one pass (k_sp2_step_tc1).  The reduced-precision runs
 // stop at their own rounding floor and are rescaled to the exact trace, as in the mixed SCF.
 int density_purify_one(int n, const double* F, double nocc, double weight, int precision, double* P, int* steps_out,
                        Mem* mem_override = nullptr) {
     g_err.clear();
     if (n < 1 || n > 448 || !F || !P) return fail(AM1GPU_INVALID_INPUT, "n must be 1..448 and the pointers non-null");
-    if (precision < 0 || precision > 3) return fail(AM1GPU_INVALID_INPUT, "precision must be 0, 1, 2 or 3");
+    if (precision < 0 || precision > 4) return fail(AM1GPU_INVALID_INPUT, "precision must be 0, 1, 2, 3 or 4");
     if (!(nocc >= 0.0 && nocc <= n)) return fail(AM1GPU_INVALID_INPUT, "nocc outside 0..n");
     for (long long i = 0; i < (long long)n * n; ++i)
         if (!std::isfinite(F[i])) return fail(AM1GPU_LINALG, "the matrix is not finite");
@@ -2559,9 +2577,9 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     jb.ldf = ldf;
     jb.Xf0 = (float*)(((uintptr_t)(D + o_xf) + 15) & ~(uintptr_t)15);
     jb.Xf1 = jb.Xf0 + (size_t)n * ldf;
-    jb.lowp_tc = precision == 1 ? 1 : 0;
+    jb.lowp_tc = precision == 1 ? 1 : precision == 4 ? 2 : 0;
     jb.tc_tile0 = 0;
-    jb.tc_ntiles = precision == 1 ? nt128 : 0;
+    jb.tc_ntiles = (precision == 1 || precision == 4) ? nt128 : 0;
     jb.oz = precision == 3 ? 1 : 0;
     jb.oz_tile0 = 0;
     jb.oz_ntiles = precision == 3 ? ntoz : 0;
@@ -2586,7 +2604,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         for (int y = x; y < t128; ++y) h128[k++] = GemmTile{0, x, y};
     MolState ms{};
     ms.active = 1;
-    ms.lowp = (precision == 1 || precision == 2) ? 1 : 0;
+    ms.lowp = (precision == 1 || precision == 2 || precision == 4) ? 1 : 0;
     std::memcpy(H + o_ms, &ms, sizeof ms);
     double* hf = (double*)(H + o_f);
     double* hmin = (double*)(H + o_rmin);
@@ -2630,6 +2648,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
             k_sp2_step_oz<<<ntoz, 128, oz_smem_bytes(), s>>>(dj, (const GemmTile*)(D + o_toz), ntoz, dsst, dact + 2);
         } else if (precision == 2) {
             k_sp2_step_tf32<<<nt64, 128, tf32_smem_bytes(), s>>>(dj, d64, nt64, dsst);
+        } else if (precision == 4) {
+            k_sp2_step_tc1<<<nt128, 128, tc1_smem_bytes(), s>>>(dj, d128, nt128, dsst, dact + 2);
         } else {
             k_sp2_step_tc<<<nt128, 128, tc_smem_bytes(), s>>>(dj, d128, nt128, dsst, dact + 2);
         }
@@ -3107,10 +3127,8 @@ int am1gpu_lowp_tuning(int32_t* choice, float* ms) {
     std::lock_guard<std::mutex> lock(t.mu);
     for (int c = 0; c < am1::kTuneClasses; ++c) {
         if (choice) choice[c] = t.choice[c];
-        if (ms) {
-            ms[2 * c] = t.ms[c][0];
-            ms[2 * c + 1] = t.ms[c][1];
-        }
+        if (ms)
+            for (int k = 0; k < 3; ++k) ms[3 * c + k] = t.ms[c][k];
     }
     return AM1GPU_OK;
 }

@@ -403,7 +403,7 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
             float* Xr = jb.Xf0 + (long long)r * jb.ldf;
             for (int c = lane; c < jb.ldf; c += 32) {
                 const float xf = c < n ? (float)(((c == r ? emax : 0.0) - Fr[c]) * inv) : 0.0f;
-                const float x = jb.lowp_tc ? xf : tf32_round(xf);
+                const float x = jb.lowp_tc == 1 ? xf : tf32_round(xf);  // 3xTF32 keeps the full FP32 iterate
                 Xr[c] = x;
                 if (c >= n) jb.Xf1[(long long)r * jb.ldf + c] = 0.0f;
                 fr += (double)x * x;

@@ -19,6 +19,10 @@
 //
 // Every mbarrier wait is bounded; a wait that runs out sets bit 8 of the job's error word, the CTA
 // waits (bounded) for its MMAs, frees its TMEM and returns without writing the tile.
+//
+// k_sp2_step_tc1 is the single-pass form for iterates held as TF32 values (Sp2Job::lowp_tc == 2, the
+// precision of the mma.sync TF32 kernel): no lo parts, one MMA per K = 8, every stored iterate rounded
+// to the nearest TF32 value; its stages are half the size, so two CTAs fit an SM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,6 +39,7 @@ constexpr int TC_BK = 32;                   // floats per k-stage: one 128-byte 
 constexpr int TC_STAGES = 3;
 constexpr int TC_OP_BYTES = TC_TILE * 128;  // one operand of one stage: 128 rows x 128 B
 constexpr int TC_STAGE_BYTES = 4 * TC_OP_BYTES;  // A, B, A_lo, B_lo
+constexpr int TC1_STAGE_BYTES = 2 * TC_OP_BYTES;  // A, B (single pass)
 constexpr int TC_THREADS = 128;
 constexpr int TC_OUT_LD = TC_TILE + 1;      // staged output tile row stride (floats)
 constexpr uint32_t TC_TMEM_COLS = 128;      // FP32 accumulator: 128 lanes x 128 columns
@@ -139,9 +144,15 @@ __device__ __forceinline__ void tc_split(unsigned char* stage) {
 }  // namespace
 
 size_t tc_smem_bytes() { return (size_t)TC_STAGES * TC_STAGE_BYTES + 1024; }
+size_t tc1_smem_bytes() { return (size_t)TC_STAGES * TC1_STAGE_BYTES + 1024; }
+static_assert(TC_STAGES * TC1_STAGE_BYTES >= TC_TILE * TC_OUT_LD * (int)sizeof(float), "the staged output tile fits the stages");
 
-__global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                               int ntiles, const Sp2State* __restrict__ sst, int* __restrict__ err) {
+// SPLIT: 3xTF32 from unrounded FP32 iterates (lowp_tc == 1); otherwise one TF32 pass over TF32
+// iterates (lowp_tc == 2)
+template <bool SPLIT>
+__device__ __forceinline__ void sp2_step_tc_body(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
+                                                 const Sp2State* __restrict__ sst, int* __restrict__ err) {
+    constexpr int STAGE_BYTES = SPLIT ? TC_STAGE_BYTES : TC1_STAGE_BYTES;
     extern __shared__ unsigned char tc_raw[];
     __shared__ __align__(8) uint64_t bars[TC_STAGES];
     __shared__ uint32_t tmem_slot;
@@ -152,7 +163,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
     const GemmTile tl = tiles[t];
     const Sp2State* sp = sst + tl.job;
     const Sp2Job* jp = jobs + tl.job;
-    if (!sp->active || !sp->lowp || !jp->lowp_tc) return;  // FP64 steps and mma.sync TF32 steps elsewhere
+    if (!sp->active || !sp->lowp || jp->lowp_tc != (SPLIT ? 1 : 2)) return;  // FP64, mma.sync TF32, other tcgen05 form elsewhere
     const int n = jp->n, ldf = jp->ldf;
     const int cur = sp->cur;
     const float* X = cur ? jp->Xf1 : jp->Xf0;
@@ -179,7 +190,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
     const uint32_t tmem = tmem_slot;
     const int KT = (n + TC_BK - 1) / TC_BK;
     for (int s = 0; s < TC_STAGES - 1 && s < KT; ++s) {
-        tc_load(sbase + s * TC_STAGE_BYTES, X, ldf, n, m0, n0, s);
+        tc_load(sbase + s * STAGE_BYTES, X, ldf, n, m0, n0, s);
         asm volatile("cp.async.commit_group;\n");
     }
     uint32_t phase_bits = 0;  // parity of the next completion of each stage's barrier
@@ -189,18 +200,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
         // stage st holds k-stage kt once this thread's copies of it have landed
         if (kt + 1 < KT) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        tc_split(base + st * TC_STAGE_BYTES);
+        if constexpr (SPLIT) tc_split(base + st * STAGE_BYTES);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (tid == 0) {
-            const uint32_t a = sbase + st * TC_STAGE_BYTES, b = a + TC_OP_BYTES, alo = a + 2 * TC_OP_BYTES, blo = a + 3 * TC_OP_BYTES;
+            const uint32_t a = sbase + st * STAGE_BYTES, b = a + TC_OP_BYTES, alo = a + 2 * TC_OP_BYTES, blo = a + 3 * TC_OP_BYTES;
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 8; ++kk) {  // K = 8 per MMA: 32 bytes along the swizzled row
                 const uint32_t o = 32u * kk;
                 tc_mma(tmem, tc_desc(a + o), tc_desc(b + o), (kt > 0 || kk > 0) ? 1u : 0u);
-                tc_mma(tmem, tc_desc(a + o), tc_desc(blo + o), 1u);
-                tc_mma(tmem, tc_desc(alo + o), tc_desc(b + o), 1u);
+                if constexpr (SPLIT) {
+                    tc_mma(tmem, tc_desc(a + o), tc_desc(blo + o), 1u);
+                    tc_mma(tmem, tc_desc(alo + o), tc_desc(b + o), 1u);
+                }
             }
             tc_commit(smem_addr(&bars[st]));
         }
@@ -212,7 +225,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
                 if (!mbar_wait(smem_addr(&bars[ns]), (phase_bits >> ns) & 1u)) ok = false;
                 phase_bits ^= 1u << ns;
             }
-            tc_load(sbase + ns * TC_STAGE_BYTES, X, ldf, n, m0, n0, nk);
+            tc_load(sbase + ns * STAGE_BYTES, X, ldf, n, m0, n0, nk);
         }
         asm volatile("cp.async.commit_group;\n");
         if (__syncthreads_or(!ok)) {  // every thread leaves together (the barrier at the top of the loop)
@@ -272,7 +285,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
             sj = i;
         }
         const float x2 = out[si * TC_OUT_LD + sj];
-        const float y = square ? x2 : 2.0f * X[(long long)(m0 + si) * ldf + (n0 + sj)] - x2;
+        const float y0 = square ? x2 : 2.0f * X[(long long)(m0 + si) * ldf + (n0 + sj)] - x2;
+        const float y = SPLIT ? y0 : tf32_round(y0);
         Y[(long long)r * ldf + c] = y;
         if (diag) {
             fr += (double)y * y;
@@ -287,8 +301,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
             const int r = m0 + i, c = n0 + j;
             if (r >= n || c >= n) continue;
             const float x2 = out[i * TC_OUT_LD + j];
-            const float y = square ? x2 : 2.0f * X[(long long)r * ldf + c] - x2;
-            Y[(long long)c * ldf + r] = y;
+            const float y0 = square ? x2 : 2.0f * X[(long long)r * ldf + c] - x2;
+            Y[(long long)c * ldf + r] = SPLIT ? y0 : tf32_round(y0);
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -305,6 +319,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
         p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
         p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
     }
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                               int ntiles, const Sp2State* __restrict__ sst, int* __restrict__ err) {
+    sp2_step_tc_body<true>(jobs, tiles, ntiles, sst, err);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 2) k_sp2_step_tc1(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
+                                                                int ntiles, const Sp2State* __restrict__ sst, int* __restrict__ err) {
+    sp2_step_tc_body<false>(jobs, tiles, ntiles, sst, err);
 }
 
 }  // namespace am1

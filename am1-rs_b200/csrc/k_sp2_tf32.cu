@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(TF_THREADS, 4) k_sp2_step_tf32(const Sp2Job* _
     const GemmTile tl = tiles[t];
     const Sp2State* sp = sst + tl.job;
     const Sp2Job* jp = jobs + tl.job;
-    if (!sp->active || !sp->lowp || jp->lowp_tc) return;  // FP64 runs: k_sp2_step16 / k_sp2_step8; tcgen05: k_sp2_step_tc
+    if (!sp->active || !sp->lowp || jp->lowp_tc) return;  // FP64 runs: k_sp2_step_tma / 16 / 8; tcgen05: k_sp2_step_tc / _tc1
     const int n = jp->n, ldf = jp->ldf;
     const int cur = sp->cur;
     const float* X = cur ? jp->Xf1 : jp->Xf0;

@@ -87,9 +87,10 @@ struct Sp2Job {
     float* Xf0;
     float* Xf1;
     int ldf;
-    // 1: the reduced-precision products run on tcgen05 at FP32 accuracy (k_sp2_step_tc, 128 x 128
-    // tiles tc_tile0 .. tc_tile0 + tc_ntiles - 1 of their launch, FP32 iterates); 0: mma.sync TF32
-    // (k_sp2_step_tf32, TF32-rounded iterates)
+    // the reduced-precision products: 1 on tcgen05 at FP32 accuracy (k_sp2_step_tc, 3xTF32, FP32
+    // iterates), 2 on tcgen05 in one TF32 pass (k_sp2_step_tc1, TF32-rounded iterates), both on the
+    // 128 x 128 tiles tc_tile0 .. tc_tile0 + tc_ntiles - 1 of their launch; 0 mma.sync TF32
+    // (k_sp2_step_tf32, TF32-rounded iterates, the 64 x 64 tiles)
     int lowp_tc, tc_tile0, tc_ntiles;
     // 1: the FP64 products run on tcgen05's integer path from the iterate's 7-bit digit planes
     // (k_sp2_step_oz, 128 x 48 tiles oz_tile0 .. oz_tile0 + oz_ntiles - 1 of their launch); the digits of
@@ -197,6 +198,7 @@ __global__ void k_commutator_tma(const ChanJob* jobs, const GemmTile* tiles, int
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
 size_t tc_smem_bytes();
+size_t tc1_smem_bytes();
 size_t oz_smem_bytes();
 __global__ void k_sp2_step_oz(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
 // The eight 7-bit digits of y (|y| < 2) packed one per byte, digit i in byte i: d_i = rint(r_i 2^(5+7i)),
@@ -222,6 +224,7 @@ __device__ __forceinline__ void oz_digits_of(double y, int8_t* __restrict__ D, l
     oz_store_digits(oz_digits_packed(y), D, plane, o);
 }
 __global__ void k_sp2_step_tc(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
+__global__ void k_sp2_step_tc1(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
                              int* big_stall, int* big_count);
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each

@@ -505,6 +505,7 @@ def run_ours(args):
                       "scf_iterations_mean": float(np.mean([r["iterations"] for r in res_m])),
                       "max_abs_dHf_kcal_vs_fp64": dhf_m64, "max_abs_dq_vs_fp64": dq_m64,
                       "max_abs_dHf_kcal_vs_oracle": dhf_m, "batched_over_plain": world * nmol * args.steps / mixed_s / world / plain_rate,
+                      "lowp_kernels": {c: v["kernel"] for c, v in native.lowp_tuning().items()},
                       "tf32_products_per_step": sum(s["lowp_purification_steps"] for s in mixed_stats) / args.steps,
                       "fp64_products_per_step": sum(s["purification_steps"] for s in mixed_stats) / args.steps},
             "gradient": {"value": world * nmol / grad_s, "unit": "SCF + gradient solves/s",

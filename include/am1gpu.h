@@ -256,7 +256,8 @@ int am1gpu_symmetric_eigenvalues(int32_t n, const double* a, double* w);
  * (src/scf.rs:654-661, 503-524), alone.  precision: 0 FP64 tensor cores (the products of the FP64
  * SCF), 1 FP32-accurate products on the fifth-generation tensor cores (tcgen05, TF32 operands split
  * in two, as the mixed path's early iterations use), 2 TF32 products on mma.sync, 3 FP64 products on
- * tcgen05's integer path from 7-bit digit planes of the iterate (AM1GPU_FP64_DIGITS).  The reduced-
+ * tcgen05's integer path from 7-bit digit planes of the iterate (AM1GPU_FP64_DIGITS), 4 TF32 products
+ * on tcgen05 in one pass over TF32-rounded iterates.  The reduced-
  * precision runs stop at their own rounding floor and are rescaled to trace n_occ.  *steps (may be
  * NULL) receives the number of products.  A matrix whose gap is too small to purify in 100 steps
  * returns AM1GPU_LINALG.
@@ -266,10 +267,10 @@ int am1gpu_density_purify(int32_t n, const double* f, double n_occ, double weigh
 
 /*
  * The autotuner's table for the current device: which kernel the mixed path's reduced-precision
- * purification products use per size class (n <= 128, <= 256, <= 384, larger): choice[c] = 1
- * tcgen05 (FP32-accurate), 0 mma.sync TF32, -1 not tuned yet; ms[2c], ms[2c+1] the time of one
- * purification of the class's test matrix with each (mma.sync, tcgen05).  Either pointer may be
- * NULL.  No counterpart in the reference.
+ * purification products use per size class (n <= 128, <= 256, <= 384, larger): choice[c] = 0
+ * mma.sync TF32, 1 tcgen05 at FP32 accuracy (3xTF32), 2 tcgen05 in one TF32 pass, -1 not tuned
+ * yet; ms[3c + k] (12 floats) the time of one purification of the class's test matrix with kernel
+ * k.  Either pointer may be NULL.  No counterpart in the reference.
  */
 int am1gpu_lowp_tuning(int32_t* choice, float* ms);
 

@@ -52,6 +52,52 @@ def test_mixed_matches_fp64_and_oracle(gpu, oracle, method):
         assert abs(rmx[i]["heat_of_formation_kcal"] - o["heat_of_formation_kcal"]) < DHF_BAR
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_mixed_with_each_reduced_precision_kernel(tmp_path, kernel):
+    # AM1GPU_LOWP_TC forces the kernel of the TF32 phase (0 mma.sync TF32, 1 tcgen05 3xTF32, 2 tcgen05
+    # in one TF32 pass) instead of the autotuner's choice; every one must give the FP64 results
+    import subprocess
+    import sys
+    import textwrap
+
+    from conftest import ROOT
+
+    script = textwrap.dedent(f"""
+        import sys
+        sys.path[:0] = [{str(ROOT / 'am1-rs_b200')!r}, {str(ROOT / 'tests')!r}]
+        import numpy as np
+        from am1gpu import native
+        from test_gpu_mixed import _mols, DHF_BAR, Q_TOL
+        mols = _mols(43)
+        s64, r64 = native.scf_batch(mols, want_matrices=True)
+        smx, rmx = native.scf_batch(mols, want_matrices=True, precision="mixed")
+        st = native.last_call_stats()
+        assert st["lowp_purification_steps"] > 0, st
+        assert all(x == 0 for x in s64) and all(x == 0 for x in smx), (s64, smx)
+        for a, b in zip(r64, rmx):
+            assert abs(a["heat_of_formation_kcal"] - b["heat_of_formation_kcal"]) < DHF_BAR
+            assert np.max(np.abs(a["charges"] - b["charges"])) < Q_TOL
+            assert np.max(np.abs(a["density"] - b["density"])) < Q_TOL
+        print("ok")
+    """)
+    f = tmp_path / "lowp.py"
+    f.write_text(script)
+    env = dict(__import__("os").environ, AM1GPU_LOWP_TC=str(kernel))
+    r = subprocess.run([sys.executable, str(f)], env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+def test_autotuner_reports_three_kernels(gpu):
+    gpu.scf_batch(_mols(5)[:4], precision="mixed")
+    tab = gpu.lowp_tuning()
+    tuned = [v for v in tab.values() if v["kernel"] is not None]
+    assert tuned
+    for v in tuned:
+        assert v["kernel"] in gpu.LOWP_KERNELS
+        assert all(t > 0.0 for t in v["ms"].values())
+        assert v["ms"][v["kernel"]] == min(v["ms"].values())
+
+
 def test_mixed_large_molecule(gpu):
     # 540 orbitals: TF32 purification on the large-matrix path too
     from am1gpu import workloads as W, _abi
