@@ -438,6 +438,20 @@ bool encode_square_map(TmaDesc* out, const double* base, int n) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The tensor map k_sp2_step_tc1 reads an FP32 iterate through: n rows of ldf floats (ldf a multiple
+// of 4, so the row pitch is a multiple of 16 bytes), boxes of 32 floats (128 bytes) x 128 rows,
+// 128-byte swizzle, zero fill past the edges.
+bool encode_rows_map_f32(TmaDesc* out, const float* base, int ldf, int n) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+    if (!enc || n < 1 || ldf % 4 != 0 || !aligned16(base)) return false;
+    const cuuint64_t dim[2] = {(cuuint64_t)ldf, (cuuint64_t)n};
+    const cuuint64_t pitch[1] = {(cuuint64_t)ldf * sizeof(float)};
+    const cuuint32_t box[2] = {32, 128}, es[2] = {1, 1};
+    return enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dim, pitch, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 inline int oz_ldq(int n) { return (n + 15) & ~15; }
 inline int oz_tiles_of(int n) {  // 128 x 48 tiles with an element on or above the diagonal
     int k = 0;
@@ -457,7 +471,7 @@ int lowp_tc_env() {
 
 int lowp_tc_for(int n) {
     const int env = lowp_tc_env();
-    if (env >= 0) return env <= 2 ? env : 1;
+    if (env >= 0) return env == 0 ? 0 : (env == 2 && tma_encoder()) ? 2 : 1;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
     const int c = g_lowp_tune[dev].choice[tune_class(n)];
@@ -685,6 +699,7 @@ struct Batch {
     Sp2Job* d_sp2;
     GemmTile* d_sp2_tiles;  // upper-triangle tiles: the pair-copy jobs' first, then the others
     TmaDesc* d_sp2_maps;    // tensor maps of every pair-copy job's X0, X1, F, P (4 per job)
+    TmaDesc* d_xf_maps;     // tensor maps of the FP32 iterates Xf0, Xf1 of every single-pass tcgen05 job (2 per job)
     bool sp2_tma = false;   // the pair-copy tiles run k_sp2_step_tma and k_commutator_tma (every map encoded)
     bool has_tc3 = false, has_tc1 = false;  // some job's reduced-precision products run k_sp2_step_tc / _tc1
     int nt_sp2 = 0, nt_sp2_pairs = 0, sp2_nblk = 1;
@@ -793,6 +808,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_sp2 = take(st, sizeof(Sp2Job) * nch_total);
     const size_t o_sp2t = take(st, sizeof(GemmTile) * std::max(tiles_up, 1));
     const size_t o_maps = take(st, sizeof(TmaDesc) * 4 * std::max<long long>(nch_total, 1));
+    const size_t o_xfmaps = take(st, mixed ? sizeof(TmaDesc) * 2 * std::max<long long>(nch_total, 1) : sizeof(TmaDesc) * 2);
     const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
     const size_t o_ozt = take(st, sizeof(GemmTile) * std::max(tiles_oz, 1));
     const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
@@ -864,6 +880,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     b.d_sp2_maps = (TmaDesc*)dptr(o_maps);
     TmaDesc* hmaps = (TmaDesc*)(Hs + o_maps);
     b.sp2_tma = tma_encoder() != nullptr;
+    b.d_xf_maps = (TmaDesc*)dptr(o_xfmaps);
+    TmaDesc* hxfmaps = (TmaDesc*)(Hs + o_xfmaps);
     b.d_tc_tiles = (GemmTile*)dptr(o_tct);
     GemmTile* htct = (GemmTile*)(Hs + o_tct);
     int ntc = 0;
@@ -1042,6 +1060,9 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.Xf0 = (float*)(((uintptr_t)(base + SLOT_VS * nn) + 15) & ~(uintptr_t)15);
             sj.Xf1 = sj.Xf0 + n * sj.ldf;
             sj.lowp_tc = mixed ? lowp_tc_for((int)n) : 0;
+            if (sj.lowp_tc == 2 && !(encode_rows_map_f32(&hxfmaps[2 * job], sj.Xf0, sj.ldf, (int)n) &&
+                                     encode_rows_map_f32(&hxfmaps[2 * job + 1], sj.Xf1, sj.ldf, (int)n)))
+                sj.lowp_tc = 1;  // no tensor maps: the 3xTF32 kernel
             if (sj.lowp_tc == 1) b.has_tc3 = true;
             if (sj.lowp_tc == 2) b.has_tc1 = true;
             sj.tc_tile0 = ntc;
@@ -1490,7 +1511,8 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
             ++nl;
         }
         if (b.nt_tc > 0 && b.has_tc1) {
-            k_sp2_step_tc1<<<b.nt_tc, 128, tc1_smem_bytes(), s>>>(b.d_sp2, b.d_tc_tiles, b.nt_tc, b.d_sp2_state, b.d_sp2_active + 2);
+            k_sp2_step_tc1<<<b.nt_tc, 128, tc1_smem_bytes(), s>>>(b.d_sp2, b.d_tc_tiles, b.nt_tc, b.d_sp2_state, b.d_xf_maps,
+                                                                  b.d_sp2_active + 2);
             ++nl;
         }
     }
@@ -2037,23 +2059,23 @@ int tune_lowp_kernels(const std::vector<MolPlan>& plans) {
             }
         }
         float best[3] = {0.f, 0.f, 0.f};
-        bool ok = true;
+        bool ok[3] = {true, true, tma_encoder() != nullptr};
         // kind 0: mma.sync TF32 (precision 2), 1: tcgen05 3xTF32 (precision 1), 2: tcgen05 TF32 (precision 4)
         const int prec_of[3] = {2, 1, 4};
         for (int kind = 0; kind < 3; ++kind) {
-            for (int rep = 0; rep < 3 && ok; ++rep) {
+            for (int rep = 0; rep < 3 && ok[kind]; ++rep) {
                 const auto t0 = std::chrono::steady_clock::now();
                 int steps = 0;
-                if (density_purify_one(n, f.data(), nocc, 2.0, prec_of[kind], p.data(), &steps, &tl_mem_eig)) ok = false;
+                if (density_purify_one(n, f.data(), nocc, 2.0, prec_of[kind], p.data(), &steps, &tl_mem_eig)) ok[kind] = false;
                 const float ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
                 if (rep > 0) best[kind] = rep == 1 ? ms : std::min(best[kind], ms);
             }
         }
-        int pick = 0;
-        for (int kind = 1; kind < 3; ++kind)
-            if (best[kind] < best[pick]) pick = kind;
-        for (int kind = 0; kind < 3; ++kind) t.ms[c][kind] = best[kind];
-        t.choice[c] = ok ? pick : 1;
+        int pick = -1;
+        for (int kind = 0; kind < 3; ++kind)
+            if (ok[kind] && (pick < 0 || best[kind] < best[pick])) pick = kind;
+        for (int kind = 0; kind < 3; ++kind) t.ms[c][kind] = ok[kind] ? best[kind] : 0.f;
+        t.choice[c] = pick >= 0 ? pick : 1;
     }
     g_err = saved;
     return AM1GPU_OK;
@@ -2539,7 +2561,8 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         off += bytes;
         return o;
     };
-    const size_t o_job = take(sizeof(Sp2Job)), o_maps = take(4 * sizeof(TmaDesc)), o_t64 = take(sizeof(GemmTile) * nt64),
+    const size_t o_job = take(sizeof(Sp2Job)), o_maps = take(4 * sizeof(TmaDesc)), o_xfmaps = take(2 * sizeof(TmaDesc)),
+                 o_t64 = take(sizeof(GemmTile) * nt64),
                  o_t128 = take(sizeof(GemmTile) * nt128),
                  o_toz = take(sizeof(GemmTile) * ntoz),
                  o_ms = take(sizeof(MolState)), o_f = take(8 * nn), o_rmin = take(8 * (size_t)n), o_rmax = take(8 * (size_t)n);
@@ -2589,6 +2612,9 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
     std::memcpy(H + o_job, &jb, sizeof jb);
     TmaDesc* hmaps = (TmaDesc*)(H + o_maps);
     const bool tma = encode_square_map(&hmaps[0], jb.X0, n) && encode_square_map(&hmaps[1], jb.X1, n);
+    TmaDesc* hxfmaps = (TmaDesc*)(H + o_xfmaps);
+    if (precision == 4 && !(encode_rows_map_f32(&hxfmaps[0], jb.Xf0, ldf, n) && encode_rows_map_f32(&hxfmaps[1], jb.Xf1, ldf, n)))
+        return fail(AM1GPU_UNSUPPORTED, "no tensor-map encoder on this device: the single-pass tcgen05 products are not available");
     GemmTile* hoz = (GemmTile*)(H + o_toz);
     int koz = 0;
     for (int tm = 0; tm < t128; ++tm)
@@ -2649,7 +2675,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
         } else if (precision == 2) {
             k_sp2_step_tf32<<<nt64, 128, tf32_smem_bytes(), s>>>(dj, d64, nt64, dsst);
         } else if (precision == 4) {
-            k_sp2_step_tc1<<<nt128, 128, tc1_smem_bytes(), s>>>(dj, d128, nt128, dsst, dact + 2);
+            k_sp2_step_tc1<<<nt128, 128, tc1_smem_bytes(), s>>>(dj, d128, nt128, dsst, (const TmaDesc*)(D + o_xfmaps), dact + 2);
         } else {
             k_sp2_step_tc<<<nt128, 128, tc_smem_bytes(), s>>>(dj, d128, nt128, dsst, dact + 2);
         }

@@ -22,7 +22,8 @@
 //
 // k_sp2_step_tc1 is the single-pass form for iterates held as TF32 values (Sp2Job::lowp_tc == 2, the
 // precision of the mma.sync TF32 kernel): no lo parts, one MMA per K = 8, every stored iterate rounded
-// to the nearest TF32 value; its stages are half the size, so two CTAs fit an SM.
+// to the nearest TF32 value, the operands copied by TMA from tensor maps of the FP32 iterates; its
+// stages are half the size, so two CTAs fit an SM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -147,8 +148,95 @@ size_t tc_smem_bytes() { return (size_t)TC_STAGES * TC_STAGE_BYTES + 1024; }
 size_t tc1_smem_bytes() { return (size_t)TC_STAGES * TC1_STAGE_BYTES + 1024; }
 static_assert(TC_STAGES * TC1_STAGE_BYTES >= TC_TILE * TC_OUT_LD * (int)sizeof(float), "the staged output tile fits the stages");
 
-// SPLIT: 3xTF32 from unrounded FP32 iterates (lowp_tc == 1); otherwise one TF32 pass over TF32
-// iterates (lowp_tc == 2)
+// The tile after its MMAs (every thread; `good`: the k-loop finished): the accumulator out of TMEM
+// into the free stages, TMEM freed, then Y = X^2 or 2X - X^2 written along rows (the direct block)
+// and along the mirrored rows, with the tile's share of tr Y and ||Y||_F^2.  ROUND: every stored
+// value rounded to the nearest TF32 value.
+template <bool ROUND>
+__device__ __forceinline__ void tc_epilogue(const Sp2Job* __restrict__ jp, const Sp2State* __restrict__ sp, int t, const float* X, float* Y,
+                                            int n, int ldf, int m0, int n0, bool diag, uint32_t tmem, unsigned char* base, bool good,
+                                            int* __restrict__ err, double (&red)[2][4]) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float* out = reinterpret_cast<float*>(base);  // the stages are free: the tile of X.X, row stride TC_OUT_LD
+    if (good) {
+        const int r = warp * 32 + lane;  // the tile row this thread reads from TMEM lane r
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_TILE; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+                  "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+                  "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+                  "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; ++j) out[r * TC_OUT_LD + c0 + j] = __uint_as_float(v[j]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    if (!good) {
+        if (tid == 0) atomicOr(err, 1 << 8);
+        return;
+    }
+    // Y = X^2 or 2X - X^2, written along rows (the direct block) and along the mirrored rows; on a
+    // diagonal tile element (i, j) takes the value of (min, max), so Y is exactly symmetric
+    const int square = sp->square;
+    double tr = 0.0, fr = 0.0;
+    for (int idx = tid; idx < TC_TILE * TC_TILE; idx += TC_THREADS) {
+        const int i = idx / TC_TILE, j = idx % TC_TILE;  // consecutive threads: consecutive columns
+        const int r = m0 + i, c = n0 + j;
+        if (r >= n || c >= n) continue;
+        int si = i, sj = j;
+        if (diag && i > j) {
+            si = j;
+            sj = i;
+        }
+        const float x2 = out[si * TC_OUT_LD + sj];
+        const float y0 = square ? x2 : 2.0f * X[(long long)(m0 + si) * ldf + (n0 + sj)] - x2;
+        const float y = ROUND ? tf32_round(y0) : y0;
+        Y[(long long)r * ldf + c] = y;
+        if (diag) {
+            fr += (double)y * y;
+            if (i == j) tr += y;
+        } else {
+            fr += 2.0 * (double)y * y;
+        }
+    }
+    if (!diag) {
+        for (int idx = tid; idx < TC_TILE * TC_TILE; idx += TC_THREADS) {
+            const int j = idx / TC_TILE, i = idx % TC_TILE;  // consecutive threads: consecutive tile rows
+            const int r = m0 + i, c = n0 + j;
+            if (r >= n || c >= n) continue;
+            const float x2 = out[i * TC_OUT_LD + j];
+            const float y0 = square ? x2 : 2.0f * X[(long long)r * ldf + c] - x2;
+            Y[(long long)c * ldf + r] = ROUND ? tf32_round(y0) : y0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_xor_sync(0xffffffffu, tr, o);
+        fr += __shfl_xor_sync(0xffffffffu, fr, o);
+    }
+    if (lane == 0) {
+        red[0][warp] = tr;
+        red[1][warp] = fr;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double* p = jp->part + 2 * (t - jp->tc_tile0);
+        p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
+        p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
+    }
+}
+
+
+// The cp.async-fed k-loop: SPLIT, 3xTF32 from unrounded FP32 iterates (k_sp2_step_tc, lowp_tc == 1);
+// otherwise one TF32 pass over TF32 iterates (lowp_tc == 2; k_sp2_step_tc1 feeds that one by TMA)
 template <bool SPLIT>
 __device__ __forceinline__ void sp2_step_tc_body(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
                                                  const Sp2State* __restrict__ sst, int* __restrict__ err) {
@@ -170,7 +258,7 @@ __device__ __forceinline__ void sp2_step_tc_body(const Sp2Job* __restrict__ jobs
     float* Y = cur ? jp->Xf0 : jp->Xf1;
     const int m0 = tl.tm * TC_TILE, n0 = tl.tn * TC_TILE;
     const bool diag = tl.tm == tl.tn;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
     // 1024-byte aligned stages (the swizzle atom)
     unsigned char* base = tc_raw + ((1024u - (smem_addr(tc_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_addr(base);
@@ -243,82 +331,7 @@ __device__ __forceinline__ void sp2_step_tc_body(const Sp2Job* __restrict__ jobs
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const bool good = fail == 0;
-    float* out = reinterpret_cast<float*>(base);  // the stages are free: the tile of X.X, row stride TC_OUT_LD
-    if (good) {
-        const int r = warp * 32 + lane;  // the tile row this thread reads from TMEM lane r
-#pragma unroll 1
-        for (int c0 = 0; c0 < TC_TILE; c0 += 32) {
-            uint32_t v[32];
-            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-                  "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
-                  "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-                  "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(addr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-            for (int j = 0; j < 32; ++j) out[r * TC_OUT_LD + c0 + j] = __uint_as_float(v[j]);
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_TMEM_COLS));
-    if (!good) {
-        if (tid == 0) atomicOr(err, 1 << 8);
-        return;
-    }
-    // Y = X^2 or 2X - X^2, written along rows (the direct block) and along the mirrored rows; on a
-    // diagonal tile element (i, j) takes the value of (min, max), so Y is exactly symmetric
-    const int square = sp->square;
-    double tr = 0.0, fr = 0.0;
-    for (int idx = tid; idx < TC_TILE * TC_TILE; idx += TC_THREADS) {
-        const int i = idx / TC_TILE, j = idx % TC_TILE;  // consecutive threads: consecutive columns
-        const int r = m0 + i, c = n0 + j;
-        if (r >= n || c >= n) continue;
-        int si = i, sj = j;
-        if (diag && i > j) {
-            si = j;
-            sj = i;
-        }
-        const float x2 = out[si * TC_OUT_LD + sj];
-        const float y0 = square ? x2 : 2.0f * X[(long long)(m0 + si) * ldf + (n0 + sj)] - x2;
-        const float y = SPLIT ? y0 : tf32_round(y0);
-        Y[(long long)r * ldf + c] = y;
-        if (diag) {
-            fr += (double)y * y;
-            if (i == j) tr += y;
-        } else {
-            fr += 2.0 * (double)y * y;
-        }
-    }
-    if (!diag) {
-        for (int idx = tid; idx < TC_TILE * TC_TILE; idx += TC_THREADS) {
-            const int j = idx / TC_TILE, i = idx % TC_TILE;  // consecutive threads: consecutive tile rows
-            const int r = m0 + i, c = n0 + j;
-            if (r >= n || c >= n) continue;
-            const float x2 = out[i * TC_OUT_LD + j];
-            const float y0 = square ? x2 : 2.0f * X[(long long)r * ldf + c] - x2;
-            Y[(long long)c * ldf + r] = SPLIT ? y0 : tf32_round(y0);
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        tr += __shfl_xor_sync(0xffffffffu, tr, o);
-        fr += __shfl_xor_sync(0xffffffffu, fr, o);
-    }
-    if (lane == 0) {
-        red[0][warp] = tr;
-        red[1][warp] = fr;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double* p = jp->part + 2 * (t - jp->tc_tile0);
-        p[0] = red[0][0] + red[0][1] + red[0][2] + red[0][3];
-        p[1] = red[1][0] + red[1][1] + red[1][2] + red[1][3];
-    }
+    tc_epilogue<!SPLIT>(jp, sp, t, X, Y, n, ldf, m0, n0, diag, tmem, base, fail == 0, err, red);
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
@@ -326,9 +339,111 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_sp2_step_tc(const Sp2Job* __r
     sp2_step_tc_body<true>(jobs, tiles, ntiles, sst, err);
 }
 
+// Single pass with TMA-fed operands.  Thread 0 alone runs the k-loop: each k-stage of A and B is one
+// 32-float x 128-row box (cp.async.bulk.tensor, 128-byte swizzle: exactly the layout the UMMA
+// descriptors describe) counted on the stage's full mbarrier; after the MMAs of k-stage kt it
+// commits them to the stage's empty mbarrier and refills the stage k-stage kt - 1 used once that
+// one's MMAs are done, so copies and MMAs overlap with no CTA barrier in the loop.  A diagonal tile
+// loads one box per k-stage.  Every wait is bounded; a wait that runs out stops the loop, thread 0
+// lets its copies and MMAs still in flight finish (bounded), and the tile is not written.
 __global__ void __launch_bounds__(TC_THREADS, 2) k_sp2_step_tc1(const Sp2Job* __restrict__ jobs, const GemmTile* __restrict__ tiles,
-                                                                int ntiles, const Sp2State* __restrict__ sst, int* __restrict__ err) {
-    sp2_step_tc_body<false>(jobs, tiles, ntiles, sst, err);
+                                                                int ntiles, const Sp2State* __restrict__ sst,
+                                                                const TmaDesc* __restrict__ maps, int* __restrict__ err) {
+    extern __shared__ unsigned char tc_raw[];
+    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES];
+    __shared__ uint32_t tmem_slot;
+    __shared__ double red[2][4];
+    __shared__ int fail;
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const GemmTile tl = tiles[t];
+    const Sp2State* sp = sst + tl.job;
+    const Sp2Job* jp = jobs + tl.job;
+    if (!sp->active || !sp->lowp || jp->lowp_tc != 2) return;
+    const int n = jp->n, ldf = jp->ldf;
+    const int cur = sp->cur;
+    const float* X = cur ? jp->Xf1 : jp->Xf0;
+    float* Y = cur ? jp->Xf0 : jp->Xf1;
+    const int m0 = tl.tm * TC_TILE, n0 = tl.tn * TC_TILE;
+    const bool diag = tl.tm == tl.tn;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned char* base = tc_raw + ((1024u - (smem_addr(tc_raw) & 1023u)) & 1023u);
+    const uint32_t sbase = smem_addr(base);
+    if (tid == 0) {
+        fail = 0;
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(smem_addr(&full[s]), 1);
+            mbar_init(smem_addr(&empty[s]), 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const int KT = (n + TC_BK - 1) / TC_BK;
+    if (tid == 0) {
+        const void* map = maps + 2 * tl.job + cur;
+        const uint32_t tx = diag ? TC_OP_BYTES : 2 * TC_OP_BYTES;
+        auto load = [&](int kt) {
+            const int s = kt % TC_STAGES;
+            const uint32_t fb = smem_addr(&full[s]);
+            const uint32_t a = sbase + s * TC1_STAGE_BYTES;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(tx) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(a),
+                "l"(map), "r"(kt * TC_BK), "r"(m0), "r"(fb)
+                : "memory");
+            if (!diag)
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+                        a + TC_OP_BYTES),
+                    "l"(map), "r"(kt * TC_BK), "r"(n0), "r"(fb)
+                    : "memory");
+        };
+        int issued = 0, landed = 0, mma_last = -1;
+        for (; issued < TC_STAGES && issued < KT; ++issued) load(issued);
+        bool ok = true;
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % TC_STAGES;
+            if (!mbar_wait(smem_addr(&full[s]), (kt / TC_STAGES) & 1)) {
+                ok = false;
+                break;
+            }
+            landed = kt + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t a = sbase + s * TC1_STAGE_BYTES, b = diag ? a : a + TC_OP_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 8; ++kk) {
+                const uint32_t o = 32u * kk;
+                tc_mma(tmem, tc_desc(a + o), tc_desc(b + o), (kt > 0 || kk > 0) ? 1u : 0u);
+            }
+            tc_commit(smem_addr(&empty[s]));
+            mma_last = kt;
+            if (kt >= 1 && issued < KT) {  // issued == kt - 1 + TC_STAGES
+                const int kp = kt - 1;
+                if (!mbar_wait(smem_addr(&empty[kp % TC_STAGES]), (kp / TC_STAGES) & 1)) {
+                    ok = false;
+                    break;
+                }
+                load(issued++);
+            }
+        }
+        // every MMA is done once the commit of the last k-stage has arrived (commits are in order)
+        if (mma_last >= 0 && !mbar_wait(smem_addr(&empty[mma_last % TC_STAGES]), (mma_last / TC_STAGES) & 1)) ok = false;
+        if (!ok) {
+            for (int k = landed; k < issued; ++k) mbar_wait(smem_addr(&full[k % TC_STAGES]), (k / TC_STAGES) & 1);
+            fail = 1;
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    tc_epilogue<true>(jp, sp, t, X, Y, n, ldf, m0, n0, diag, tmem, base, fail == 0, err, red);
 }
 
 }  // namespace am1

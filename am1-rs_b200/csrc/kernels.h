@@ -224,7 +224,9 @@ __device__ __forceinline__ void oz_digits_of(double y, int8_t* __restrict__ D, l
     oz_store_digits(oz_digits_packed(y), D, plane, o);
 }
 __global__ void k_sp2_step_tc(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
-__global__ void k_sp2_step_tc1(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, int* err);
+// maps[2 job + i]: the tensor map of job's Xf_i (ldf x n FP32, box 32 x 128, 128-byte swizzle)
+__global__ void k_sp2_step_tc1(const Sp2Job* jobs, const GemmTile* tiles, int ntiles, const Sp2State* sst, const TmaDesc* maps,
+                               int* err);
 __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolState* st, int* need_eigen, double* work,
                              int* big_stall, int* big_count);
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each
