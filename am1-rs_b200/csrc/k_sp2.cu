@@ -71,6 +71,27 @@ __device__ double lz_eig(const double* a, const double* b, int m, int k, double 
     return 0.5 * (lo + hi);
 }
 
+// The same eigenvalue by one warp: 32-way multisection, each round 31 Sturm counts at interior
+// points of [lo, hi] on the lanes and the interval narrowed to the gap where the count passes k (a
+// factor 32 per round; 11 rounds reach the rounding level of the bisection).  Every lane of the warp
+// calls it and gets the same value.
+__device__ double lz_eig_warp(const double* a, const double* b, int m, int k, double lo, double hi) {
+    const int lane = threadIdx.x & 31;
+    for (int round = 0; round < 11; ++round) {
+        const double h = (hi - lo) * (1.0 / 32.0);
+        if (!(h > 0.0)) break;
+        const double x = lo + h * (lane + 1);
+        const bool below = lane < 31 && lz_count(a, b, m, x) <= k;  // x <= the k-th eigenvalue
+        const unsigned ball = __ballot_sync(0xffffffffu, below);
+        const int j = ball ? 31 - __clz(ball) : -1;  // the last interior point still below it
+        const double nlo = j >= 0 ? lo + h * (j + 1) : lo;
+        const double nhi = j + 2 <= 31 ? lo + h * (j + 2) : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    return 0.5 * (lo + hi);
+}
+
 // |last component| of the unit eigenvector of T for an exterior eigenvalue: inverse iteration
 // with the shift sigma just outside the spectrum, so T - sigma I is definite and the
 // tridiagonal solve needs no pivoting.
@@ -199,7 +220,7 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
         __syncthreads();
     }
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
         // Gershgorin interval of T contains its spectrum
         double tlo = 1e300, thi = -1e300;
         for (int i = 0; i < m; ++i) {
@@ -210,8 +231,9 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
         const double pad = 1e-12 * (fabs(tlo) + fabs(thi)) + 1e-300;
         tlo -= pad;
         thi += pad;
-        const double th_min = lz_eig(alpha, beta, m, 0, tlo, thi);
-        const double th_max = lz_eig(alpha, beta, m, m - 1, tlo, thi);
+        const double th_min = lz_eig_warp(alpha, beta, m, 0, tlo, thi);
+        const double th_max = lz_eig_warp(alpha, beta, m, m - 1, tlo, thi);
+        if (lane != 0) return;
         const double width = fmax(th_max - th_min, 1e-6);
         const double eps = 1e-8 * (fabs(th_min) + fabs(th_max) + 1.0);
         const double bm = beta[m - 1];
