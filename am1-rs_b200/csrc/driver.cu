@@ -452,6 +452,18 @@ bool encode_rows_map_f32(TmaDesc* out, const float* base, int ldf, int n) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// k_bisect for njobs matrices of at most maxn rows: a warp per eigenvalue while the whole launch stays
+// within about two waves of resident threads (one molecule, small batches), a thread per eigenvalue
+// otherwise (the warp form does about seven times the work, so it only pays when the GPU is idle).
+// warp_ok = false keeps the thread-per-eigenvalue bisection: the eigenvalues that seed inverse
+// iteration (whose cluster treatment was tuned on them).
+void bisect_launch(const TriJob* jobs, int njobs, int maxn, cudaStream_t s, bool warp_ok) {
+    constexpr long long kTwoWaves = 2LL * 148 * 2048;  // resident threads of two waves on a B200
+    const int lanes = warp_ok && (long long)njobs * maxn * 32 <= kTwoWaves ? 32 : 1;
+    const int per_block = 512 / lanes;
+    k_bisect<<<dim3(njobs, (maxn + per_block - 1) / per_block), 512, 2 * sizeof(double) * maxn, s>>>(jobs, nullptr, lanes);
+}
+
 inline int oz_ldq(int n) { return (n + 15) & ~15; }
 inline int oz_tiles_of(int n) {  // 128 x 48 tiles with an element on or above the diagonal
     int k = 0;
@@ -1480,7 +1492,9 @@ int enq_head(IterEnq& e, bool lowp_left) {
 // One purification step of every channel still purifying: the FP64 products (and the TF32 ones
 // while any molecule may be in its TF32 phase), then the trace bookkeeping.  zero_count: clear the
 // count of channels still purifying first (the captured loop's condition kernel clears it instead).
-int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
+// cond (captured solve only): the update also takes the loop's decision on that handle
+// (k_sp2_update_cond, batches of at most SP2_UPDATE_ONE channels), so no k_sp2_cond follows.
+int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count, const cudaGraphConditionalHandle* cond = nullptr) {
     Batch& b = e.b;
     const cudaStream_t s = e.s;
     Run& run = *e.run;
@@ -1518,8 +1532,12 @@ int enq_step(IterEnq& e, int sp2_max, bool lowp_left, bool zero_count) {
     }
     run.launched(AM1GPU_PHASE_DENSITY_CORE, nl);
     if ((rc = run.end(AM1GPU_PHASE_DENSITY_CORE, pc))) return rc;
-    if (zero_count) CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
-    k_sp2_update<<<cdiv(e.njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, e.njobs, sp2_max, b.d_sp2_active, b.d_work);
+    if (cond) {
+        k_sp2_update_cond<<<1, SP2_UPDATE_ONE, 0, s>>>(b.d_sp2, b.d_sp2_state, e.njobs, sp2_max, b.d_work, *cond, b.d_loop);
+    } else {
+        if (zero_count) CK(cudaMemsetAsync(b.d_sp2_active, 0, sizeof(int), s));
+        k_sp2_update<<<cdiv(e.njobs, 128), 128, 0, s>>>(b.d_sp2, b.d_sp2_state, e.njobs, sp2_max, b.d_sp2_active, b.d_work);
+    }
     run.launched(AM1GPU_PHASE_EIGEN);
     CK(cudaGetLastError());
     return AM1GPU_OK;
@@ -1661,7 +1679,9 @@ int add_if(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, cud
 
 // The SCF loop of run_device as one graph launch:
 //   k_scf_arm -> WHILE(scf) { head -> k_sp2_arm -> WHILE(sp2) { step -> k_sp2_cond } -> tail -> k_scf_cond }
-// and, in a graph kept for a resident batch's later runs, the tail split as
+// (for batches of at most SP2_UPDATE_ONE channels the step's update kernel sets the purification
+// loop's condition itself, k_sp2_update_cond, in place of k_sp2_update + k_sp2_cond) and, in a graph
+// kept for a resident batch's later runs, the tail split as
 //   finish -> k_stall_arm -> IF(stall) { stalled-purification eigensolver } -> rest -> k_scf_cond.
 // The kernels are the eager loop's, in the same order; only the loop decisions moved to the device
 // (k_graph.cu), and the eigensolver kernels for stalled purifications, which change nothing in an
@@ -1718,14 +1738,15 @@ int scf_loop_graph(IterEnq& e, const am1gpu_options& o, bool* launched) {
     const int64_t per_head = cnt.kernel_launches - head0 + 1;
     if ((rc = add_while(body, head, h_sp2, &w_sp2, &body2))) return rc;
     const int64_t step0 = cnt.kernel_launches;
+    const bool fused = e.njobs <= SP2_UPDATE_ONE;  // the update takes the loop's decision itself
     if ((rc = capture_into(cs, body2, nullptr, 0, &step, [&]() -> int {
-             int r = enq_step(ce, sp2_max, false, false);
+             int r = enq_step(ce, sp2_max, false, false, fused ? &h_sp2 : nullptr);
              if (r) return r;
-             k_sp2_cond<<<1, 32, 0, cs>>>(h_sp2, b.d_loop, b.d_sp2_active, sp2_max);
+             if (!fused) k_sp2_cond<<<1, 32, 0, cs>>>(h_sp2, b.d_loop, b.d_sp2_active, sp2_max);
              return AM1GPU_OK;
          })))
         return rc;
-    const int64_t per_step = cnt.kernel_launches - step0 + 1;
+    const int64_t per_step = cnt.kernel_launches - step0 + (fused ? 0 : 1);
     const int64_t tail0 = cnt.kernel_launches;
     int64_t per_stall = 0, per_tail = 0;
     if (b.graph_cacheable) {
@@ -1859,7 +1880,7 @@ int run_device(Batch& b, Mem& mem, const DevElem* dp, const am1gpu_options& o, a
     if ((rc = launch_tridiag(b, ws))) return rc;
     int64_t big_tri_launches = 0;
     if ((rc = launch_big_tridiag(b, s, &big_tri_launches))) return rc;
-    k_bisect<<<dim3(njobs, cdiv(b.maxn, 512)), 512, 2 * sizeof(double) * b.maxn, s>>>(b.d_tri, nullptr);  // a thread per eigenvalue
+    bisect_launch(b.d_tri, njobs, b.maxn, s, true);
     k_results<<<cdiv(b.nmol, 128), 128, 0, s>>>(b.d_mols, b.d_jobs, b.d_job0, b.nmol, b.d_st, b.d_status, dp, b.d_atom_z,
                                                  b.d_atom_xyz, b.d_res, b.d_charges);
     run.launched(AM1GPU_PHASE_FINAL, 5 + (int)b.tri_buckets.size() + (int)big_tri_launches);
@@ -2436,7 +2457,7 @@ int eigen_large_run(int n, const double* a_host, const double* a_dev, Mem& m, cu
     b.tri_big = {tj};
     int64_t launches = 0;
     if ((rc = launch_big_tridiag(b, s, &launches))) return rc;
-    k_bisect<<<dim3(1, cdiv(n, 512)), 512, 2 * sizeof(double) * n, s>>>(b.d_tri, nullptr);
+    bisect_launch(b.d_tri, 1, n, s, false);
     CK(cudaGetLastError());
     SteinJob sj{};
     sj.d = tj.d;
@@ -2853,7 +2874,7 @@ int symmetric_eigenvalues_one(int n, const double* a, double* w) {
         rc = launch_big_tridiag(b, ws->stream, &launches);
     }
     if (rc) return rc;
-    k_bisect<<<dim3(1, cdiv(n, 512)), 512, 2 * sizeof(double) * n, ws->stream>>>(b.d_tri, nullptr);
+    bisect_launch(b.d_tri, 1, n, ws->stream, true);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(w, D + o_eps, (size_t)n * 8, cudaMemcpyDeviceToHost, ws->stream));
     CK(cudaStreamSynchronize(ws->stream));

@@ -393,7 +393,11 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e2, in
     return c;
 }
 
-__global__ void k_bisect(const TriJob* __restrict__ jobs, const int* __restrict__ mask) {
+// lanes = 1: a thread per eigenvalue, bisection; lanes = 32: a warp per eigenvalue, 32-way
+// multisection (31 Sturm counts per round on the lanes, the interval narrowed to the gap where the
+// count passes k: a factor 32 per round, to the bisection's stopping width), for launches with few
+// eigenvalues, where the latency of one thread's ~50 dependent counts is the cost.
+__global__ void k_bisect(const TriJob* __restrict__ jobs, const int* __restrict__ mask, int lanes) {
     const TriJob jb = jobs[blockIdx.x];
     if (mask && !mask[jb.mol]) return;
     const int n = jb.n;
@@ -418,6 +422,25 @@ __global__ void k_bisect(const TriJob* __restrict__ jobs, const int* __restrict_
         bounds[1] = hi + pad;
     }
     __syncthreads();
+    if (lanes == 32) {
+        const int k = (blockIdx.y * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+        if (k >= n) return;  // whole warps: blockDim is a multiple of 32
+        double lo = bounds[0], hi = bounds[1];
+        for (int round = 0; round < 16; ++round) {
+            const double h = (hi - lo) * (1.0 / 32.0);
+            if (!(h > 0.0) || hi - lo <= 4.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi))) break;
+            const double x = lo + h * (lane + 1);
+            const bool below = lane < 31 && sturm_count(d, e2, n, x) <= k;
+            const unsigned ball = __ballot_sync(0xffffffffu, below);
+            const int j = ball ? 31 - __clz(ball) : -1;
+            const double nlo = j >= 0 ? lo + h * (j + 1) : lo;
+            const double nhi = j + 2 <= 31 ? lo + h * (j + 2) : hi;
+            lo = nlo;
+            hi = nhi;
+        }
+        if (lane == 0) jb.eps[k] = 0.5 * (lo + hi);
+        return;
+    }
     const int k0 = blockIdx.y * blockDim.x;  // this block's share of the eigenvalue indices
     if (k0 >= n) return;
     for (int k = k0 + threadIdx.x; k < min(n, k0 + (int)blockDim.x); k += blockDim.x) {

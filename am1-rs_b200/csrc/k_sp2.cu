@@ -601,12 +601,11 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step_tma(const Sp2Job* __
 }
 
 // After a step: reduce the tile partials (in tile order), test idempotency, choose the next branch.
-__global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs, int max_steps,
-                             int* __restrict__ active_count, double* __restrict__ work) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= njobs) return;
+// The update of channel j after its product; true while it still purifies.
+__device__ __forceinline__ bool sp2_update_job(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int j, int max_steps,
+                                               double* __restrict__ work) {
     Sp2State& s = sst[j];
-    if (!s.active) return;
+    if (!s.active) return false;
     const Sp2Job jb = jobs[j];
     // algorithmic work of the product just taken: a symmetric X.X, n^3 flops
     if (s.lowp) {
@@ -639,15 +638,39 @@ __global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restri
     if (low_done || floor_reached || idem < 1.0e-15 * fmax(1.0, (double)jb.n)) {
         s.active = 0;
         s.converged = 1;
-        return;
+        return false;
     }
     if (s.steps >= max_steps) {
         s.active = 0;
         s.converged = s.lowp;
-        return;
+        return false;
     }
     s.square = fabs(fr - jb.nocc) < fabs(2.0 * tr - fr - jb.nocc) ? 1 : 0;
-    atomicAdd(active_count, 1);
+    return true;
+}
+
+__global__ void k_sp2_update(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs, int max_steps,
+                             int* __restrict__ active_count, double* __restrict__ work) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    if (sp2_update_job(jobs, sst, j, max_steps, work)) atomicAdd(active_count, 1);
+}
+
+// The update of every channel and the purification loop's decision in one CTA (the captured solve
+// of a batch of at most SP2_UPDATE_ONE channels): the same per-channel update, the channels still
+// purifying counted by the CTA, then k_sp2_cond's step counters and condition.
+__global__ void __launch_bounds__(SP2_UPDATE_ONE) k_sp2_update_cond(const Sp2Job* __restrict__ jobs, Sp2State* __restrict__ sst, int njobs,
+                                                                    int max_steps, double* __restrict__ work,
+                                                                    cudaGraphConditionalHandle h, GraphLoop* __restrict__ loop) {
+    const int j = threadIdx.x;
+    const bool more_j = j < njobs && sp2_update_job(jobs, sst, j, max_steps, work);
+    const int active = __syncthreads_count(more_j);
+    if (threadIdx.x == 0) {
+        const int step = loop->sp2_step + 1;
+        loop->sp2_step = step;
+        loop->sp2_total += 1;
+        cudaGraphSetConditional(h, (active > 0 && step < max_steps) ? 1u : 0u);
+    }
 }
 
 // P_new = w X (the converged X); molecules whose purification stalled are flagged for the

@@ -197,6 +197,9 @@ __global__ void k_commutator_tma(const ChanJob* jobs, const GemmTile* tiles, int
                                  int* err);
 size_t dgemm_smem_bytes();
 __global__ void k_sp2_update(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, int* active_count, double* work);
+constexpr int SP2_UPDATE_ONE = 1024;  // channels k_sp2_update_cond takes in its one CTA
+__global__ void k_sp2_update_cond(const Sp2Job* jobs, Sp2State* sst, int njobs, int max_steps, double* work, cudaGraphConditionalHandle h,
+                                  GraphLoop* loop);
 size_t tc_smem_bytes();
 size_t tc1_smem_bytes();
 size_t oz_smem_bytes();
@@ -232,8 +235,9 @@ __global__ void k_sp2_finish(const Sp2Job* jobs, const Sp2State* sst, const MolS
 // launched in clusters of C CTAs (one cluster per job), tridiag_smem_bytes(n, C) each
 __global__ void k_tridiag(const TriJob* jobs, const int* mask);
 size_t tridiag_smem_bytes(int n, int C);
-// a thread per eigenvalue; blockIdx.y selects the block of 512 eigenvalue indices (large n)
-__global__ void k_bisect(const TriJob* jobs, const int* mask);
+// lanes = 1: a thread per eigenvalue, blockIdx.y the block of blockDim eigenvalue indices; lanes =
+// 32: a warp per eigenvalue, blockIdx.y the block of blockDim / 32 indices (bisect_launch sizes both)
+__global__ void k_bisect(const TriJob* jobs, const int* mask, int lanes);
 // matrices too large for a cluster's shared memory, the matrix in global memory: one cooperative
 // launch over the whole GPU (grid <= co-resident CTAs of TRIB_THREADS threads), or a cluster of
 // C CTAs per matrix (grid (C, count), blockIdx.y indexes jobs); tridiag_big_smem_bytes(largest n)
