@@ -181,7 +181,8 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
         extern __shared__ __align__(1024) unsigned char ctsm[];
         __shared__ DtBars bars;
         const TmaDesc* mp = maps + 4 * tl.job;  // F and P are symmetric: B = F or P read by rows
-        if (!dg_mainloop_tma(dt_stages(ctsm), bars, mp + 2, mp + 3, mp + 3, mp + 2, false, n, m0, n0, acc, compute)) {
+        const int shape = dg_quarter_shape(m0, n0, n, n, tl.tm == tl.tn);
+        if (!dg_mainloop_tma(dt_stages(ctsm), bars, mp + 2, mp + 3, mp + 3, mp + 2, false, n, m0, n0, acc, shape)) {
             if (threadIdx.x == 0) atomicOr(err, 1 << 11);
             return;
         }

@@ -590,10 +590,11 @@ __global__ void __launch_bounds__(DG_THREADS, 4) k_sp2_step_tma(const Sp2Job* __
     if (!sp->active || sp->lowp || jp->oz) return;
     const int n = jp->n;
     const int m0 = tl.tm * DG_TILE, n0 = tl.tn * DG_TILE;
-    const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
+    const int shape = dg_quarter_shape(m0, n0, n, n, tl.tm == tl.tn);
+    const bool compute = shape != 0;
     const TmaDesc* map = maps + 4 * tl.job + sp->cur;
     double acc[2][4][4];
-    if (!dg_mainloop_tma(dt_stages(dtsm), bars, map, map, nullptr, nullptr, tl.tm == tl.tn, n, m0, n0, acc, compute)) {
+    if (!dg_mainloop_tma(dt_stages(dtsm), bars, map, map, nullptr, nullptr, tl.tm == tl.tn, n, m0, n0, acc, shape)) {
         if (threadIdx.x == 0) atomicOr(err, 1 << 11);
         return;
     }
