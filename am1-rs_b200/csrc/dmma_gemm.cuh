@@ -96,8 +96,9 @@ __device__ __forceinline__ void dg_load(double* smem, int st, const double* __re
 
 // Whether this warp's 32x32 quarter of the 64x64 tile needs computing: not when it is padding
 // or, in a tile on the diagonal of a symmetric result (only its upper triangle is needed), when it
-// lies below the diagonal.  (Skipping finer 16x8 blocks inside a quarter costs more in predicated
-// issue than it saves.)
+// lies below the diagonal.  (In the cp.async loops, skipping finer 16x8 blocks inside a quarter by
+// predicates cost more in issue than it saved; the TMA loop dispatches once per k-tile on the
+// quarter's shape instead, dg_quarter_shape.)
 __device__ __forceinline__ bool dg_quarter_on(int m0, int n0, int M, int N, bool diag_tile) {
     const int warp = threadIdx.x >> 5;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
@@ -301,48 +302,54 @@ __device__ __forceinline__ int dg_quarter_shape(int m0, int n0, int M, int N, bo
     return dt_shape(mi, nj, (diag_tile && r0 - m0 == c0 - n0 && mi == 2) ? 1 : 0);
 }
 
-// one k-step of 8 over the blocks of shape (MI, NJ, DG), operands in the 128-byte-swizzled boxes
+// one k-tile (two k-steps of 8; the second skipped when K ends inside the first) over the blocks of
+// shape (MI, NJ, DG), operands in the 128-byte-swizzled boxes; c0 = (tq >> 1) ^ g of the lane
 template <int MI, int NJ, bool DG>
-__device__ __forceinline__ void dt_kstep(const unsigned char* As, const unsigned char* Bs, int ra, int rb, int x0, int x1,
+__device__ __forceinline__ void dt_ktile(const unsigned char* As, const unsigned char* Bs, int ra, int rb, int c0, int kbase, int K,
                                          double acc[2][4][4]) {
-    double a[MI][4], b[NJ][2];
 #pragma unroll
-    for (int i = 0; i < MI; ++i) {
-        const unsigned char* p = As + ra + i * 16 * 128;
-        a[i][0] = *reinterpret_cast<const double*>(p + x0);
-        a[i][1] = *reinterpret_cast<const double*>(p + 8 * 128 + x0);
-        a[i][2] = *reinterpret_cast<const double*>(p + x1);
-        a[i][3] = *reinterpret_cast<const double*>(p + 8 * 128 + x1);
+    for (int kk = 0; kk < DG_BK; kk += 8) {
+        if (kk > 0 && kbase + kk >= K) break;
+        const int x0 = (c0 ^ (kk >> 1)) << 4, x1 = (c0 ^ ((kk >> 1) | 2)) << 4;
+        double a[MI][4], b[NJ][2];
+#pragma unroll
+        for (int i = 0; i < MI; ++i) {
+            const unsigned char* p = As + ra + i * 16 * 128;
+            a[i][0] = *reinterpret_cast<const double*>(p + x0);
+            a[i][1] = *reinterpret_cast<const double*>(p + 8 * 128 + x0);
+            a[i][2] = *reinterpret_cast<const double*>(p + x1);
+            a[i][3] = *reinterpret_cast<const double*>(p + 8 * 128 + x1);
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const unsigned char* p = Bs + rb + j * 8 * 128;
+            b[j][0] = *reinterpret_cast<const double*>(p + x0);
+            b[j][1] = *reinterpret_cast<const double*>(p + x1);
+        }
+#pragma unroll
+        for (int i = 0; i < MI; ++i)
+#pragma unroll
+            for (int j = 0; j < NJ; ++j)
+                if (!(DG && i == 1 && j < 2)) dg_mma(acc[i][j], a[i], b[j]);
     }
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-        const unsigned char* p = Bs + rb + j * 8 * 128;
-        b[j][0] = *reinterpret_cast<const double*>(p + x0);
-        b[j][1] = *reinterpret_cast<const double*>(p + x1);
-    }
-#pragma unroll
-    for (int i = 0; i < MI; ++i)
-#pragma unroll
-        for (int j = 0; j < NJ; ++j)
-            if (!(DG && i == 1 && j < 2)) dg_mma(acc[i][j], a[i], b[j]);
 }
 
-__device__ __forceinline__ void dt_kstep_shape(int shape, const unsigned char* As, const unsigned char* Bs, int ra, int rb, int x0,
-                                               int x1, double acc[2][4][4]) {
+__device__ __forceinline__ void dt_ktile_shape(int shape, const unsigned char* As, const unsigned char* Bs, int ra, int rb, int c0,
+                                               int kbase, int K, double acc[2][4][4]) {
     if (shape == DT_FULL) {
-        dt_kstep<2, 4, false>(As, Bs, ra, rb, x0, x1, acc);
+        dt_ktile<2, 4, false>(As, Bs, ra, rb, c0, kbase, K, acc);
         return;
     }
     switch (shape) {
-        case dt_shape(2, 4, 1): dt_kstep<2, 4, true>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(2, 3, 1): dt_kstep<2, 3, true>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(2, 3, 0): dt_kstep<2, 3, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(2, 2, 0): dt_kstep<2, 2, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(2, 1, 0): dt_kstep<2, 1, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(1, 4, 0): dt_kstep<1, 4, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(1, 3, 0): dt_kstep<1, 3, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(1, 2, 0): dt_kstep<1, 2, false>(As, Bs, ra, rb, x0, x1, acc); break;
-        case dt_shape(1, 1, 0): dt_kstep<1, 1, false>(As, Bs, ra, rb, x0, x1, acc); break;
+        case dt_shape(2, 4, 1): dt_ktile<2, 4, true>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(2, 3, 1): dt_ktile<2, 3, true>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(2, 3, 0): dt_ktile<2, 3, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(2, 2, 0): dt_ktile<2, 2, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(2, 1, 0): dt_ktile<2, 1, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(1, 4, 0): dt_ktile<1, 4, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(1, 3, 0): dt_ktile<1, 3, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(1, 2, 0): dt_ktile<1, 2, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
+        case dt_shape(1, 1, 0): dt_ktile<1, 1, false>(As, Bs, ra, rb, c0, kbase, K, acc); break;
         default: break;
     }
 }
@@ -440,12 +447,7 @@ __device__ __forceinline__ bool dg_mainloop_tma(unsigned char* stages, DtBars& b
                         for (int e = 0; e < 4; ++e) acc[i][j][e] = -acc[i][j][e];
             }
             const int kbase = (kt < KT ? kt : kt - KT) * DG_BK;
-#pragma unroll
-            for (int kk = 0; kk < DG_BK; kk += 8) {
-                if (kk > 0 && kbase + kk >= K) break;
-                const int x0 = (c0 ^ (kk >> 1)) << 4, x1 = (c0 ^ ((kk >> 1) | 2)) << 4;
-                dt_kstep_shape(shape, As, Bs, ra, rb, x0, x1, acc);
-            }
+            dt_ktile_shape(shape, As, Bs, ra, rb, c0, kbase, K, acc);
         }
         __syncwarp();
         if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(dt_saddr(&bars.empty[s])) : "memory");

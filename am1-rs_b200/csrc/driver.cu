@@ -846,7 +846,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         const long long tn = (p.nao + 63) / 64;
         const long long sp2part = 2 * std::max<long long>(sp2_nblk, tn * (tn + 1) / 2);
         const long long cpart = CP_N * tn * (tn + 1) / 2;
-        misc += p.nch * (4LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 2 + 128);
+        misc += p.nch * (5LL * p.nao + p.npad + (long long)nblk * (RED_N + 1) + sp2part + cpart + 4 + 128);
     }
     const size_t o_misc = take(dv, sizeof(double) * misc);
     const size_t o_colid = take(dv, sizeof(int) * (size_t)(nch_total * (b.maxn + 64)));
@@ -1025,6 +1025,8 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             mi_off += n;
             cj.rowmax = d_misc + mi_off;
             mi_off += n;
+            cj.rowdf = d_misc + mi_off;
+            mi_off += n;
             cj.eps = b.d_eps + eps_off;
             eps_off += n;
             double* tri_d = d_misc + mi_off;
@@ -1035,7 +1037,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             double* sp2part = d_misc + mi_off;
             mi_off += 2 * std::max<long long>(sp2_nblk, tn_ * (tn_ + 1) / 2);
             double* sp2bounds = d_misc + mi_off;
-            mi_off += 2;
+            mi_off += 4;
             double* lam = d_misc + mi_off;
             mi_off += p.npad;
             cj.red = d_misc + mi_off;
@@ -1051,6 +1053,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             sj.F = cj.Fx;
             sj.rowmin = cj.rowmin;
             sj.rowmax = cj.rowmax;
+            sj.rowdf = cj.rowdf;
             sj.X0 = base + SLOT_GT * nn;
             sj.X1 = base + SLOT_VS * nn;
             sj.P = cj.Pnew;
@@ -2588,7 +2591,7 @@ int density_purify_one(int n, const double* F, double nocc, double weight, int p
                  o_toz = take(sizeof(GemmTile) * ntoz),
                  o_ms = take(sizeof(MolState)), o_f = take(8 * nn), o_rmin = take(8 * (size_t)n), o_rmax = take(8 * (size_t)n);
     const size_t staged = align256(off);
-    const size_t o_sst = take(sizeof(Sp2State)), o_bnd = take(16), o_x0 = take(8 * nn), o_x1 = take(8 * nn), o_p = take(8 * nn),
+    const size_t o_sst = take(sizeof(Sp2State)), o_bnd = take(32), o_x0 = take(8 * nn), o_x1 = take(8 * nn), o_p = take(8 * nn),
                  o_part = take(16 * (size_t)std::max(32, nt64)), o_xf = take(8 * (size_t)n * ldf + 64), o_need = take(16),
                  o_work = take(8 * kWorkN), o_act = take(16), o_stall = take(16),
                  o_dq = take(2 * (size_t)kOzPlanes * n * ldq);

@@ -435,6 +435,8 @@ __global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __
     }
 }
 
+constexpr int COMBINE_CHUNK = 4;
+
 __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int force) {
     const ChanJob jb = jobs[blockIdx.y];
     const MolState& s = st[jb.mol];
@@ -443,31 +445,66 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const long long ls = packed_sym_len(n);
     const int m = s.hist_count;
+    // from the second iteration on, F* still holds the previous iteration's: the distance between the
+    // two (row sums of squares) lets k_sp2_bounds widen the previous spectral interval instead of
+    // running the Lanczos bounds again
+    const bool diff = s.iter > 0;
+    const int mode = s.mode;
+    const double* hrow[MAX_DIIS];  // history entries in logical order, and their coefficients
+    double cf[MAX_DIIS];
+#pragma unroll
+    for (int i = 0; i < MAX_DIIS; ++i) {
+        hrow[i] = jb.hF + ((s.hist_head + i) % MAX_DIIS) * ls;
+        cf[i] = i < m ? s.coeff[i] : 0.0;
+    }
     for (int r = blockIdx.x * nw + warp; r < n; r += gridDim.x * nw) {
         double* out = jb.Fx + (long long)r * n;
-        double bound = 0.0, diag = 0.0;
-        for (int c = lane; c < n; c += 32) {
-            double v;
-            if (s.mode == 0) {
-                v = jb.F[(long long)r * n + c];
-            } else {
-                const int lo = min(r, c), hi = max(r, c);
-                const long long si = sym_row(lo, n) + (hi - lo);
-                v = 0.0;
-                for (int i = 0; i < m; ++i) v += s.coeff[i] * jb.hF[((s.hist_head + i) % MAX_DIIS) * ls + si];
+        double bound = 0.0, diag = 0.0, dd = 0.0;
+        // chunks of COMBINE_CHUNK columns per lane: every load of a chunk (history entries, the previous
+        // F*) is issued before any of its stores; each lane still visits its columns in ascending order
+        for (int c0 = 0; c0 < n; c0 += 32 * COMBINE_CHUNK) {
+            double val[COMBINE_CHUNK];
+#pragma unroll
+            for (int u = 0; u < COMBINE_CHUNK; ++u) {
+                const int c = c0 + 32 * u + lane;
+                double v = 0.0;
+                if (c < n) {
+                    if (mode == 0) {
+                        v = jb.F[(long long)r * n + c];
+                    } else {
+                        const int lo = min(r, c), hi = max(r, c);
+                        const long long si = sym_row(lo, n) + (hi - lo);
+#pragma unroll
+                        for (int i = 0; i < MAX_DIIS; ++i)
+                            if (i < m) v += cf[i] * hrow[i][si];
+                    }
+                    if (diff) {
+                        const double d = v - out[c];
+                        dd = fma(d, d, dd);
+                    }
+                }
+                val[u] = v;
             }
-            out[c] = v;
-            if (c == r) diag = v;
-            else bound += fabs(v);
+#pragma unroll
+            for (int u = 0; u < COMBINE_CHUNK; ++u) {
+                const int c = c0 + 32 * u + lane;
+                if (c < n) {
+                    out[c] = val[u];
+                    if (c == r) diag = val[u];
+                    else bound += fabs(val[u]);
+                }
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             bound += __shfl_xor_sync(0xffffffffu, bound, o);
             diag += __shfl_xor_sync(0xffffffffu, diag, o);
+            dd += __shfl_xor_sync(0xffffffffu, dd, o);
         }
         if (lane == 0) {
             jb.rowmin[r] = diag - bound;
             jb.rowmax[r] = diag + bound;
+            jb.rowdf[r] = dd;
         }
     }
 }

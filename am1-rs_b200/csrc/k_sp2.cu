@@ -35,6 +35,8 @@ namespace cg = cooperative_groups;
 // the interval maps just outside [0, 1], where the trace-correcting steps pull it back; a run
 // that still fails to converge falls back to the eigensolver.  One CTA per channel.
 constexpr int SP2_LANCZOS = 12;
+// largest widening of a reused spectral interval, as a fraction of the width of the last Lanczos run's
+constexpr double SP2_REUSE_FRAC = 0.01;
 constexpr int SP2_BOUND_THREADS = 512;
 
 __device__ double bounds_block_sum(double v, double* red) {
@@ -145,6 +147,36 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
         gred[0][warp] = glo;
         gred[1][warp] = ghi;
     }
+    // From the second SCF iteration on, F* has moved by delta = ||F* - F*_previous||_F from the matrix
+    // of the previous interval, and no eigenvalue moves further than that (Weyl's inequality,
+    // |lambda_i(A + E) - lambda_i(A)| <= ||E||_2 <= ||E||_F).  While the widening added since the last
+    // Lanczos run stays below SP2_REUSE_FRAC of that run's width, the previous interval widened by
+    // delta on both sides (and capped by the Gershgorin interval of F*) is taken instead of a new run.
+    const bool may_reuse = jb.rowdf != nullptr && st[jb.mol].iter > 0;
+    const double b_lo = jb.bounds[0], b_hi = jb.bounds[1], b_slack = jb.bounds[2], b_width = jb.bounds[3];
+    double dsum = 0.0;
+    if (may_reuse)
+        for (int i = tid; i < n; i += SP2_BOUND_THREADS) dsum += jb.rowdf[i];
+    dsum = bounds_block_sum(dsum, red);  // its barriers also publish gred
+    if (may_reuse) {
+        double rlo = gred[0][0], rhi = gred[1][0];
+        for (int v = 1; v < NW; ++v) {
+            rlo = fmin(rlo, gred[0][v]);
+            rhi = fmax(rhi, gred[1][v]);
+        }
+        const double delta = sqrt(dsum) * (1.0 + 1e-12);
+        const double slack = b_slack + delta;
+        const double lo = fmax(b_lo - delta, rlo), hi = fmin(b_hi + delta, rhi);
+        if (isfinite(slack) && b_width > 0.0 && slack <= SP2_REUSE_FRAC * b_width && hi > lo) {
+            __syncthreads();  // every thread has read the previous interval
+            if (tid == 0) {
+                jb.bounds[0] = lo;
+                jb.bounds[1] = hi;
+                jb.bounds[2] = slack;
+            }
+            return;
+        }
+    }
     // fixed start vector, normalised
     double nq = 0.0;
     for (int i = tid; i < n; i += SP2_BOUND_THREADS) {
@@ -247,6 +279,8 @@ __global__ void __launch_bounds__(SP2_BOUND_THREADS) k_sp2_bounds(const Sp2Job* 
         }
         jb.bounds[0] = fmax(lo, glo);
         jb.bounds[1] = fmin(hi, ghi);
+        jb.bounds[2] = 0.0;
+        jb.bounds[3] = jb.bounds[1] - jb.bounds[0];
     }
 }
 

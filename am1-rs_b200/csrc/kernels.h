@@ -59,6 +59,7 @@ struct ChanJob {
     double* hD;       // packed history of P  [8][n(n+1)/2] (A-DIIS) or nullptr
     double* rowmin;   // n: Gershgorin lower bound of each row of F*
     double* rowmax;   // n: Gershgorin upper bound
+    double* rowdf;    // n: sum over the row of (F* - F* of the previous iteration)^2 (from the second iteration on)
     double* red;      // per-block partial sums [nblk][RED_N]
     double* red2;     // per-block partial sums of (P_new - P)^2 [nblk]
     double* cpart;    // per-tile partial sums of the commutator pass [ntiles][CP_N]
@@ -74,11 +75,13 @@ struct Sp2Job {
     const double* F;        // the extrapolated Fock matrix F*
     const double* rowmin;   // Gershgorin bounds of F*
     const double* rowmax;
+    const double* rowdf;    // row sums of (F* - F*_previous)^2, or nullptr (always run the Lanczos bounds)
     double* X0;             // ping-pong iterates, n x n each
     double* X1;
     double* P;              // output density (w X), n x n (may alias X0)
     double* part;           // partial sums [max(nblk, ntiles)][2]
-    double* bounds;         // [2] spectral interval of F* used for the mapping (k_sp2_bounds)
+    double* bounds;         // [4] spectral interval of F* used for the mapping (k_sp2_bounds), the widening
+                            // added since the last Lanczos run, the width of that run's interval
     double nocc, weight;
     int n, mol, tile0, ntiles;
     int fallback;           // 1: a stalled purification falls back to the eigensolver; 0: LINALG
