@@ -6,8 +6,8 @@
 //     lane-parallel, a partner per lane, 32 at a time, in registers, and reduced over the warp once
 //     per atom;
 //   * the exchange blocks K_AB = -s sum P^s_ab (mu nu | lambda sigma) (src/fock.rs:449-466) of a
-//     heavy A with heavy B > A: two pairs at a time, their adjacent 100-integral blocks staged
-//     through shared memory with coalesced loads, a half-warp per pair and a lane per output,
+//     heavy A with heavy B > A: four pairs at a time, their adjacent 100-integral blocks staged
+//     through shared memory with coalesced loads, eight lanes per pair and a lane per two outputs,
 //     written to F_AB and F_BA;
 //   * the exchange of every other pair (a hydrogen on either side: blocks of 10 or 1 integrals)
 //     lane-parallel, the lane of the partner writing F_AB and F_BA when A is the pair's first atom.
@@ -37,6 +37,7 @@ __device__ __forceinline__ double oc_integral(int a, int b, int c, int d, const 
 }
 
 constexpr int FOCK_WARPS = 8;
+constexpr int FOCK_XX_ROUND = 4;  // heavy-heavy exchange blocks per round of a warp
 
 // the AO pair of packed index q (inverse of pack2)
 __host__ __device__ constexpr int pair_hi(int q) { return q < 1 ? 0 : q < 3 ? 1 : q < 6 ? 2 : 3; }
@@ -46,9 +47,9 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __re
                                                          int natoms_total, const DevElem* __restrict__ params,
                                                          const int* __restrict__ atom_z, const double* __restrict__ wstore,
                                                          double* __restrict__ arena, const MolState* __restrict__ st, int force) {
-    __shared__ double s_w[FOCK_WARPS][200];
+    __shared__ double s_w[FOCK_WARPS][100 * FOCK_XX_ROUND];
     __shared__ double s_q[FOCK_WARPS][10];
-    __shared__ double s_pab[FOCK_WARPS][2][2][16];
+    __shared__ double s_pab[FOCK_WARPS][FOCK_XX_ROUND][2][16];
     __shared__ double s_j[FOCK_WARPS][10];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int a = blockIdx.x * FOCK_WARPS + warp;
@@ -109,41 +110,49 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __re
                 }
             }
         }
-        // exchange blocks with the heavier-indexed heavy partners (A is the pair's first atom), two
-        // partners at a time: lanes 0..15 take B0, lanes 16..31 take B0 + 1, a lane per output
-        // element of the 4 x 4 block (the same sum, in the same order, as one partner at a time)
-        const int half = lane >> 4, l16 = lane & 15;
-        for (int B0 = A + 1; B0 < h; B0 += 2) {
-            const int nb = min(2, h - B0);  // partners in this round
+        // exchange blocks with the heavier-indexed heavy partners (A is the pair's first atom), four
+        // partners at a time: lanes 8p..8p+7 take B0 + p, a lane per two output elements of the 4 x 4
+        // block (each element the same sum, in the same order, as one partner at a time)
+        const int slot = lane >> 3, l8 = lane & 7;
+        for (int B0 = A + 1; B0 < h; B0 += FOCK_XX_ROUND) {
+            const int nb = min(FOCK_XX_ROUND, h - B0);  // partners in this round
             const double* blk0 = w + 100LL * ((long long)A * h - (long long)A * (A + 1) / 2 + (B0 - A - 1));
-            for (int l = lane; l < 100 * nb; l += 32) wb[l] = blk0[l];  // the blocks of (A, B0), (A, B0 + 1) are adjacent
-            const int B = B0 + half;
-            const bool mine = half < nb;
+            for (int l = lane; l < 100 * nb; l += 32) wb[l] = blk0[l];  // the blocks of (A, B0 ..) are adjacent
+            const int B = B0 + slot;
+            const bool mine = slot < nb;
             const int oB = 4 * B;
             if (mine) {
-                const long long idx = (long long)(oA + (l16 >> 2)) * n + oB + (l16 & 3);
-                s_pab[warp][half][0][l16] = P0[idx];
-                if (P1) s_pab[warp][half][1][l16] = P1[idx];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int e = 2 * l8 + u;
+                    const long long idx = (long long)(oA + (e >> 2)) * n + oB + (e & 3);
+                    s_pab[warp][slot][0][e] = P0[idx];
+                    if (P1) s_pab[warp][slot][1][e] = P1[idx];
+                }
             }
             __syncwarp();
             if (mine) {
-                const int mu = l16 >> 2, la = l16 & 3;
-                const long long ab = (long long)(oA + mu) * n + oB + la;
-                const long long ba = (long long)(oB + la) * n + oA + mu;
-                const double hab = H0[ab];
-                const double* wbh = wb + 100 * half;
-                for (int c = 0; c < md.nch; ++c) {
-                    double acc = 0.0;
+                const double* wbh = wb + 100 * slot;
 #pragma unroll
-                    for (int nu = 0; nu < 4; ++nu) {
-                        const double* row = wbh + pack2(mu, nu) * 10;
+                for (int u = 0; u < 2; ++u) {
+                    const int e = 2 * l8 + u;
+                    const int mu = e >> 2, la = e & 3;
+                    const long long ab = (long long)(oA + mu) * n + oB + la;
+                    const long long ba = (long long)(oB + la) * n + oA + mu;
+                    const double hab = H0[ab];
+                    for (int c = 0; c < md.nch; ++c) {
+                        double acc = 0.0;
 #pragma unroll
-                        for (int sg = 0; sg < 4; ++sg) acc += s_pab[warp][half][c][nu * 4 + sg] * row[pack2(la, sg)];
+                        for (int nu = 0; nu < 4; ++nu) {
+                            const double* row = wbh + pack2(mu, nu) * 10;
+#pragma unroll
+                            for (int sg = 0; sg < 4; ++sg) acc += s_pab[warp][slot][c][nu * 4 + sg] * row[pack2(la, sg)];
+                        }
+                        const double v = hab - acc * sc;
+                        double* F = c == 0 ? F0 : F1;
+                        F[ab] = v;
+                        F[ba] = v;
                     }
-                    const double v = hab - acc * sc;
-                    double* F = c == 0 ? F0 : F1;
-                    F[ab] = v;
-                    F[ba] = v;
                 }
             }
             __syncwarp();

@@ -157,6 +157,8 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
 // COPY: how the operands reach shared memory: 0 8-byte cp.async, 1 16-byte cp.async (even n, 16-byte
 // aligned rows), 2 tensor-memory-accelerator boxes from the job's tensor maps of F and P
 // (maps[4 job + 2], maps[4 job + 3]; a copy wait that runs out sets bit 11 of *err).
+constexpr int CT_LD = DG_TILE + 1;  // row stride of the staged commutator tile (doubles)
+
 template <int COPY>
 __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int ntiles,
                                                 const MolState* __restrict__ st, const TmaDesc* __restrict__ maps, int* __restrict__ err) {
@@ -177,6 +179,7 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
     // e is antisymmetric: a warp whose quarter is padding or lies below the diagonal issues no MMAs
     const bool compute = dg_quarter_on(m0, n0, n, n, tl.tm == tl.tn);
     double acc[2][4][4];
+    double* T;  // the tile staged for the epilogue, in the pipeline's shared memory (free after the k-loop)
     if constexpr (COPY == 2) {
         extern __shared__ __align__(1024) unsigned char ctsm[];
         __shared__ DtBars bars;
@@ -186,34 +189,47 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
             if (threadIdx.x == 0) atomicOr(err, 1 << 11);
             return;
         }
+        T = reinterpret_cast<double*>(dt_stages(ctsm));
     } else {
         extern __shared__ __align__(16) double dsm[];
         dg_mainloop_diff<COPY == 1>(dsm, jb.F, jb.P, jb.P, jb.F, n, n, m0, n0, acc, compute);
+        T = dsm;
     }
+    // e by tile rows: the strict upper triangle of a row is contiguous in the packed history, so each
+    // warp's stores of e and loads of the live slots' error vectors are runs of consecutive words
+    if (compute) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) T[dg_row(i, e) * CT_LD + dg_col(j, e)] = acc[i][j][e];
+    }
+    __syncthreads();
     double v[CP_N];
 #pragma unroll
     for (int k = 0; k < CP_N; ++k) v[k] = 0.0;
+    for (int rl = warp; rl < DG_TILE; rl += DG_THREADS / 32) {
+        const int r = m0 + rl;
+        if (r >= n) break;
+        const long long arow = anti_row(r, n) - r - 1;  // packed index of (r, c) is arow + c
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+        for (int hlf = 0; hlf < 2; ++hlf) {
+            const int cl = lane + 32 * hlf, c = n0 + cl;
+            if (r < c && c < n) {
+                const double ev = T[rl * CT_LD + cl];
+                const long long ai = arow + c;
+                jb.hE[newslot * la + ai] = ev;
+                v[CP_ERR2] += 2.0 * ev * ev;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int r = m0 + dg_row(i, e);
-                const int c = n0 + dg_col(j, e);
-                if (compute && r < c && c < n) {
-                    const double ev = acc[i][j][e];
-                    const long long ai = anti_row(r, n) + (c - r - 1);
-                    jb.hE[newslot * la + ai] = ev;
-                    v[CP_ERR2] += 2.0 * ev * ev;
-#pragma unroll
-                    for (int q = 0; q < MAX_DIIS; ++q)
-                        if (q == newslot)
-                            v[CP_B + q] += ev * ev;
-                        else if (live >> q & 1u)
-                            v[CP_B + q] += ev * jb.hE[q * la + ai];
-                }
+                for (int q = 0; q < MAX_DIIS; ++q)
+                    if (q == newslot)
+                        v[CP_B + q] += ev * ev;
+                    else if (live >> q & 1u)
+                        v[CP_B + q] += ev * jb.hE[q * la + ai];
             }
+        }
+    }
 #pragma unroll
     for (int k = 0; k < CP_N; ++k) {
         double x = v[k];
@@ -224,8 +240,8 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
     __syncthreads();
     if (tid < CP_N) {
         // index of tile (tm, tn), tm <= tn, in the channel's row-major upper-triangle tile list
-        const int T = (n + DG_TILE - 1) / DG_TILE;
-        const int local = tl.tm * T - tl.tm * (tl.tm - 1) / 2 + (tl.tn - tl.tm);
+        const int nt = (n + DG_TILE - 1) / DG_TILE;
+        const int local = tl.tm * nt - tl.tm * (tl.tm - 1) / 2 + (tl.tn - tl.tm);
         jb.cpart[(long long)local * CP_N + tid] = red[tid][0] + red[tid][1] + red[tid][2] + red[tid][3];
     }
 }
