@@ -155,6 +155,18 @@ int g_sms = 148;        // SMs of the current device
 
 // Smallest cluster (1, 2, 4, 8, 16 CTAs) whose row share of an n x n matrix fits one CTA's
 // shared memory; 0 when none does.
+// Largest matrix one tridiagonalisation CTA holds (the order the cluster reductions hand over at).
+int tridiag_one_cta_max() {
+    static thread_local int cached_budget = -1, cached = 0;
+    if (cached_budget != g_tridiag_budget) {
+        int m = 2;
+        while (tridiag_smem_bytes(m + 1, 1) <= (size_t)g_tridiag_budget) ++m;
+        cached = m;
+        cached_budget = g_tridiag_budget;
+    }
+    return cached;
+}
+
 int tridiag_cluster(int n) {
     for (int C = 1; C <= 16; C *= 2)
         if (tridiag_smem_bytes(n, C) <= (size_t)g_tridiag_budget) return C;
@@ -823,7 +835,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_xfmaps = take(st, mixed ? sizeof(TmaDesc) * 2 * std::max<long long>(nch_total, 1) : sizeof(TmaDesc) * 2);
     const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
     const size_t o_ozt = take(st, sizeof(GemmTile) * std::max(tiles_oz, 1));
-    const size_t o_tri = take(st, sizeof(TriJob) * nch_total);
+    const size_t o_tri = take(st, sizeof(TriJob) * 2 * nch_total);  // the jobs, then the one-CTA continuations
     const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
     const size_t par_bytes = host_tab ? sizeof(DevElem) * 2 * (MAX_Z + 1) : 0;
@@ -1204,6 +1216,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     std::stable_sort(tix.begin(), tix.end(), [&](int x, int y) { return tri_all[x].n > tri_all[y].n; });
     b.tri_buckets.clear();
     b.tri_big.clear();
+    int nhand = 0;
     for (size_t i = 0; i < tix.size(); ++i) {
         const TriJob& tj = tri_all[tix[i]];
         htri[i] = tj;
@@ -1215,6 +1228,30 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
         if (b.tri_buckets.empty() || b.tri_buckets.back().C != C) b.tri_buckets.push_back({(int)i, 0, C, 0});
         b.tri_buckets.back().count++;
         b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tj.n, C));
+        // a cluster reduction stops once its trailing block fits one CTA, writes it to the channel's
+        // free GT slot, and a one-CTA job (launched with the single-CTA matrices, after every cluster
+        // launch) finishes it: the cluster's SMs are freed for the other matrices
+        const int m1 = tridiag_one_cta_max();
+        if (C > 1 && m1 >= 8 && m1 < tj.n) {
+            htri[i].stop = tj.n - m1;
+            TriJob h2 = tj;
+            h2.A = tj.W;
+            h2.W = nullptr;
+            h2.work = nullptr;
+            h2.d = tj.d + htri[i].stop;
+            h2.e = tj.e + htri[i].stop;
+            h2.eps = nullptr;
+            h2.n = m1;
+            h2.stop = 0;
+            htri[tix.size() + nhand++] = h2;
+        }
+    }
+    if (nhand > 0) {  // the continuations follow the single-CTA matrices (the last jobs, by size)
+        const bool extend = !b.tri_buckets.empty() && b.tri_buckets.back().C == 1 &&
+                            b.tri_buckets.back().off + b.tri_buckets.back().count == (int)tix.size();
+        if (!extend) b.tri_buckets.push_back({(int)tix.size(), 0, 1, 0});
+        b.tri_buckets.back().count += nhand;
+        b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tridiag_one_cta_max(), 1));
     }
     std::stable_sort(b.sp2_big.begin(), b.sp2_big.end(), [&](int x, int y) { return hsp2[x].n > hsp2[y].n; });
     std::copy(b.sp2_big.begin(), b.sp2_big.end(), (int*)(Hs + o_sp2big));

@@ -189,6 +189,21 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const TriJob* __restric
         const double kk = 0.5 * beta * pv;
         for (int r = s + 1 + tid; r < n; r += TRI_THREADS) wb[(size_t)nxt * n + r] -= kk * vn[r];
         __syncthreads();
+        if (s + 1 == jb.stop) {  // uniform over the cluster
+            // hand-off: the trailing block with update s applied, to W (m x m, row-major)
+            const int s0 = s + 1, m = n - s0;
+            const double* wv = wb + (size_t)nxt * n;
+            for (int lr = (s0 - crank + C - 1) / C + warp; lr < R; lr += TRI_WARPS) {
+                const int c = lr * C + crank;
+                if (c >= n) break;
+                const double vc = vn[c], wc = wv[c];
+                const double* arow = A + (size_t)lr * n;
+                double* out = jb.W + (size_t)(c - s0) * m - s0;
+                for (int r = s0 + lane; r < n; r += 32) out[r] = arow[r] - vc * wv[r] - wc * vn[r];
+            }
+            csync();  // no CTA leaves while another may still address its shared memory
+            return;
+        }
     }
     __syncthreads();
     // the last 2 x 2 block (or the 1 x 1 matrix)

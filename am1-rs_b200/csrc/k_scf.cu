@@ -452,6 +452,7 @@ __global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __
 }
 
 constexpr int COMBINE_CHUNK = 4;
+constexpr double COMBINE_DIFF_GATE = 0.5;
 
 __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int force) {
     const ChanJob jb = jobs[blockIdx.y];
@@ -463,8 +464,10 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
     const int m = s.hist_count;
     // from the second iteration on, F* still holds the previous iteration's: the distance between the
     // two (row sums of squares) lets k_sp2_bounds widen the previous spectral interval instead of
-    // running the Lanczos bounds again
-    const bool diff = s.iter > 0;
+    // running the Lanczos bounds again.  It is only worth its extra read of F* once the density has
+    // nearly settled (||P - P_previous||_F < COMBINE_DIFF_GATE); before that the rows report NaN and
+    // the bounds run Lanczos.
+    const bool diff = s.iter > 0 && s.dp * n < COMBINE_DIFF_GATE;
     const int mode = s.mode;
     const double* hrow[MAX_DIIS];  // history entries in logical order, and their coefficients
     double cf[MAX_DIIS];
@@ -520,7 +523,7 @@ __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __re
         if (lane == 0) {
             jb.rowmin[r] = diag - bound;
             jb.rowmax[r] = diag + bound;
-            jb.rowdf[r] = dd;
+            jb.rowdf[r] = diff ? dd : __longlong_as_double(0x7ff8000000000000LL);
         }
     }
 }

@@ -121,6 +121,11 @@ struct TriJob {
     double* e;         // off-diagonal, n
     double* eps;       // ascending eigenvalues, n
     int n, mol;
+    // k_tridiag on a cluster: 0 runs the reduction to the end; stop > 0 ends it after `stop`
+    // reflectors and writes the trailing block (rows and columns >= stop, its last update applied)
+    // row-major to W, n - stop rows of n - stop, which a one-CTA job (A = W, d and e from index
+    // stop on) then reduces
+    int stop;
 };
 
 // Loop counters of the captured solve (k_graph.cu), in device memory.
