@@ -155,16 +155,19 @@ int g_sms = 148;        // SMs of the current device
 
 // Smallest cluster (1, 2, 4, 8, 16 CTAs) whose row share of an n x n matrix fits one CTA's
 // shared memory; 0 when none does.
-// Largest matrix one tridiagonalisation CTA holds (the order the cluster reductions hand over at).
-int tridiag_one_cta_max() {
-    static thread_local int cached_budget = -1, cached = 0;
+// Largest matrix a tridiagonalisation cluster of C CTAs holds (the order a reduction on 2 C CTAs
+// hands over at).
+int tridiag_cluster_max(int C) {
+    static thread_local int cached_budget = -1, cached[5] = {};
     if (cached_budget != g_tridiag_budget) {
-        int m = 2;
-        while (tridiag_smem_bytes(m + 1, 1) <= (size_t)g_tridiag_budget) ++m;
-        cached = m;
+        for (int k = 0; k < 5; ++k) {
+            int m = 2;
+            while (tridiag_smem_bytes(m + 1, 1 << k) <= (size_t)g_tridiag_budget) ++m;
+            cached[k] = m;
+        }
         cached_budget = g_tridiag_budget;
     }
-    return cached;
+    return cached[C == 1 ? 0 : C == 2 ? 1 : C == 4 ? 2 : C == 8 ? 3 : 4];
 }
 
 int tridiag_cluster(int n) {
@@ -835,7 +838,7 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     const size_t o_xfmaps = take(st, mixed ? sizeof(TmaDesc) * 2 * std::max<long long>(nch_total, 1) : sizeof(TmaDesc) * 2);
     const size_t o_tct = take(st, sizeof(GemmTile) * std::max(tiles_tc, 1));
     const size_t o_ozt = take(st, sizeof(GemmTile) * std::max(tiles_oz, 1));
-    const size_t o_tri = take(st, sizeof(TriJob) * 2 * nch_total);  // the jobs, then the one-CTA continuations
+    const size_t o_tri = take(st, sizeof(TriJob) * 5 * nch_total);  // the jobs, then up to 4 continuations each
     const size_t o_sp2big = take(st, sizeof(int) * nch_total);
     const size_t o_st = take(st, sizeof(MolState) * b.nmol);
     const size_t par_bytes = host_tab ? sizeof(DevElem) * 2 * (MAX_Z + 1) : 0;
@@ -1216,7 +1219,14 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
     std::stable_sort(tix.begin(), tix.end(), [&](int x, int y) { return tri_all[x].n > tri_all[y].n; });
     b.tri_buckets.clear();
     b.tri_big.clear();
-    int nhand = 0;
+    // A cluster reduction of C CTAs stops once its trailing block fits C / 2 CTAs, writes it to the
+    // channel's free GT slot (W), and a job on C / 2 CTAs continues from there (A = W), down to one
+    // CTA: each level frees SMs for the other matrices.  Launch order: per cluster size, largest
+    // first, the matrices of that size, then the continuations into it (each after its parent).
+    std::vector<TriJob> conts[5];  // continuations into 1, 2, 4, 8, 16 CTAs
+    int first_of[5], count_of[5];
+    for (int k = 0; k < 5; ++k) first_of[k] = -1, count_of[k] = 0;
+    auto lg = [](int C) { return C == 1 ? 0 : C == 2 ? 1 : C == 4 ? 2 : C == 8 ? 3 : 4; };
     for (size_t i = 0; i < tix.size(); ++i) {
         const TriJob& tj = tri_all[tix[i]];
         htri[i] = tj;
@@ -1225,33 +1235,50 @@ int build_batch(const am1gpu_molecule* in, const am1gpu_options& o, std::vector<
             b.tri_big.push_back(tj);
             continue;
         }
-        if (b.tri_buckets.empty() || b.tri_buckets.back().C != C) b.tri_buckets.push_back({(int)i, 0, C, 0});
-        b.tri_buckets.back().count++;
-        b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tj.n, C));
-        // a cluster reduction stops once its trailing block fits one CTA, writes it to the channel's
-        // free GT slot, and a one-CTA job (launched with the single-CTA matrices, after every cluster
-        // launch) finishes it: the cluster's SMs are freed for the other matrices
-        const int m1 = tridiag_one_cta_max();
-        if (C > 1 && m1 >= 8 && m1 < tj.n) {
-            htri[i].stop = tj.n - m1;
-            TriJob h2 = tj;
+        if (first_of[lg(C)] < 0) first_of[lg(C)] = (int)i;
+        count_of[lg(C)]++;
+        TriJob* parent = &htri[i];
+        int n_cur = tj.n;
+        for (int c = C; c > 1; c /= 2) {
+            const int m = tridiag_cluster_max(c / 2);
+            if (m < 8 || m >= n_cur) break;
+            parent->stop = n_cur - m;
+            TriJob h2 = *parent;
             h2.A = tj.W;
-            h2.W = nullptr;
+            h2.W = tj.W;
             h2.work = nullptr;
-            h2.d = tj.d + htri[i].stop;
-            h2.e = tj.e + htri[i].stop;
+            h2.d = parent->d + parent->stop;
+            h2.e = parent->e + parent->stop;
             h2.eps = nullptr;
-            h2.n = m1;
+            h2.n = m;
             h2.stop = 0;
-            htri[tix.size() + nhand++] = h2;
+            conts[lg(c / 2)].push_back(h2);
+            parent = &conts[lg(c / 2)].back();
+            n_cur = m;
         }
     }
-    if (nhand > 0) {  // the continuations follow the single-CTA matrices (the last jobs, by size)
-        const bool extend = !b.tri_buckets.empty() && b.tri_buckets.back().C == 1 &&
-                            b.tri_buckets.back().off + b.tri_buckets.back().count == (int)tix.size();
-        if (!extend) b.tri_buckets.push_back({(int)tix.size(), 0, 1, 0});
-        b.tri_buckets.back().count += nhand;
-        b.tri_buckets.back().smem = std::max(b.tri_buckets.back().smem, tridiag_smem_bytes(tridiag_one_cta_max(), 1));
+    {
+        // continuations go after the jobs (k_bisect reads jobs 0 .. njobs - 1), largest cluster first;
+        // a parent's stop is final before it is copied, since a job's continuation is pushed after it
+        size_t at = tix.size();
+        int cont_first[5];
+        for (int k = 4; k >= 0; --k) {
+            cont_first[k] = (int)at;
+            for (const TriJob& h2 : conts[k]) htri[at++] = h2;
+        }
+        for (int k = 4; k >= 0; --k) {
+            const int C = 1 << k;
+            if (count_of[k] > 0) {
+                size_t sm = 0;
+                for (int i = first_of[k]; i < first_of[k] + count_of[k]; ++i) sm = std::max(sm, tridiag_smem_bytes(htri[i].n, C));
+                b.tri_buckets.push_back({first_of[k], count_of[k], C, sm});
+            }
+            if (!conts[k].empty()) {
+                size_t sm = 0;
+                for (const TriJob& h2 : conts[k]) sm = std::max(sm, tridiag_smem_bytes(h2.n, C));
+                b.tri_buckets.push_back({cont_first[k], (int)conts[k].size(), C, sm});
+            }
+        }
     }
     std::stable_sort(b.sp2_big.begin(), b.sp2_big.end(), [&](int x, int y) { return hsp2[x].n > hsp2[y].n; });
     std::copy(b.sp2_big.begin(), b.sp2_big.end(), (int*)(Hs + o_sp2big));
