@@ -535,11 +535,24 @@ __global__ void k_density_post(const ChanJob* __restrict__ jobs, const MolState*
     if ((int)blockIdx.x >= nb) return;
     const long long nn = (long long)jb.n * jb.n;
     double acc = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)nb * blockDim.x) {
-        const double pn = jb.Pnew[i];
-        const double d = pn - jb.P[i];
-        acc += d * d;
-        jb.P[i] = pn;
+    const long long stride = (long long)nb * blockDim.x;
+    // four elements per trip, their loads before their stores; each thread keeps its order of the sum
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < nn; i0 += 4 * stride) {
+        double pn[4], po[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long i = i0 + u * stride;
+            pn[u] = i < nn ? jb.Pnew[i] : 0.0;
+            po[u] = i < nn ? jb.P[i] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long i = i0 + u * stride;
+            if (i >= nn) break;
+            const double d = pn[u] - po[u];
+            acc += d * d;
+            jb.P[i] = pn[u];
+        }
     }
     __shared__ double part[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

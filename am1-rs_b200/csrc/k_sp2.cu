@@ -468,11 +468,20 @@ __global__ void k_sp2_init(const Sp2Job* __restrict__ jobs, Sp2State* __restrict
             continue;
         }
         double* Xr = jb.X0 + (long long)r * n;
-        for (int c = lane; c < n; c += 32) {
-            const double x = ((c == r ? emax : 0.0) - Fr[c]) * inv;
-            Xr[c] = x;
-            fr += x * x;
-            if (c == r) tr += x;
+        // four columns per lane per trip, their loads before their stores (each lane keeps its order)
+        for (int c0 = lane; c0 < n; c0 += 128) {
+            double f[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) f[u] = c0 + 32 * u < n ? Fr[c0 + 32 * u] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + 32 * u;
+                if (c >= n) break;
+                const double x = ((c == r ? emax : 0.0) - f[u]) * inv;
+                Xr[c] = x;
+                fr += x * x;
+                if (c == r) tr += x;
+            }
         }
         if (jb.oz) {  // the digit planes of X0, and zero pad columns in both digit buffers
             const long long plane = (long long)n * jb.ldq;
@@ -741,8 +750,15 @@ __global__ void k_sp2_finish(const Sp2Job* __restrict__ jobs, const Sp2State* __
         return;
     }
     const double* X = s.cur ? jb.X1 : jb.X0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x)
-        jb.P[i] = jb.weight * X[i];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < nn; i0 += 4 * stride) {
+        double x[4];  // P may be X0: every load of the trip before its stores
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = i0 + u * stride < nn ? X[i0 + u * stride] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (i0 + u * stride < nn) jb.P[i0 + u * stride] = jb.weight * x[u];
+    }
 }
 
 size_t dgemm_smem_bytes() { return DG_SMEM; }
