@@ -111,12 +111,21 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
         const double* Hr = jb.H + (long long)r * n;
         const long long rs = sym_row(r, n);
         for (int c = r + lane; c < n; c += 32) {
+            const long long si = rs + (c - r);
+            // the live history entries are loaded with F, P and H, before this element's stores, so
+            // an element costs one round trip to memory
+            double hf[MAX_DIIS], hd[MAX_DIIS];
+#pragma unroll
+            for (int j = 0; j < MAX_DIIS; ++j) {
+                const bool ld = !energy_only && adiis && j != newslot && (live >> j & 1u);
+                hf[j] = ld ? jb.hF[j * ls + si] : 0.0;
+                hd[j] = ld ? jb.hD[j * ls + si] : 0.0;
+            }
             const double f = Fr[c], p = Pr[c], hh = Hr[c];
             const double wgt = c == r ? 1.0 : 2.0;
             acc[RED_E_H] += wgt * p * hh;
             acc[RED_E_F] += wgt * p * f;
             if (energy_only) continue;
-            const long long si = rs + (c - r);
             jb.hF[newslot * ls + si] = f;
             if (adiis) {
                 jb.hD[newslot * ls + si] = p;
@@ -125,8 +134,8 @@ __global__ void __launch_bounds__(32 * POST_WARPS) k_post_fock(const ChanJob* __
                     if (j == newslot) {
                         acc[RED_GROW + j] += wgt * p * f;
                     } else if (live >> j & 1u) {
-                        acc[RED_GROW + j] += wgt * p * jb.hF[j * ls + si];
-                        acc[RED_GCOL + j] += wgt * jb.hD[j * ls + si] * f;
+                        acc[RED_GROW + j] += wgt * p * hf[j];
+                        acc[RED_GCOL + j] += wgt * hd[j] * f;
                     }
             }
         }
@@ -213,6 +222,16 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
         const int r = m0 + rl;
         if (r >= n) break;
         const long long arow = anti_row(r, n) - r - 1;  // packed index of (r, c) is arow + c
+        // both columns' loads of the live slots before the row's stores: one round trip per row
+        double eq[2][MAX_DIIS];
+#pragma unroll
+        for (int hlf = 0; hlf < 2; ++hlf) {
+            const int c = n0 + lane + 32 * hlf;
+            const bool in = r < c && c < n;
+#pragma unroll
+            for (int q = 0; q < MAX_DIIS; ++q)
+                eq[hlf][q] = in && q != newslot && (live >> q & 1u) ? jb.hE[q * la + arow + c] : 0.0;
+        }
 #pragma unroll
         for (int hlf = 0; hlf < 2; ++hlf) {
             const int cl = lane + 32 * hlf, c = n0 + cl;
@@ -226,7 +245,7 @@ __device__ __forceinline__ void commutator_body(const ChanJob* __restrict__ jobs
                     if (q == newslot)
                         v[CP_B + q] += ev * ev;
                     else if (live >> q & 1u)
-                        v[CP_B + q] += ev * jb.hE[q * la + ai];
+                        v[CP_B + q] += ev * eq[hlf][q];
             }
         }
     }
@@ -451,7 +470,7 @@ __global__ void k_diis_solve(const MolDesc* __restrict__ mols, const ChanJob* __
     }
 }
 
-constexpr int COMBINE_CHUNK = 4;
+constexpr int COMBINE_CHUNK = 8;
 constexpr double COMBINE_DIFF_GATE = 0.5;
 
 __global__ void k_combine(const ChanJob* __restrict__ jobs, const MolState* __restrict__ st, int force) {
