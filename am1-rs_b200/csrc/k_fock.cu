@@ -199,22 +199,40 @@ __global__ void __launch_bounds__(32 * FOCK_WARPS, 2) k_fock(const MolDesc* __re
             }
             jl[0] += acc;
         }
-        // hydrogen partners B (HH blocks); exchange when A is the first atom (B > A)
-        for (int B = h + lane; B < N; B += 32) {
-            if (B == A) continue;
-            const int B2 = B - h;
-            const int i2 = min(A2, B2), j2 = max(A2, B2);
-            const double wv = w[xxsz + xhsz + ((long long)i2 * Hn - (long long)i2 * (i2 + 1) / 2 + (j2 - i2 - 1))];
-            const int oB = 4 * h + B2;
-            jl[0] += wv * ptot((long long)oB * n + oB);
-            if (B > A) {
-                const long long ab = (long long)oA * n + oB, ba = (long long)oB * n + oA;
-                const double hab = H0[ab];
-                for (int c = 0; c < md.nch; ++c) {
-                    const double v = hab - sc * (c == 0 ? P0 : P1)[ab] * wv;
-                    double* F = c == 0 ? F0 : F1;
-                    F[ab] = v;
-                    F[ba] = v;
+        // hydrogen partners B (HH blocks); exchange when A is the first atom (B > A).  Two partners per
+        // lane per trip, every load of the trip before its stores; each lane keeps its partner order.
+        for (int B0 = h + lane; B0 < N; B0 += 64) {
+            double wv[2], pbb[2], hab[2], pab[2][2];
+            long long ab[2], ba[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int B = B0 + 32 * u;
+                const bool valid = B < N && B != A, ex = valid && B > A;
+                const int B2 = B - h;
+                const int i2 = min(A2, B2), j2 = max(A2, B2);
+                const int oB = 4 * h + B2;
+                wv[u] = valid ? w[xxsz + xhsz + ((long long)i2 * Hn - (long long)i2 * (i2 + 1) / 2 + (j2 - i2 - 1))] : 0.0;
+                pbb[u] = valid ? ptot((long long)oB * n + oB) : 0.0;
+                ab[u] = (long long)oA * n + oB;
+                ba[u] = (long long)oB * n + oA;
+                hab[u] = ex ? H0[ab[u]] : 0.0;
+                pab[u][0] = ex ? P0[ab[u]] : 0.0;
+                pab[u][1] = ex && P1 ? P1[ab[u]] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int B = B0 + 32 * u;
+                if (!(B < N && B != A)) continue;
+                jl[0] += wv[u] * pbb[u];
+                if (B > A) {
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        if (c >= md.nch) break;
+                        const double v = hab[u] - sc * pab[u][c] * wv[u];
+                        double* F = c == 0 ? F0 : F1;
+                        F[ab[u]] = v;
+                        F[ba[u]] = v;
+                    }
                 }
             }
         }
