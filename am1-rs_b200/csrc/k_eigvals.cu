@@ -30,6 +30,10 @@ namespace cg = cooperative_groups;
 //   cluster barrier: every CTA's share ready; each CTA sums the C shares itself -> p, w_s
 // Column s below the diagonal is never updated: row s holds the same numbers and is the one read.
 // All control flow is uniform over the cluster, so every CTA takes the same barriers.
+// With job.stop > 0 the loop ends after reflector stop - 1: the trailing block (rows and columns
+// >= stop) with update stop - 1 applied goes to job.W (row-major, n - stop rows), and a job on fewer
+// CTAs reduces it as a matrix of its own, writing d and e from index stop on.  Its tridiagonal
+// continues this one's: the block's reflectors act on indices >= stop + 1 and leave e[stop - 1] as is.
 constexpr int TRI_THREADS = 512;
 constexpr int TRI_WARPS = TRI_THREADS / 32;
 
